@@ -1,0 +1,226 @@
+/*
+ * witwin_channel_b200 -- C ABI of the B200 deterministic radiomap/path engine.
+ *
+ * Plain pointers, sizes and a cudaStream_t (passed as void*); no C++ or
+ * framework types.  Every entry point returns a wcb_status; device-side
+ * failures are reported through a status word the host reads, never by a
+ * device trap.  The caller owns every buffer passed in; scene handles own
+ * their scene tables.
+ *
+ * Reference interfaces replaced (paths within witwin-ai/witwin-channel):
+ *   wcb_scene_create   <- scene/compiler.py:1306-1450 (compile) +
+ *                         scene/resources.py:169-240 (RayD scene build) +
+ *                         propagation/geometry.py:128-161 (coplanar groups) +
+ *                         native/channel/kernels/diffraction.cu:803-900 and
+ *                         scene/resources.py:356-405 (edge selection/refinement)
+ *   wcb_solve          <- deterministic.py:786-949 (_solve_pipeline) through
+ *                         propagation/enumerated.py:549-836 and the native ops
+ *                         it calls (los.cu:74-125, paths.cu:317-361,
+ *                         rayd/reflection.cpp:24-57, rayd/diffraction.cpp,
+ *                         rayd/geometry.cpp:188-212, fields.cu:36-204,
+ *                         deterministic.cu:829-970)
+ *   wcb_rows_*         <- evaluated_paths.cu:560-760 (canonical sort, dedup,
+ *                         max_paths) + deterministic.py:461-514 (path table)
+ *   wcb_field_*        <- kernels/fields.py facades over fields.cu:36-204 and
+ *                         RayD's field_transmission_sequence
+ *   wcb_rows_vjp       <- kernels/deterministic.py:186-367 and the field AD
+ *                         Functions in kernels/fields.py:1087-2140
+ */
+#ifndef WITWIN_CHANNEL_B200_H
+#define WITWIN_CHANNEL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    WCB_OK = 0,
+    WCB_ERR_INVALID_ARGUMENT = 1,
+    WCB_ERR_CUDA = 2,
+    WCB_ERR_CAPACITY = 3,        /* a caller buffer is too small; *_needed reports the size */
+    WCB_ERR_BVH_DEPTH = 4,       /* traversal stack would overflow */
+    WCB_ERR_NOT_SUPPORTED = 5,
+    WCB_ERR_DEVICE_STATUS = 6    /* a kernel reported a failure bit */
+} wcb_status;
+
+/* Component bits. */
+#define WCB_COMPONENT_LOS 1
+#define WCB_COMPONENT_REFLECTION 2
+#define WCB_COMPONENT_DIFFRACTION 4
+#define WCB_COMPONENT_TRANSMISSION 8
+
+/* Precision modes. */
+#define WCB_PRECISION_MIXED 0 /* FP32 traversal/fields, FP64 image solve, length and phase */
+#define WCB_PRECISION_FP64 1  /* every stage in FP64 */
+
+typedef struct wcb_scene wcb_scene;
+
+/* Scene build.  All pointers are device pointers.
+ * vertices (V,3) f32; faces (F,3) i32; face_surface, face_structure,
+ * face_material (F) i32.  boundary_half_plane: keep boundary edges as
+ * half-planes; vertical_only with vertical_ratio filters edges by |dz|/length. */
+int wcb_scene_create(const float* vertices, int64_t num_vertices, const int32_t* faces, int64_t num_faces,
+                     const int32_t* face_surface, const int32_t* face_structure, const int32_t* face_material,
+                     int32_t boundary_half_plane, int32_t vertical_only, double vertical_ratio, void* stream,
+                     wcb_scene** out);
+int wcb_scene_destroy(wcb_scene* scene);
+/* counts[0..5] = faces, groups, selected edges, bvh depth, bvh nodes, representative faces */
+int wcb_scene_info(const wcb_scene* scene, int64_t* counts);
+/* Group table export: face_group (F) i32, group_rep (G) i32 (device). */
+int wcb_scene_groups(const wcb_scene* scene, int32_t* face_group, int32_t* group_rep, void* stream);
+/* Selected edge export: edge_id (E) i32 (device). */
+int wcb_scene_edges(const wcb_scene* scene, int32_t* edge_id, void* stream);
+
+/* Material tables at each solve frequency.  Per-material arrays are (NF, M)
+ * row-major; layer arrays are (NF, L) with a CSR (offset, count) per material
+ * shared across frequencies. */
+typedef struct {
+    int32_t num_materials;
+    const float* eps_r;
+    const float* sigma_e;
+    const float* mu_r;
+    const float* gain;
+    const float* thickness;
+    const int32_t* volumetric; /* (M) */
+    int32_t num_layers;
+    const int32_t* layer_offset; /* (M) */
+    const int32_t* layer_count;  /* (M) */
+    const float* layer_thickness;
+    const float* layer_eps_r;
+    const float* layer_sigma_e;
+    const float* layer_mu_r;
+} wcb_materials;
+
+/* Endpoints and solve options. */
+typedef struct {
+    int32_t num_tx;
+    const float* tx_pos;    /* (T,3) device */
+    const float* tx_power;  /* (T)   device */
+    const float* tx_pol;    /* (T,3) device */
+    int32_t rx_kind;        /* 0: points, 1: grid */
+    int32_t num_rx;
+    const float* rx_pos;    /* (R,3) device; points only */
+    float grid_origin[3];
+    float grid_x_axis[3];
+    float grid_y_axis[3];
+    int32_t grid_rows;
+    int32_t grid_cols;
+    float grid_spacing[2];
+    const float* rx_pol;     /* (R,3) or (1,3) device */
+    int32_t rx_pol_stride;   /* 3 for per-receiver polarization, 0 for one shared vector */
+    int32_t num_freq;
+    const double* frequency_hz; /* host array (NF) */
+    int32_t components;      /* WCB_COMPONENT_* bits */
+    int32_t max_depth;
+    int32_t coherent;
+    int32_t precision;       /* WCB_PRECISION_* */
+    int32_t discovery_rays;  /* 0 selects the default 262144 */
+} wcb_solve_desc;
+
+/* Per-cell outputs, all device, NF-major:
+ *   path_gain (NF,T,R) f32, field (NF,T,R) complex64 (interleaved f32 pairs),
+ *   comp_power (6,NF,T,R) f32, comp_field (6,NF,T,R) complex64,
+ *   diff_vec_power (NF,T,R) f32 (sum over xyz of |sum_paths E|^2).
+ * Any pointer may be NULL to skip that output.  In FP64 precision mode the
+ * same outputs are float64 / complex128.
+ * rows: optional compact path records (wcb_row, 48 bytes each); row_count is
+ * a device int64 that receives the number of valid paths (it may exceed
+ * row_capacity, in which case the call returns WCB_ERR_CAPACITY).
+ * status: device int32 receiving device failure bits. */
+typedef struct {
+    void* path_gain;
+    void* field;
+    void* comp_power;
+    void* comp_field;
+    void* diff_vec_power;
+    void* rows;
+    int64_t row_capacity;
+    int64_t* row_count;
+    int32_t* status;
+} wcb_outputs;
+
+/* Compact path record (the frozen topology of one path). */
+typedef struct {
+    int32_t tx;
+    int32_t rx;
+    int16_t component;  /* 0 LoS, 1 reflection, 2 diffraction, 5 transmission */
+    int16_t depth;
+    int32_t seq[5];     /* resolved face ids, -1 padded */
+    int32_t edge;       /* reference edge id for diffraction, else -1 */
+    float length;       /* path length (m) */
+    int32_t reserved[2];
+} wcb_row;
+
+/* Scratch bytes a wcb_solve call needs for `desc`. */
+int wcb_solve_workspace_size(const wcb_scene* scene, const wcb_solve_desc* desc, int64_t* bytes);
+
+/* Full fused solve on one scene. */
+int wcb_solve(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_materials* materials,
+              const wcb_outputs* outputs, void* workspace, int64_t workspace_bytes, void* stream);
+
+/* Canonical order of path records: sorts, removes duplicate identities
+ * (shortest kept, NaN drops the group) and applies max_paths (-1 = none;
+ * scope 0 global, 1 per pair).  Writes the selected record indices in
+ * canonical order to `selected` (capacity num_rows) and their count to
+ * *num_selected (host). */
+int wcb_rows_select(const void* rows, int64_t num_rows, int32_t width, int64_t max_paths, int32_t scope,
+                    int64_t* selected, int64_t* num_selected, void* workspace, int64_t workspace_bytes, void* stream);
+int wcb_rows_select_workspace_size(int64_t num_rows, int64_t* bytes);
+
+/* Field evaluation of selected path records at one frequency (index freq
+ * into the materials tables).  Writes the path-table columns; any output
+ * pointer may be NULL. */
+typedef struct {
+    float* path_length_m;   /* (K) */
+    float* delay_s;         /* (K) */
+    float* path_gain;       /* (K) */
+    float* path_field;      /* (K) complex64 */
+    float* coefficient;     /* (K) complex64 */
+    float* field_xyz;       /* (K,3) complex64, unit excitation */
+    float* field_direction; /* (K,3) */
+    float* interaction_positions; /* (K,W,3) */
+    float* interaction_normals;   /* (K,W,3) */
+    float* phase_rad;       /* (K) */
+} wcb_row_fields;
+
+int wcb_rows_evaluate(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_materials* materials,
+                      int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
+                      int32_t width, const wcb_row_fields* out, void* stream);
+
+/* Per-cell accumulation of evaluated rows (selected, canonical order):
+ * per-slot coherent sums and gains written like wcb_outputs for one
+ * frequency (NF = 1).  Deterministic: every cell sums its rows in canonical
+ * order. */
+int wcb_rows_accumulate(const void* rows, const int64_t* selected, int64_t num_selected,
+                        const float* path_gain, const float* path_field, const float* field_xyz,
+                        const float* tx_power, int32_t num_tx, int32_t num_rx, int32_t coherent,
+                        const wcb_outputs* outputs, void* stream);
+
+/* Standalone field operators (reference kernels/fields.py facades).  All
+ * arrays are device f32; complex outputs interleaved.  N rows. */
+int wcb_field_free_space(int64_t n, const float* source, const float* target, const float* tx_power,
+                         const float* tx_pol, const float* rx_pol, double frequency_hz, float* field_vector,
+                         float* coefficient, float* path_field, float* path_gain, float* path_length,
+                         float* delay, float* direction, void* stream);
+int wcb_field_reflection_sequence(int64_t n, int32_t depth, const float* source, const float* target,
+                                  const float* positions, const float* normals, const float* tx_power,
+                                  const float* tx_pol, const float* rx_pol, const float* eps_r,
+                                  const float* sigma_e, const float* mu_r, const float* gain,
+                                  const float* thickness, double frequency_hz, float* field_vector,
+                                  float* coefficient, float* path_field, float* path_gain, float* path_length,
+                                  float* delay, float* direction, void* stream);
+int wcb_field_project_complex3(int64_t n, const float* field_vector, const float* direction, const float* rx_pol,
+                               float* coefficient, float* path_gain, void* stream);
+
+/* Runtime info: writes a NUL-terminated description (architecture, build). */
+int wcb_build_info(char* buffer, int64_t capacity);
+/* Number of kernel launches issued by this library since load. */
+int64_t wcb_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WITWIN_CHANNEL_B200_H */

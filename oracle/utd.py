@@ -1,0 +1,217 @@
+"""First-order UTD wedge diffraction (oracle, float64/complex128).
+
+The reference evaluates this inside RayD (``rayd/diffraction.cpp:405-455``,
+``utd_math.h``), whose source is not available.  This module restates the
+published Kouyoumjian-Pathak UTD with Luebbers' finite-conductivity
+reflection factors and the finite-edge rules the reference documents in
+``docs/dev/audit/utd-continuity-fix-design.md``:
+
+* F1  incident field = unnormalised transverse Tx polarization, amplitude
+      ``1/(2 k s')`` (the free-space convention), vector output;
+* F3  receiver angle clamped into ``[0, n*pi]`` by nearest-boundary wrap;
+* F4  visibility from the clamped point offset along the exterior bisector;
+* F5c/F5e/F5f  per-term odd/even split about the nearest GO boundary with
+      locality window ``w``, corner sigmoid ``gamma(u)``, monotone truncation
+      ``T_mono`` and the boundary-distance blend ``B`` with ``C_BLEND = 0.35``.
+
+The Keller stationary point and the edge numbering reproduce the reference's
+single-wedge golden lengths exactly; its amplitudes are pinned only loosely.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+from scipy.special import fresnel
+
+from . import em
+
+C_BLEND = 0.35
+GAMMA_SCALE = 0.1
+WINDOW_CUTOFF = 1.0e-3
+GAIN_FLOOR = 1.0e-30
+RAY_BIAS = 1.0e-4
+MIN_DISTANCE = 1.0e-4  # F2
+
+
+def fresnel_cs(x):
+    s, c = fresnel(x)
+    return c + 1.0j * s
+
+
+def transition(x: float) -> complex:
+    """KP transition function ``F(x) = 2j sqrt(x) e^{jx} int_{sqrt x}^inf e^{-j t^2} dt``."""
+    if x <= 0.0:
+        return 0.0 + 0.0j
+    sx = np.sqrt(x)
+    u0 = sx * np.sqrt(2.0 / np.pi)
+    cs = fresnel_cs(u0)
+    integral = np.sqrt(np.pi / 2.0) * ((0.5 - cs.real) - 1.0j * (0.5 - cs.imag))
+    return 2.0j * sx * np.exp(1.0j * x) * integral
+
+
+def term(beta: float, n: float, kl: float, sign: int) -> complex:
+    """``cot((pi + sign*beta)/(2n)) F(kL a^sign(beta))`` written in the distance
+    ``eps`` to the term's own singular point: ``cot(eps/(2n)) F(2 kL sin^2(eps/2))``
+    (identical to the textbook N-selection form; numerically stable near the
+    shadow boundaries, where the KP limit
+    ``n (sgn(eps) sqrt(2 pi kL) - 2 kL eps e^{j pi/4}) e^{j pi/4}`` is used)."""
+    arg = np.pi + sign * beta
+    m = np.round(arg / (2.0 * n * np.pi))
+    eps = arg - 2.0 * n * np.pi * m
+    ej = np.exp(1.0j * np.pi / 4.0)
+    if abs(eps) < 1e-9:
+        sg = -1.0 if eps < 0 else 1.0
+        return n * (sg * np.sqrt(2.0 * np.pi * kl) - 2.0 * kl * eps * ej) * ej
+    return transition(2.0 * kl * np.sin(eps / 2.0) ** 2) / np.tan(eps / (2.0 * n))
+
+
+def edge_frame(edge: dict, e: int):
+    """Unit edge direction ``e_hat``, face-0 tangent ``t0`` (into face 0) and
+    ``n0`` with ``t0 = n0 x e_hat``, so ``phi = atan2(d.n0, d.t0)`` runs from
+    face 0 (0) through the exterior to face n (``n*pi``)."""
+    e_hat = edge["edge_dir"][e].copy()
+    n0 = edge["n0"][e]
+    t0 = np.cross(n0, e_hat)
+    t0 /= np.linalg.norm(t0)
+    if np.dot(edge["opp0"][e] - edge["edge_pos"][e], t0) < 0.0:
+        e_hat = -e_hat
+        t0 = -t0
+    return e_hat, t0, n0
+
+
+def _angle(d: np.ndarray, t0: np.ndarray, n0: np.ndarray) -> float:
+    a = np.arctan2(np.dot(d, n0), np.dot(d, t0))
+    return a + 2.0 * np.pi if a < 0.0 else a
+
+
+def stationary_point(S, R, c, e_hat):
+    ts = np.dot(S - c, e_hat)
+    rs = np.linalg.norm(S - c - ts * e_hat)
+    tr = np.dot(R - c, e_hat)
+    rr = np.linalg.norm(R - c - tr * e_hat)
+    if rs + rr <= 0.0:
+        return ts
+    return ts + (tr - ts) * rs / (rs + rr)
+
+
+def _tails(sigma, t_star, t_min, t_max):
+    f_inf = 0.5 + 0.5j
+    half = 0.5 + 0.5j
+    hi = half * np.conj(f_inf - fresnel_cs(sigma * (t_max - t_star)))
+    lo = half * np.conj(fresnel_cs(sigma * (t_min - t_star)) + f_inf)
+    return lo, hi
+
+
+def source_exterior(S, edge: dict, e: int) -> tuple[bool, float]:
+    e_hat, t0, n0 = edge_frame(edge, e)
+    d = S - edge["edge_pos"][e]
+    d = d - np.dot(d, e_hat) * e_hat
+    phi_p = _angle(d, t0, n0)
+    n = edge["exterior_angle"][e] / np.pi
+    return bool(phi_p <= n * np.pi), phi_p
+
+
+def diffraction_field(S, R, tx_pol, edge: dict, e: int, mats: dict, frequency: float):
+    """UTD field at ``R`` for edge ``e``.
+
+    Returns ``(field_xyz_unit, Q_star, Q_clamped_biased, s_prime, s)`` or ``None``
+    when the source lies inside the wedge.  ``field_xyz_unit`` is the
+    unit-excitation complex 3-vector (multiply by sqrt(P) for the path field).
+    """
+    k = em.wave_number(frequency)
+    c = edge["edge_pos"][e]
+    e_hat, t0, n0 = edge_frame(edge, e)
+    n = edge["exterior_angle"][e] / np.pi
+    h = 0.5 * edge["length"][e]
+    t_min, t_max = -h, h
+    # the frame may have flipped e_hat; the stationary parameter is along e_hat
+    t_star = stationary_point(S, R, c, e_hat)
+    q = c + t_star * e_hat
+    tc = min(max(t_star, t_min), t_max)
+    bis = edge["n0"][e] + edge["n1"][e]
+    bl = np.linalg.norm(bis)
+    bis = bis / bl if bl > 1e-6 else -t0
+    q_vis = c + tc * e_hat + RAY_BIAS * bis
+    sp_vec = q - S
+    s_vec = R - q
+    s_p = max(np.linalg.norm(sp_vec), MIN_DISTANCE)
+    s = max(np.linalg.norm(s_vec), MIN_DISTANCE)
+    sh_p = sp_vec / s_p
+    sh = s_vec / s
+    dsrc = S - c
+    dsrc = dsrc - np.dot(dsrc, e_hat) * e_hat
+    drx = R - c
+    drx = drx - np.dot(drx, e_hat) * e_hat
+    phi_p = _angle(dsrc, t0, n0)
+    phi = _angle(drx, t0, n0)
+    if phi_p > n * np.pi:
+        return None
+    if phi > n * np.pi:
+        phi = n * np.pi if (phi - n * np.pi) < (2.0 * np.pi - phi) else 0.0
+    cos_b = np.clip(np.dot(sh_p, e_hat), -1.0, 1.0)
+    sin_b = max(np.sqrt(max(1.0 - cos_b * cos_b, 0.0)), 1e-6)
+    kl = k * s * s_p * sin_b * sin_b / (s + s_p)
+    # finite edge truncation factors (F5e, F5f)
+    rho_p = s_p * sin_b
+    rho = s * sin_b
+    kappa = rho_p * rho_p / s_p ** 3 + rho * rho / s ** 3
+    sigma = np.sqrt(k * kappa / np.pi)
+    lo, hi = _tails(sigma, t_star, t_min, t_max)
+    t_mono = min(max(1.0 - abs(lo) - abs(hi), 0.0), 1.0)
+    if abs(t_star - t_max) < abs(t_star - t_min):
+        u = sigma * (t_star - t_max)
+    else:
+        u = sigma * (t_min - t_star)
+    gamma = 1.0 / (1.0 + np.exp(min(u / GAMMA_SCALE, 700.0)))
+    unit = np.sqrt(2.0 * np.pi / kl)
+    delta_w = 4.0 * unit
+    delta_b = C_BLEND * unit
+    # face reflection factors (Luebbers): 0-face at grazing phi', n-face at n*pi - phi
+    f0 = edge["wedge_face0"][e]
+    f1 = edge["wedge_face1"][e]
+    r0 = em.slab_fresnel(np.array(np.sin(phi_p)), *(mats[x][f0] for x in ("eps_r", "sigma_e", "mu_r", "gain", "thickness")), frequency)
+    if f1 >= 0:
+        rn = em.slab_fresnel(np.array(np.sin(n * np.pi - phi)), *(mats[x][f1] for x in ("eps_r", "sigma_e", "mu_r", "gain", "thickness")), frequency)
+    else:
+        rn = em.slab_fresnel(np.array(np.sin(n * np.pi - phi)), *(mats[x][f0] for x in ("eps_r", "sigma_e", "mu_r", "gain", "thickness")), frequency)
+    bm = phi - phi_p
+    bp = phi + phi_p
+
+    def mended(beta: float, sign: int, group: str) -> complex:
+        value = term(beta, n, kl, sign)
+        if group == "inc":
+            b_star = np.pi if abs(beta - np.pi) <= abs(beta + np.pi) else -np.pi
+        else:
+            b_star = np.pi if abs(beta - np.pi) <= abs(beta - (2.0 * n - 1.0) * np.pi) else (2.0 * n - 1.0) * np.pi
+        delta = beta - b_star
+        w = np.exp(-((delta / delta_w) ** 2))
+        if w <= WINDOW_CUTOFF:
+            w = 0.0
+        mirrored = term(2.0 * b_star - beta, n, kl, sign)
+        odd = 0.5 * (value - mirrored) * w
+        wb = np.exp(-((delta / delta_b) ** 2))
+        blend = wb + (1.0 - wb) * t_mono
+        return (value - odd) * t_mono + odd * gamma * blend
+
+    t1 = mended(bm, +1, "inc")
+    t2 = mended(bm, -1, "inc")
+    t3 = mended(bp, +1, "ref")
+    t4 = mended(bp, -1, "ref")
+    pre = -np.exp(-1.0j * np.pi / 4.0) / (2.0 * n * np.sqrt(2.0 * np.pi * k) * sin_b)
+    d_soft = pre * (t1 + t2 + rn[0] * t3 + r0[0] * t4)
+    d_hard = pre * (t1 + t2 + rn[1] * t3 + r0[1] * t4)
+    # ray-fixed bases (Kouyoumjian-Pathak)
+    phi_hat_p = np.cross(e_hat, sh_p)
+    phi_hat_p /= max(np.linalg.norm(phi_hat_p), 1e-12)
+    beta_hat_p = np.cross(sh_p, phi_hat_p)
+    phi_hat = np.cross(e_hat, sh)
+    phi_hat /= max(np.linalg.norm(phi_hat), 1e-12)
+    beta_hat = np.cross(sh, phi_hat)
+    tx_axis = em.transverse_project(sh_p[None, :], np.asarray(tx_pol, dtype=np.float64)[None, :])[0]
+    inc_amp = 1.0 / (2.0 * k * s_p)
+    e_beta = np.dot(tx_axis, beta_hat_p) * inc_amp
+    e_phi = np.dot(tx_axis, phi_hat_p) * inc_amp
+    spread = np.sqrt(s_p / (s * (s_p + s)))
+    phase = np.exp(-1.0j * k * (s_p + s))
+    field = (-d_soft * e_beta * beta_hat - d_hard * e_phi * phi_hat) * spread * phase
+    return field, q, q_vis, s_p, s

@@ -1,0 +1,170 @@
+"""GPU parity: the native solve against the FP64 oracle and the reference's
+golden vectors.  Tolerances: path gain 0.01 dB, phase 1e-3 rad, lengths
+1e-5 relative; integer topology (path sets, sequences, edge ids) exact."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import solve as osolve
+from tests import scenes
+from witwin_channel_b200 import Config, solve
+
+pytestmark = pytest.mark.gpu
+
+DB_TOL = 0.01
+PHASE_TOL = 1.0e-3
+
+
+def _oracle(scene, freq, **kw):
+    arr = osolve.scene_arrays(scene, freq)
+    return osolve.solve(arr, frequency=freq, edge_policy=scene.metadata.get("imported_edge_policy"), **kw)
+
+
+def _grid_flat(x: torch.Tensor, shape):
+    rows, cols = shape
+    return x.transpose(1, 2).reshape(x.shape[0], rows * cols)
+
+
+def _db(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    mask = (a > 0) | (b > 0)
+    return np.abs(10.0 * np.log10(np.maximum(a[mask], 1e-300) / np.maximum(b[mask], 1e-300)))
+
+
+def _rows_key(t, r, c, d, seq, e):
+    return [(int(t[i]), int(r[i]), int(c[i]), int(d[i]), tuple(int(x) for x in seq[i]), int(e[i])) for i in range(len(t))]
+
+
+def _compare_paths(res, ref):
+    p = res.paths
+    got = _rows_key(p.tx_id.cpu(), p.rx_id.cpu(), p.component_id.cpu(), p.depth.cpu(), p.primitive_sequence.cpu(),
+                    p.edge_id.cpu())
+    r = ref["rows"]
+    want = _rows_key(r["tx_id"], r["rx_id"], r["component_id"], r["depth"], r["primitive_sequence"], r["edge_id"])
+    assert got == want
+    np.testing.assert_allclose(p.path_length_m.cpu().numpy(), r["path_length_m"], rtol=1e-5, atol=1e-5)
+    g = p.path_gain.cpu().numpy()
+    assert np.all(_db(g, r["path_gain"]) <= DB_TOL)
+    pf = torch.complex(p.field_real, p.field_imag).cpu().numpy()
+    strong = np.abs(r["path_field"]) > 1e-6 * np.abs(r["path_field"]).max()
+    ph = np.abs(np.angle(pf[strong] / r["path_field"][strong]))
+    assert np.all(ph <= PHASE_TOL), ph.max()
+
+
+def test_two_wall_multibounce_golden_and_oracle():
+    scene = scenes.two_wall_scene()
+    res = solve(scene, Config(components={"reflection"}, max_depth=2, coherent=True, export_paths=True),
+                reference_frequency_hz=3.0e9)
+    p = res.paths
+    # golden: tests/deterministic/test_reflection_multibounce.py:185-205
+    assert p.depth.tolist() == [1, 1, 2]
+    assert p.primitive_sequence.tolist() == [[0, -1], [2, -1], [1, 2]]
+    torch.testing.assert_close(p.path_length_m.cpu(), torch.tensor([4.123105526, 3.0, 5.0]), rtol=1e-5, atol=1e-6)
+    ref = _oracle(scene, 3.0e9, components={"reflection"}, max_depth=2)
+    _compare_paths(res, ref)
+    torch.testing.assert_close(res.path_gain.cpu(), res.field.abs().square().cpu(), rtol=2e-4, atol=1e-10)
+
+
+def test_single_wedge_edges_and_lengths_golden():
+    scene = scenes.wedge_scene()
+    res = solve(scene, Config(components={"diffraction"}, coherent=False, export_paths=True, return_field=False),
+                reference_frequency_hz=3.0e9)
+    p = res.paths
+    # golden: tests/deterministic/test_diffraction_single_wedge.py:36-80
+    assert p.edge_id.tolist() == [0, 1, 2, 5]
+    torch.testing.assert_close(p.path_length_m.cpu(),
+                               torch.tensor([3.650281668, 4.744879723, 3.768759727, 4.046976566]),
+                               rtol=1e-5, atol=1e-6)
+    ref = _oracle(scene, 3.0e9, components={"diffraction"}, max_depth=1, coherent=False)
+    _compare_paths(res, ref)
+
+
+def test_los_grid_layout_matches_closed_form():
+    scene = scenes.los_grid_scene()
+    res = solve(scene, Config(max_depth=0, components={"los"}), reference_frequency_hz=3.0e9)
+    assert tuple(res.path_gain.shape) == (1, 3, 2)
+    # reference_channel.py:35-81 closed form
+    grid = scene.receivers[0]
+    pts = grid.points().double()
+    tx = torch.tensor([0.0, 0.0, 0.0], dtype=torch.float64)
+    d = pts - tx
+    dist = d.norm(dim=-1)
+    khat = d / dist[:, None]
+    lam = 299792458.0 / 3.0e9
+    pz = torch.tensor([0.0, 0.0, 1.0], dtype=torch.float64)
+    dip = (1.0 - (khat @ pz) ** 2) ** 2
+    want = 1.5 * (lam / (4 * np.pi * dist)) ** 2 * dip
+    want = want.reshape(1, 2, 3).transpose(1, 2)
+    torch.testing.assert_close(res.path_gain.double().cpu(), want, rtol=1e-5, atol=1e-12)
+
+
+@pytest.mark.parametrize("export", [False, True])
+def test_two_ray_radiomap_matches_oracle(export):
+    from witwin_channel_b200.workloads import two_ray_scene
+
+    scene, freq = two_ray_scene(shape=(16, 16), spacing=8.0)
+    res = solve(scene, Config(components={"los", "reflection"}, max_depth=1, export_paths=export),
+                reference_frequency_hz=freq)
+    ref = _oracle(scene, freq, components={"los", "reflection"}, max_depth=1)
+    got = _grid_flat(res.path_gain, (16, 16)).cpu().numpy()
+    assert np.all(_db(got, ref["path_gain"]) <= DB_TOL)
+    gf = _grid_flat(res.field, (16, 16)).cpu().numpy()
+    assert np.all(np.abs(np.angle(gf / ref["field"])) <= PHASE_TOL)
+    if export:
+        _compare_paths(res, ref)
+
+
+def test_thin_wall_transmission_matches_oracle():
+    scene = scenes.thin_wall_scene()
+    cfg = Config(components={"los", "reflection", "transmission"}, max_depth=2, export_paths=True)
+    res = solve(scene, cfg, reference_frequency_hz=28.0e9)
+    ref = _oracle(scene, 28.0e9, components={"los", "reflection", "transmission"}, max_depth=2)
+    _compare_paths(res, ref)
+    assert int((res.paths.component_id == 5).sum()) > 0
+
+
+@pytest.mark.parametrize("coherent", [True, False])
+def test_small_city_all_components_matches_oracle(coherent):
+    scene, freq = scenes.small_city()
+    comps = {"los", "reflection", "diffraction", "transmission"}
+    cfg = Config(components=comps, max_depth=2, export_paths=True, coherent=coherent)
+    res = solve(scene, cfg, reference_frequency_hz=freq)
+    ref = _oracle(scene, freq, components=comps, max_depth=2, coherent=coherent)
+    _compare_paths(res, ref)
+    got = _grid_flat(res.path_gain, (8, 8)).cpu().numpy()
+    want = ref["path_gain"]
+    if not coherent:
+        # grid: the diffraction component power is the exact vector sum
+        want = want - ref["component_power"][2] + ref["diffraction_vector_power"]
+    assert np.all(_db(got, want) <= DB_TOL)
+
+
+def test_cell_mode_equals_row_mode():
+    scene, freq = scenes.small_city()
+    comps = {"los", "reflection", "diffraction", "transmission"}
+    a = solve(scene, Config(components=comps, max_depth=2), reference_frequency_hz=freq)
+    b = solve(scene, Config(components=comps, max_depth=2, export_paths=True), reference_frequency_hz=freq)
+    assert np.all(_db(a.path_gain.cpu().numpy(), b.path_gain.cpu().numpy()) <= 1e-3)
+    for name in a.component_power:
+        assert np.all(_db(a.component_power[name].cpu().numpy(), b.component_power[name].cpu().numpy()) <= 1e-3)
+
+
+def test_fp64_mode_matches_mixed():
+    scene, freq = scenes.small_city()
+    comps = {"los", "reflection", "diffraction", "transmission"}
+    a = solve(scene, Config(components=comps, max_depth=2), reference_frequency_hz=freq)
+    b = solve(scene, Config(components=comps, max_depth=2), reference_frequency_hz=freq, precision="fp64")
+    assert b.path_gain.dtype == torch.float64
+    assert np.all(_db(a.path_gain.cpu().numpy(), b.path_gain.cpu().numpy()) <= DB_TOL)
+
+
+def test_solve_is_deterministic():
+    scene, freq = scenes.small_city()
+    cfg = Config(components={"los", "reflection", "diffraction"}, max_depth=2)
+    a = solve(scene, cfg, reference_frequency_hz=freq).path_gain
+    b = solve(scene, cfg, reference_frequency_hz=freq).path_gain
+    assert torch.equal(a, b)

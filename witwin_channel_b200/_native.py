@@ -1,0 +1,223 @@
+"""ctypes binding of ``libwcb200.so`` (the C ABI in ``include/witwin_channel_b200.h``).
+
+The library is built in-tree (``witwin_channel_b200/csrc/libwcb200.so``).  There
+is no fallback: if it is missing or fails to load, every solve raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import torch
+
+_LIB_PATH = Path(__file__).resolve().parent / "csrc" / "libwcb200.so"
+
+WCB_OK = 0
+WCB_ERR_INVALID_ARGUMENT = 1
+WCB_ERR_CUDA = 2
+WCB_ERR_CAPACITY = 3
+WCB_ERR_BVH_DEPTH = 4
+WCB_ERR_NOT_SUPPORTED = 5
+WCB_ERR_DEVICE_STATUS = 6
+
+COMPONENT_LOS = 1
+COMPONENT_REFLECTION = 2
+COMPONENT_DIFFRACTION = 4
+COMPONENT_TRANSMISSION = 8
+
+PRECISION_MIXED = 0
+PRECISION_FP64 = 1
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_vp = ctypes.c_void_p
+
+
+class Materials(ctypes.Structure):
+    _fields_ = [
+        ("num_materials", ctypes.c_int32),
+        ("eps_r", _vp),
+        ("sigma_e", _vp),
+        ("mu_r", _vp),
+        ("gain", _vp),
+        ("thickness", _vp),
+        ("volumetric", _vp),
+        ("num_layers", ctypes.c_int32),
+        ("layer_offset", _vp),
+        ("layer_count", _vp),
+        ("layer_thickness", _vp),
+        ("layer_eps_r", _vp),
+        ("layer_sigma_e", _vp),
+        ("layer_mu_r", _vp),
+    ]
+
+
+class SolveDesc(ctypes.Structure):
+    _fields_ = [
+        ("num_tx", ctypes.c_int32),
+        ("tx_pos", _vp),
+        ("tx_power", _vp),
+        ("tx_pol", _vp),
+        ("rx_kind", ctypes.c_int32),
+        ("num_rx", ctypes.c_int32),
+        ("rx_pos", _vp),
+        ("grid_origin", ctypes.c_float * 3),
+        ("grid_x_axis", ctypes.c_float * 3),
+        ("grid_y_axis", ctypes.c_float * 3),
+        ("grid_rows", ctypes.c_int32),
+        ("grid_cols", ctypes.c_int32),
+        ("grid_spacing", ctypes.c_float * 2),
+        ("rx_pol", _vp),
+        ("rx_pol_stride", ctypes.c_int32),
+        ("num_freq", ctypes.c_int32),
+        ("frequency_hz", ctypes.POINTER(ctypes.c_double)),
+        ("components", ctypes.c_int32),
+        ("max_depth", ctypes.c_int32),
+        ("coherent", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("discovery_rays", ctypes.c_int32),
+    ]
+
+
+class Outputs(ctypes.Structure):
+    _fields_ = [
+        ("path_gain", _vp),
+        ("field", _vp),
+        ("comp_power", _vp),
+        ("comp_field", _vp),
+        ("diff_vec_power", _vp),
+        ("rows", _vp),
+        ("row_capacity", ctypes.c_int64),
+        ("row_count", _vp),
+        ("status", _vp),
+    ]
+
+
+class RowFields(ctypes.Structure):
+    _fields_ = [
+        ("path_length_m", _vp),
+        ("delay_s", _vp),
+        ("path_gain", _vp),
+        ("path_field", _vp),
+        ("coefficient", _vp),
+        ("field_xyz", _vp),
+        ("field_direction", _vp),
+        ("interaction_positions", _vp),
+        ("interaction_normals", _vp),
+        ("phase_rad", _vp),
+    ]
+
+
+ROW_BYTES = 48
+# wcb_row as int32 words: tx, rx, (component | depth << 16), seq[5], edge, length(f32 bits), reserved[2]
+ROW_WORDS = 12
+
+EXPORTED_SYMBOLS = (
+    "wcb_scene_create",
+    "wcb_scene_destroy",
+    "wcb_scene_info",
+    "wcb_scene_groups",
+    "wcb_scene_edges",
+    "wcb_solve_workspace_size",
+    "wcb_solve",
+    "wcb_rows_select_workspace_size",
+    "wcb_rows_select",
+    "wcb_rows_evaluate",
+    "wcb_rows_accumulate",
+    "wcb_field_free_space",
+    "wcb_field_reflection_sequence",
+    "wcb_field_project_complex3",
+    "wcb_build_info",
+    "wcb_launch_count",
+)
+
+_lib: ctypes.CDLL | None = None
+
+
+def library_path() -> Path:
+    return Path(os.environ.get("WITWIN_CHANNEL_B200_LIB", str(_LIB_PATH)))
+
+
+def load() -> ctypes.CDLL:
+    """Load the native library (once).  Raises if it is missing."""
+
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not path.exists():
+        raise RuntimeError(
+            f"witwin_channel_b200 native library not found at {path}; "
+            "build it with `python -c 'import __graft_entry__ as g; g.build()'` or `make -C witwin_channel_b200/csrc`"
+        )
+    lib = ctypes.CDLL(str(path))
+    lib.wcb_scene_create.argtypes = [_vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int32,
+                                     ctypes.c_int32, ctypes.c_double, _vp, ctypes.POINTER(_vp)]
+    lib.wcb_scene_destroy.argtypes = [_vp]
+    lib.wcb_scene_info.argtypes = [_vp, _i64p]
+    lib.wcb_scene_groups.argtypes = [_vp, _vp, _vp, _vp]
+    lib.wcb_scene_edges.argtypes = [_vp, _vp, _vp]
+    lib.wcb_solve_workspace_size.argtypes = [_vp, ctypes.POINTER(SolveDesc), _i64p]
+    lib.wcb_solve.argtypes = [_vp, ctypes.POINTER(SolveDesc), ctypes.POINTER(Materials), ctypes.POINTER(Outputs), _vp,
+                              ctypes.c_int64, _vp]
+    lib.wcb_rows_select_workspace_size.argtypes = [ctypes.c_int64, _i64p]
+    lib.wcb_rows_select.argtypes = [_vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, _vp, _i64p, _vp,
+                                    ctypes.c_int64, _vp]
+    lib.wcb_rows_evaluate.argtypes = [_vp, ctypes.POINTER(SolveDesc), ctypes.POINTER(Materials), ctypes.c_int32, _vp, _vp,
+                                      ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(RowFields), _vp]
+    lib.wcb_rows_accumulate.argtypes = [_vp, _vp, ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.POINTER(Outputs), _vp]
+    lib.wcb_field_free_space.argtypes = [ctypes.c_int64] + [_vp] * 5 + [ctypes.c_double] + [_vp] * 7 + [_vp]
+    lib.wcb_field_reflection_sequence.argtypes = [ctypes.c_int64, ctypes.c_int32] + [_vp] * 12 + [ctypes.c_double] + [_vp] * 7 + [_vp]
+    lib.wcb_field_project_complex3.argtypes = [ctypes.c_int64] + [_vp] * 5 + [_vp]
+    lib.wcb_build_info.argtypes = [ctypes.c_char_p, ctypes.c_int64]
+    lib.wcb_launch_count.restype = ctypes.c_int64
+    for name in EXPORTED_SYMBOLS:
+        if name != "wcb_launch_count":
+            getattr(lib, name).restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+_STATUS_TEXT = {
+    WCB_ERR_INVALID_ARGUMENT: "invalid argument",
+    WCB_ERR_CUDA: "CUDA error",
+    WCB_ERR_CAPACITY: "buffer capacity exceeded",
+    WCB_ERR_BVH_DEPTH: "BVH deeper than the traversal stack",
+    WCB_ERR_NOT_SUPPORTED: "not supported",
+    WCB_ERR_DEVICE_STATUS: "device reported a failure",
+}
+
+
+class NativeError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        super().__init__(f"{where} failed: {_STATUS_TEXT.get(status, 'status ' + str(status))}")
+        self.status = status
+
+
+def check(status: int, where: str) -> None:
+    if status != WCB_OK:
+        raise NativeError(status, where)
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def stream_handle(device: torch.device | None = None) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def launch_count() -> int:
+    return int(load().wcb_launch_count())
+
+
+def build_info() -> str:
+    buf = ctypes.create_string_buffer(256)
+    check(load().wcb_build_info(buf, 256), "wcb_build_info")
+    return buf.value.decode()

@@ -1,0 +1,291 @@
+"""Scene compile: logical scene -> device tables + native scene handle.
+
+Mirrors the reference's ``scene/compiler.py:1306-1450``: geometry is
+concatenated structure by structure (vertex offsets applied), each face keeps
+its structure, surface id (the structure's ``surface_id`` or its index) and
+material row; materials are evaluated at the solve frequency with PEC
+realised as ``sigma_e = 1e9`` (``materials.py:28-60``) and thin-sheet layer
+stacks as a CSR table (``materials.py:123-145``).  Geometry-only results (the
+LBVH, coplanar groups, edges) are cached per scene and reused across
+frequencies and material changes.
+"""
+
+from __future__ import annotations
+
+import weakref
+from dataclasses import dataclass, field
+from typing import Any
+
+import torch
+
+from . import _native
+from .constants import PEC_EFFECTIVE_SIGMA_E
+from .scene import ReceiverGrid, evaluate_material_value
+
+
+def _edge_policy(scene: Any) -> tuple[int, int, float]:
+    policy = getattr(scene, "metadata", {}).get("imported_edge_policy")
+    if policy is None:
+        return 1, 0, 0.7
+    boundary = getattr(policy, "boundary_edge_policy", "half_plane") or "half_plane"
+    mode = getattr(policy, "edge_selection_mode", "all_edges")
+    return int(boundary == "half_plane"), int(mode == "vertical_only"), float(getattr(policy, "vertical_ratio", 0.7))
+
+
+class NativeScene:
+    """Owns a ``wcb_scene`` handle and the device copies of the geometry."""
+
+    def __init__(self, vertices: torch.Tensor, faces: torch.Tensor, face_surface: torch.Tensor,
+                 face_structure: torch.Tensor, face_material: torch.Tensor, policy: tuple[int, int, float]):
+        lib = _native.load()
+        self.device = vertices.device
+        self.vertices = vertices.contiguous()
+        self.faces = faces.contiguous()
+        self.face_surface = face_surface.contiguous()
+        self.face_structure = face_structure.contiguous()
+        self.face_material = face_material.contiguous()
+        handle = _native._vp()
+        _native.check(
+            lib.wcb_scene_create(
+                _native.ptr(self.vertices), int(self.vertices.shape[0]), _native.ptr(self.faces),
+                int(self.faces.shape[0]), _native.ptr(self.face_surface), _native.ptr(self.face_structure),
+                _native.ptr(self.face_material), policy[0], policy[1], float(policy[2]),
+                _native.stream_handle(self.device), _native.ctypes.byref(handle),
+            ),
+            "wcb_scene_create",
+        )
+        self.handle = handle
+        counts = (_native.ctypes.c_int64 * 6)()
+        _native.check(lib.wcb_scene_info(handle, counts), "wcb_scene_info")
+        self.num_faces, self.num_groups, self.num_edges, self.bvh_depth, self.num_nodes, self.num_edges_total = (
+            int(c) for c in counts
+        )
+        self._finalizer = weakref.finalize(self, lib.wcb_scene_destroy, handle)
+
+    def groups(self) -> tuple[torch.Tensor, torch.Tensor]:
+        lib = _native.load()
+        fg = torch.empty(self.num_faces, dtype=torch.int32, device=self.device)
+        rep = torch.empty(self.num_groups, dtype=torch.int32, device=self.device)
+        _native.check(lib.wcb_scene_groups(self.handle, _native.ptr(fg), _native.ptr(rep),
+                                           _native.stream_handle(self.device)), "wcb_scene_groups")
+        return fg, rep
+
+    def edge_ids(self) -> torch.Tensor:
+        lib = _native.load()
+        out = torch.empty(self.num_edges, dtype=torch.int32, device=self.device)
+        _native.check(lib.wcb_scene_edges(self.handle, _native.ptr(out), _native.stream_handle(self.device)),
+                      "wcb_scene_edges")
+        return out
+
+
+@dataclass
+class MaterialTables:
+    """Per-frequency material arrays (NF, M) and layer arrays (NF, L)."""
+
+    eps_r: torch.Tensor
+    sigma_e: torch.Tensor
+    mu_r: torch.Tensor
+    gain: torch.Tensor
+    thickness: torch.Tensor
+    volumetric: torch.Tensor
+    layer_offset: torch.Tensor
+    layer_count: torch.Tensor
+    layer_thickness: torch.Tensor
+    layer_eps_r: torch.Tensor
+    layer_sigma_e: torch.Tensor
+    layer_mu_r: torch.Tensor
+
+    def as_struct(self) -> _native.Materials:
+        m = _native.Materials()
+        m.num_materials = int(self.eps_r.shape[1])
+        m.eps_r = _native.ptr(self.eps_r)
+        m.sigma_e = _native.ptr(self.sigma_e)
+        m.mu_r = _native.ptr(self.mu_r)
+        m.gain = _native.ptr(self.gain)
+        m.thickness = _native.ptr(self.thickness)
+        m.volumetric = _native.ptr(self.volumetric)
+        m.num_layers = int(self.layer_thickness.shape[1])
+        m.layer_offset = _native.ptr(self.layer_offset)
+        m.layer_count = _native.ptr(self.layer_count)
+        m.layer_thickness = _native.ptr(self.layer_thickness)
+        m.layer_eps_r = _native.ptr(self.layer_eps_r)
+        m.layer_sigma_e = _native.ptr(self.layer_sigma_e)
+        m.layer_mu_r = _native.ptr(self.layer_mu_r)
+        return m
+
+
+def _scalar(value: Any, frequency: float, *, keep_graph: bool) -> Any:
+    v = evaluate_material_value(value, frequency)
+    if isinstance(v, torch.Tensor):
+        return v.reshape(()) if keep_graph else float(v.detach())
+    return float(v)
+
+
+@dataclass
+class CompiledScene:
+    scene: Any
+    native: NativeScene
+    materials: list
+    face_material: torch.Tensor
+    num_vertices: int
+    structure_vertex_offsets: list = field(default_factory=list)
+
+    # ---- material tables ------------------------------------------------
+    def material_values(self, frequency: float, *, keep_graph: bool = False) -> dict[str, list]:
+        """Per-material scalars (floats, or 0-d tensors when ``keep_graph``)."""
+
+        out = {k: [] for k in ("eps_r", "sigma_e", "mu_r", "gain", "thickness")}
+        layers = []
+        for mat in self.materials:
+            pec = getattr(mat, "conductor_model", None) == "perfect"
+            stack = mat.stack()
+            rows = []
+            for layer in stack:
+                sig = PEC_EFFECTIVE_SIGMA_E if pec else _scalar(layer.sigma_e, frequency, keep_graph=keep_graph)
+                if pec and not isinstance(sig, torch.Tensor):
+                    sig = max(sig, PEC_EFFECTIVE_SIGMA_E)
+                rows.append((
+                    _scalar(layer.thickness_m, frequency, keep_graph=keep_graph),
+                    _scalar(layer.eps_r, frequency, keep_graph=keep_graph),
+                    sig,
+                    _scalar(layer.mu_r, frequency, keep_graph=keep_graph),
+                ))
+            layers.append(rows)
+            out["thickness"].append(rows[0][0])
+            out["eps_r"].append(rows[0][1])
+            out["sigma_e"].append(rows[0][2])
+            out["mu_r"].append(rows[0][3])
+            out["gain"].append(_scalar(mat.gain, frequency, keep_graph=keep_graph))
+        out["layers"] = layers
+        return out
+
+    def material_tables(self, frequencies: list[float], device: torch.device) -> MaterialTables:
+        per_f = [self.material_values(f) for f in frequencies]
+
+        def stack(name: str) -> torch.Tensor:
+            return torch.tensor([v[name] for v in per_f], dtype=torch.float32, device=device).reshape(len(frequencies), -1)
+
+        counts = [len(rows) for rows in per_f[0]["layers"]] if per_f else []
+        offsets = []
+        acc = 0
+        for c in counts:
+            offsets.append(acc)
+            acc += c
+        lt, le, ls, lm = [], [], [], []
+        for v in per_f:
+            flat = [row for rows in v["layers"] for row in rows]
+            lt.append([r[0] for r in flat])
+            le.append([r[1] for r in flat])
+            ls.append([r[2] for r in flat])
+            lm.append([r[3] for r in flat])
+        nf = len(frequencies)
+
+        def t2(x):
+            return torch.tensor(x, dtype=torch.float32, device=device).reshape(nf, -1)
+
+        vol = torch.tensor([int(getattr(m, "geometry_mode", "thin_sheet") == "volumetric") for m in self.materials],
+                           dtype=torch.int32, device=device)
+        return MaterialTables(
+            eps_r=stack("eps_r"), sigma_e=stack("sigma_e"), mu_r=stack("mu_r"), gain=stack("gain"),
+            thickness=stack("thickness"), volumetric=vol,
+            layer_offset=torch.tensor(offsets, dtype=torch.int32, device=device),
+            layer_count=torch.tensor(counts, dtype=torch.int32, device=device),
+            layer_thickness=t2(lt), layer_eps_r=t2(le), layer_sigma_e=t2(ls), layer_mu_r=t2(lm),
+        )
+
+
+_CACHE: "weakref.WeakKeyDictionary[Any, tuple[tuple, CompiledScene]]" = weakref.WeakKeyDictionary()
+
+
+def _geometry_token(scene: Any) -> tuple:
+    parts = []
+    for st in scene.structures:
+        v = st.vertices
+        parts.append((id(v), getattr(v, "_version", 0), tuple(v.shape), id(st.faces), id(st.material),
+                      st.surface_id))
+    parts.append(tuple(sorted((k, id(v)) for k, v in getattr(scene, "metadata", {}).items())))
+    return tuple(parts)
+
+
+def compile_scene(scene: Any, device: torch.device | None = None) -> CompiledScene:
+    """Compile (or fetch from the per-scene cache) the device scene."""
+
+    device = device or torch.device("cuda")
+    token = _geometry_token(scene)
+    try:
+        cached = _CACHE.get(scene)
+    except TypeError:
+        cached = None
+    if cached is not None and cached[0] == token:
+        return cached[1]
+    verts, faces, fsurf, fstruct, fmat = [], [], [], [], []
+    materials: list = []
+    mat_index: dict[int, int] = {}
+    offset = 0
+    offsets = []
+    for s_idx, st in enumerate(scene.structures):
+        v = st.vertices.detach().to(dtype=torch.float32).reshape(-1, 3)
+        f = st.faces.detach().to(dtype=torch.int64).reshape(-1, 3)
+        if f.numel() and (int(f.min()) < 0 or int(f.max()) >= v.shape[0]):
+            raise ValueError(f"structure {s_idx} has face indices outside its vertex table")
+        offsets.append(offset)
+        verts.append(v.cpu())
+        faces.append((f + offset).cpu())
+        nf = f.shape[0]
+        sid = st.surface_id if st.surface_id is not None else s_idx
+        fsurf.append(torch.full((nf,), int(sid), dtype=torch.int32))
+        fstruct.append(torch.full((nf,), s_idx, dtype=torch.int32))
+        key = id(st.material)
+        if key not in mat_index:
+            mat_index[key] = len(materials)
+            materials.append(st.material)
+        fmat.append(torch.full((nf,), mat_index[key], dtype=torch.int32))
+        offset += v.shape[0]
+    if verts:
+        V = torch.cat(verts).to(device)
+        Fc = torch.cat(faces).to(torch.int32).to(device)
+        fs = torch.cat(fsurf).to(device)
+        fst = torch.cat(fstruct).to(device)
+        fm = torch.cat(fmat).to(device)
+    else:
+        V = torch.zeros((0, 3), dtype=torch.float32, device=device)
+        Fc = torch.zeros((0, 3), dtype=torch.int32, device=device)
+        fs = fst = fm = torch.zeros((0,), dtype=torch.int32, device=device)
+    native = NativeScene(V, Fc, fs, fst, fm, _edge_policy(scene))
+    compiled = CompiledScene(scene=scene, native=native, materials=materials, face_material=fm,
+                             num_vertices=int(V.shape[0]), structure_vertex_offsets=offsets)
+    try:
+        _CACHE[scene] = (token, compiled)
+    except TypeError:
+        pass
+    return compiled
+
+
+def receiver_setup(scene: Any, device: torch.device) -> dict:
+    """Receiver description: a single grid stays analytic (points generated
+    on the fly in the kernels); anything else becomes explicit points."""
+
+    receivers = scene.receivers
+    if len(receivers) == 1 and isinstance(receivers[0], ReceiverGrid):
+        g = receivers[0]
+        pol = g.polarization.detach().to(device=device, dtype=torch.float32).reshape(1, 3).contiguous()
+        return {
+            "kind": "grid", "grid": g, "count": g.count, "shape": g.shape, "pol": pol, "pol_stride": 0,
+            "positions": None,
+        }
+    pos, pols = [], []
+    for r in receivers:
+        if isinstance(r, ReceiverGrid):
+            pts = r.points()
+        else:
+            pts = r.position.detach().reshape(1, 3).to(torch.float32).cpu()
+        pos.append(pts)
+        pols.append(r.polarization.detach().to(torch.float32).reshape(1, 3).cpu().expand(pts.shape[0], 3))
+    if pos:
+        P = torch.cat(pos).to(device).contiguous()
+        Q = torch.cat(pols).to(device).contiguous()
+    else:
+        P = torch.zeros((0, 3), dtype=torch.float32, device=device)
+        Q = torch.zeros((1, 3), dtype=torch.float32, device=device)
+    return {"kind": "point", "grid": None, "count": int(P.shape[0]), "shape": None, "pol": Q,
+            "pol_stride": 3 if P.shape[0] > 0 else 0, "positions": P}

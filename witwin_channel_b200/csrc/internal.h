@@ -1,0 +1,49 @@
+// Library-internal declarations shared by the CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <vector>
+
+#include "scene.cuh"
+#include "../../include/witwin_channel_b200.h"
+
+namespace wcb {
+
+struct SceneHandle {
+    SceneDev dev;
+    std::vector<void*> owned;
+    int* edge_ids = nullptr;     // (E) device, reference edge id of each selected edge
+    int* edge_slot = nullptr;    // (edges total) device, selected index of each reference edge or -1
+    std::vector<int> group_rep_host;
+    std::vector<int> face_group_host;
+    int num_edges_total = 0;
+    int num_nodes = 0;
+};
+
+int scene_create(const float* vertices, int64_t nv, const int32_t* faces, int64_t nf, const int32_t* surface,
+                 const int32_t* structure, const int32_t* material, int boundary_half_plane, int vertical_only,
+                 double vertical_ratio, cudaStream_t stream, SceneHandle** out);
+void scene_destroy(SceneHandle* h);
+
+int rows_select_workspace(int64_t n, int64_t* bytes);
+int rows_select(const void* rows, int64_t n, int width, int64_t max_paths, int scope, int64_t* selected,
+                int64_t* num_selected, void* ws, int64_t ws_bytes, cudaStream_t stream);
+int rows_evaluate(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m, int fi, const void* rows,
+                  const int64_t* selected, int64_t count, int width, const wcb_row_fields* out, cudaStream_t stream);
+int rows_accumulate(const void* rows, const int64_t* selected, int64_t n, const float* path_gain, const float* path_field,
+                    const float* field_xyz, const float* tx_power, int num_tx, int num_rx, int coherent,
+                    const wcb_outputs* out, cudaStream_t stream);
+int field_free_space(int64_t n, const float* s, const float* t, const float* pw, const float* tp, const float* rp, double f,
+                     float* fv, float* c, float* pf, float* pg, float* pl, float* dl, float* dr, cudaStream_t stream);
+int field_reflection(int64_t n, int depth, const float* s, const float* t, const float* pos, const float* nrm, const float* pw,
+                     const float* tp, const float* rp, const float* eps, const float* sig, const float* mu, const float* gain,
+                     const float* th, double f, float* fv, float* c, float* pf, float* pg, float* pl, float* dl, float* dr,
+                     cudaStream_t stream);
+int field_project(int64_t n, const float* fv, const float* dir, const float* rp, float* c, float* pg, cudaStream_t stream);
+
+extern std::atomic<long long> g_launch_count;
+inline void note_launch(int n = 1) { g_launch_count.fetch_add(n, std::memory_order_relaxed); }
+
+}  // namespace wcb

@@ -1,0 +1,671 @@
+// Path records: canonical order, identity dedup, max_paths, per-row field
+// evaluation from the frozen topology, and deterministic per-cell sums.
+//
+// Canonical order and selection follow
+// native/channel/kernels/evaluated_paths.cu:76-470 and :669-710: the key is
+// (rx, tx, depth, component, sequence[0..w-1], primitive, edge); rows with
+// the same identity (tx, rx, per-slot event type and object id) keep the
+// shortest (first on ties) and a NaN length drops the group; max_paths keeps
+// a global prefix or the first max_paths rows of each (rx, tx) pair.  Here the
+// key is packed into four 64-bit words and sorted with four stable radix
+// passes (least significant word first).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+
+#include "em.cuh"
+#include "internal.h"
+#include "paths.cuh"
+#include "solve.h"
+#include "utd.cuh"
+
+namespace wcb {
+
+namespace {
+
+constexpr int kB = 256;
+
+WCB_D unsigned long long field18(int v) { return static_cast<unsigned long long>((v + 1) & 0x3ffff); }
+
+WCB_D int row_prim(const RowRec& r) { return (r.component == 1 || r.component == 5) ? r.seq[0] : -1; }
+
+__global__ void k_row_key(long long n, const RowRec* rows, const int* order, int word, unsigned long long* keys) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const RowRec r = rows[order ? order[i] : i];
+    unsigned long long k = 0;
+    if (word == 0) {
+        k = field18(r.edge);
+    } else if (word == 1) {
+        k = (field18(r.seq[3]) << 36) | (field18(r.seq[4]) << 18) | field18(row_prim(r));
+    } else if (word == 2) {
+        k = (field18(r.seq[0]) << 36) | (field18(r.seq[1]) << 18) | field18(r.seq[2]);
+    } else {
+        k = (static_cast<unsigned long long>(r.rx) << 17) | (static_cast<unsigned long long>(r.tx & 0x7ff) << 6) |
+            (static_cast<unsigned long long>(r.depth & 7) << 3) | static_cast<unsigned long long>(r.component & 7);
+    }
+    keys[i] = k;
+}
+
+__global__ void k_iota(long long n, int* v) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) v[i] = int(i);
+}
+
+WCB_D int event_type(int component, int depth, int slot) {
+    if (component == 1 && slot < depth) return 1;
+    if (component == 2 && depth > 0 && slot == 0) return 2;
+    if (component == 5 && slot < depth) return 4;
+    return 0;
+}
+
+WCB_D bool same_identity(const RowRec& a, const RowRec& b, int width) {
+    if (a.tx != b.tx || a.rx != b.rx) return false;
+    for (int s = 0; s < width; ++s) {
+        const int ta = event_type(a.component, a.depth, s);
+        const int tb = event_type(b.component, b.depth, s);
+        if (ta != tb) return false;
+        const int oa = ta == 0 ? -1 : (a.component == 2 && s == 0 ? a.edge : a.seq[s]);
+        const int ob = tb == 0 ? -1 : (b.component == 2 && s == 0 ? b.edge : b.seq[s]);
+        if (oa != ob) return false;
+    }
+    return true;
+}
+
+__global__ void k_group_start(long long n, const RowRec* rows, const int* order, int width, int* start) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    start[i] = (i == 0 || !same_identity(rows[order[i - 1]], rows[order[i]], width)) ? 1 : 0;
+}
+
+__global__ void k_winner(long long n, const RowRec* rows, const int* order, const int* start, int* keep) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    keep[i] = 0;
+    if (!start[i]) return;
+    float best = INFINITY;
+    bool has_nan = false;
+    long long e = i;
+    while (e < n && (e == i || !start[e])) {
+        const float v = rows[order[e]].length;
+        if (isnan(v)) { has_nan = true; break; }
+        if (v < best) best = v;
+        ++e;
+    }
+    if (has_nan) return;
+    for (long long q = i; q < e; ++q) {
+        if (rows[order[q]].length == best) { keep[q] = 1; return; }
+    }
+}
+
+// per (rx, tx) pair limit on the kept rows (already compacted, canonical)
+__global__ void k_pair_limit(long long n, const RowRec* rows, const long long* kept, long long max_paths, int* keep2) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const RowRec r = rows[kept[i]];
+    const bool pair_start = i == 0 || rows[kept[i - 1]].rx != r.rx || rows[kept[i - 1]].tx != r.tx;
+    if (!pair_start) return;
+    long long e = i;
+    while (e < n) {
+        const RowRec q = rows[kept[e]];
+        if (q.rx != r.rx || q.tx != r.tx) break;
+        keep2[e] = (e - i) < max_paths ? 1 : 0;
+        ++e;
+    }
+}
+
+__global__ void k_gather_selected(long long n, const int* order, const int* keep, const int* scan, long long* out) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (keep[i]) out[scan[i] - 1] = order[i];
+}
+
+__global__ void k_gather_selected64(long long n, const long long* in, const int* keep, const int* scan, long long* out) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (keep[i]) out[scan[i] - 1] = in[i];
+}
+
+size_t al(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct SelectLayout {
+    size_t keys, keys2, idx, idx2, start, keep, scan, tmp, tmp_bytes, kept, total;
+};
+
+SelectLayout select_layout(long long n) {
+    SelectLayout L;
+    size_t o = 0;
+    auto take = [&](size_t b) { size_t a = o; o = al(o + b); return a; };
+    const size_t m = size_t(std::max<long long>(n, 1));
+    L.keys = take(m * 8);
+    L.keys2 = take(m * 8);
+    L.idx = take(m * 4);
+    L.idx2 = take(m * 4);
+    L.start = take(m * 4);
+    L.keep = take(m * 4);
+    L.scan = take(m * 4);
+    size_t a = 0, b = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, a, (unsigned long long*)nullptr, (unsigned long long*)nullptr, (int*)nullptr,
+                                    (int*)nullptr, int(m), 0, 64);
+    cub::DeviceScan::InclusiveSum(nullptr, b, (int*)nullptr, (int*)nullptr, int(m));
+    L.tmp_bytes = std::max(a, b);
+    L.tmp = take(L.tmp_bytes);
+    L.kept = take(m * 8);
+    L.total = o;
+    return L;
+}
+
+}  // namespace
+
+int rows_select_workspace(int64_t n, int64_t* bytes) {
+    *bytes = int64_t(select_layout(n).total);
+    return 0;
+}
+
+int rows_select(const void* rows_v, int64_t n, int width, int64_t max_paths, int scope, int64_t* selected,
+                int64_t* num_selected, void* ws, int64_t ws_bytes, cudaStream_t stream) {
+    if (n < 0 || n > INT_MAX - 1) return 1;
+    const SelectLayout L = select_layout(n);
+    if (ws_bytes < int64_t(L.total)) return 3;
+    *num_selected = 0;
+    if (n == 0) return 0;
+    const RowRec* rows = static_cast<const RowRec*>(rows_v);
+    char* b = static_cast<char*>(ws);
+    auto* keys = reinterpret_cast<unsigned long long*>(b + L.keys);
+    auto* keys2 = reinterpret_cast<unsigned long long*>(b + L.keys2);
+    int* idx = reinterpret_cast<int*>(b + L.idx);
+    int* idx2 = reinterpret_cast<int*>(b + L.idx2);
+    int* start = reinterpret_cast<int*>(b + L.start);
+    int* keep = reinterpret_cast<int*>(b + L.keep);
+    int* scan = reinterpret_cast<int*>(b + L.scan);
+    void* tmp = b + L.tmp;
+    long long* kept = reinterpret_cast<long long*>(b + L.kept);
+    const int grid = int((n + kB - 1) / kB);
+    k_iota<<<grid, kB, 0, stream>>>(n, idx);
+    note_launch();
+    const int end_bits[4] = {18, 54, 54, 38};
+    for (int w = 0; w < 4; ++w) {
+        k_row_key<<<grid, kB, 0, stream>>>(n, rows, idx, w, keys);
+        size_t tb = L.tmp_bytes;
+        cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, idx, idx2, int(n), 0, end_bits[w], stream);
+        std::swap(idx, idx2);
+        note_launch(2);
+    }
+    k_group_start<<<grid, kB, 0, stream>>>(n, rows, idx, width, start);
+    k_winner<<<grid, kB, 0, stream>>>(n, rows, idx, start, keep);
+    size_t tb = L.tmp_bytes;
+    cub::DeviceScan::InclusiveSum(tmp, tb, keep, scan, int(n), stream);
+    k_gather_selected<<<grid, kB, 0, stream>>>(n, idx, keep, scan, kept);
+    note_launch(4);
+    int count = 0;
+    cudaMemcpyAsync(&count, scan + n - 1, 4, cudaMemcpyDeviceToHost, stream);
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return 2;
+    long long final_count = count;
+    if (max_paths >= 0 && scope == 0) {
+        final_count = std::min<long long>(count, max_paths);
+        cudaMemcpyAsync(selected, kept, size_t(final_count) * 8, cudaMemcpyDeviceToDevice, stream);
+    } else if (max_paths >= 0 && scope == 1 && count > 0) {
+        const int g2 = int((count + kB - 1) / kB);
+        cudaMemsetAsync(keep, 0, size_t(count) * 4, stream);
+        k_pair_limit<<<g2, kB, 0, stream>>>(count, rows, kept, max_paths, keep);
+        tb = L.tmp_bytes;
+        cub::DeviceScan::InclusiveSum(tmp, tb, keep, scan, int(count), stream);
+        k_gather_selected64<<<g2, kB, 0, stream>>>(count, kept, keep, scan, reinterpret_cast<long long*>(selected));
+        note_launch(3);
+        int c2 = 0;
+        cudaMemcpyAsync(&c2, scan + count - 1, 4, cudaMemcpyDeviceToHost, stream);
+        if (cudaStreamSynchronize(stream) != cudaSuccess) return 2;
+        final_count = c2;
+    } else {
+        cudaMemcpyAsync(selected, kept, size_t(count) * 8, cudaMemcpyDeviceToDevice, stream);
+    }
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return 2;
+    *num_selected = final_count;
+    return 0;
+}
+
+// ------------------------------------------------------------ evaluation
+namespace {
+
+struct EvalParams {
+    SceneDev sc;
+    const int* edge_slot;  // reference edge id -> selected edge index
+    const float* tx_pos;
+    const float* tx_power;
+    const float* tx_pol;
+    int rx_kind;
+    const float* rx_pos;
+    float grid_origin[3], grid_x[3], grid_y[3];
+    int grid_rows, grid_cols;
+    float grid_spacing[2];
+    const float* rx_pol;
+    int rx_pol_stride;
+    double freq;
+    double k;
+    int num_materials;
+    const float* eps_r;
+    const float* sigma_e;
+    const float* mu_r;
+    const float* gain;
+    const float* thickness;
+    int num_layers;
+    const int* layer_offset;
+    const int* layer_count;
+    const float* layer_thickness;
+    const float* layer_eps_r;
+    const float* layer_sigma_e;
+    const float* layer_mu_r;
+    const RowRec* rows;
+    const long long* selected;
+    long long count;
+    int width;
+    wcb_row_fields out;
+};
+
+WCB_D V3<double> eval_rx(const EvalParams& p, int r) {
+    if (p.rx_kind == 1) {
+        const int row = r / p.grid_cols;
+        const int col = r - row * p.grid_cols;
+        const float u = __fmul_rn(float(row), p.grid_spacing[0]);
+        const float v = __fmul_rn(float(col), p.grid_spacing[1]);
+        return v3<double>(__fadd_rn(__fadd_rn(p.grid_origin[0], __fmul_rn(p.grid_x[0], u)), __fmul_rn(p.grid_y[0], v)),
+                          __fadd_rn(__fadd_rn(p.grid_origin[1], __fmul_rn(p.grid_x[1], u)), __fmul_rn(p.grid_y[1], v)),
+                          __fadd_rn(__fadd_rn(p.grid_origin[2], __fmul_rn(p.grid_x[2], u)), __fmul_rn(p.grid_y[2], v)));
+    }
+    return v3<double>(p.rx_pos[3 * r], p.rx_pos[3 * r + 1], p.rx_pos[3 * r + 2]);
+}
+
+WCB_D Slab<float> slab_of(const EvalParams& p, int face) {
+    const int m = p.sc.face_material[face];
+    return Slab<float>{p.eps_r[m], p.sigma_e[m], p.mu_r[m], p.gain[m], p.thickness[m]};
+}
+
+WCB_D void store_c(float* dst, long long i, Cx<float> v) {
+    if (dst) { dst[2 * i] = v.re; dst[2 * i + 1] = v.im; }
+}
+
+__global__ void k_eval_rows(EvalParams p) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= p.count) return;
+    const RowRec row = p.rows[p.selected[i]];
+    const int t = row.tx, r = row.rx;
+    const SceneDev& sc = p.sc;
+    const V3<double> S = v3<double>(p.tx_pos[3 * t], p.tx_pos[3 * t + 1], p.tx_pos[3 * t + 2]);
+    const V3<double> R = eval_rx(p, r);
+    const V3<float> Sf = cast3<float>(S), Rf = cast3<float>(R);
+    const V3<float> tx_pol = v3<float>(p.tx_pol[3 * t], p.tx_pol[3 * t + 1], p.tx_pol[3 * t + 2]);
+    const float* rp = p.rx_pol + (long long)r * p.rx_pol_stride;
+    const V3<float> rx_pol = v3<float>(rp[0], rp[1], rp[2]);
+    const float P = fmaxf(p.tx_power[t], 0.0f);
+    const float sq = sqrtf(P);
+    C3<float> unit_field;
+    Cx<float> coef;
+    V3<float> dir;
+    double length = 0.0;
+    V3<double> hits[kMaxDepth];
+    V3<float> normals[kMaxDepth];
+    int nh = 0;
+    Cx<float> path_field;
+    float path_gain;
+    const int W = p.width;
+    if (row.component == 0) {
+        length = wcb::length(R - S);
+        const PathEval<float> ev = eval_free_space(Sf, Rf, tx_pol, rx_pol, p.k, length);
+        unit_field = ev.field;
+        coef = ev.coefficient;
+        dir = ev.direction;
+        path_field = coef * sq;
+        path_gain = cabs2(path_field);
+    } else if (row.component == 1) {
+        const int d = row.depth;
+        double planes[4 * kMaxDepth], images[3 * kMaxDepth];
+        V3<double> pp = S;
+        for (int k = 0; k < d; ++k) {
+            const int g = sc.face_group[row.seq[k]];
+            const double* pl = sc.group_plane + 4 * g;
+            for (int q = 0; q < 4; ++q) planes[4 * k + q] = pl[q];
+            const V3<double> n = v3(pl[0], pl[1], pl[2]);
+            pp = pp - n * (2.0 * (dot(pp, n) - pl[3]));
+            images[3 * k] = pp.x; images[3 * k + 1] = pp.y; images[3 * k + 2] = pp.z;
+        }
+        if (!back_project(R, planes, images, d, hits)) {
+            for (int k = 0; k < d; ++k) hits[k] = v3(nan(""), nan(""), nan(""));
+        }
+        nh = d;
+        length = wcb::length(R - pp);
+        const float wl = float(kC0 / p.freq);
+        V3<float> prev = Sf;
+        V3<float> incident = safe_normalize(cast3<float>(hits[0]) - prev, v3(0.f, 0.f, 1.f));
+        C3<float> value = c3_from_real(transverse(incident, tx_pol));
+        V3<float> outgoing = incident;
+        for (int k = 0; k < d; ++k) {
+            const V3<float> hit = cast3<float>(hits[k]);
+            incident = safe_normalize(hit - prev, outgoing);
+            const float* nf = sc.face_normal + 3 * row.seq[k];
+            normals[k] = v3(nf[0], nf[1], nf[2]);
+            reflect_bounce(value, outgoing, incident, normals[k], slab_of(p, row.seq[k]), p.freq, wl);
+            prev = hit;
+        }
+        dir = safe_normalize(Rf - prev, outgoing);
+        const float amp = 1.0f / (2.0f * float(p.k) * float(fmax(length, kUtdEps)));
+        value = c3_scale(value, phasor_neg_kd<float>(p.k, length) * amp);
+        unit_field = value;
+        coef = project_receiver(value, dir, rx_pol);
+        path_field = coef * sq;
+        path_gain = cabs2(path_field);
+    } else if (row.component == 5) {
+        const int d = row.depth;
+        length = wcb::length(R - S);
+        dir = safe_normalize(Rf - Sf, v3(0.f, 0.f, 1.f));
+        C3<float> value = c3_from_real(transverse(dir, tx_pol));
+        float shorten = 0.0f;
+        const LayerTable<float> lt{p.layer_offset, p.layer_count, p.layer_thickness, p.layer_eps_r, p.layer_sigma_e, p.layer_mu_r};
+        const V3<double> seg = R - S;
+        for (int k = 0; k < d; ++k) {
+            const int f = row.seq[k];
+            const float* nf = sc.face_normal + 3 * f;
+            normals[k] = v3(nf[0], nf[1], nf[2]);
+            const double* pl = sc.face_plane + 4 * f;
+            const V3<double> n = v3(pl[0], pl[1], pl[2]);
+            const double den = dot(seg, n);
+            const double tt = den != 0.0 ? (pl[3] - dot(S, n)) / den : 0.0;
+            hits[k] = S + seg * tt;
+            transmit_wall(value, shorten, dir, normals[k], sc.face_material[f], lt, p.freq);
+        }
+        nh = d;
+        const float amp = 1.0f / (2.0f * float(p.k) * float(fmax(length, kUtdEps)));
+        value = c3_scale(value, phasor_neg_kd<float>(p.k, length - double(shorten)) * amp);
+        unit_field = value;
+        coef = project_receiver(value, dir, rx_pol);
+        path_field = coef * sq;
+        path_gain = cabs2(path_field);
+    } else {
+        const int slot = p.edge_slot[row.edge];
+        const EdgeDev& ed = sc.edges[slot];
+        const DiffractionResult<float> res = utd_field<float>(ed, S, R, tx_pol, slab_of(p, ed.mat_face0), slab_of(p, ed.mat_face1), p.freq);
+        length = res.length;
+        const V3<double> q = v3(res.q[0], res.q[1], res.q[2]);
+        hits[0] = q;
+        normals[0] = v3(0.f, 0.f, 0.f);
+        nh = 1;
+        dir = safe_normalize(cast3<float>(R - q), v3(0.f, 0.f, 1.f));
+        const C3<float> powered = c3_scale(res.field, cx(sq, 0.0f));
+        path_field = project_receiver(powered, dir, rx_pol);
+        path_gain = cabs2(path_field);
+        const float amp = sqrtf(fmaxf(P, 1e-30f));
+        unit_field = c3_scale(powered, cx(1.0f / amp, 0.0f));
+        coef = path_field * (1.0f / amp);
+    }
+    const wcb_row_fields& o = p.out;
+    if (o.path_length_m) o.path_length_m[i] = float(length);
+    if (o.delay_s) o.delay_s[i] = float(length / kC0);
+    if (o.path_gain) o.path_gain[i] = path_gain;
+    store_c(o.path_field, i, path_field);
+    store_c(o.coefficient, i, coef);
+    if (o.field_xyz) {
+        store_c(o.field_xyz, 3 * i + 0, unit_field.x);
+        store_c(o.field_xyz, 3 * i + 1, unit_field.y);
+        store_c(o.field_xyz, 3 * i + 2, unit_field.z);
+    }
+    if (o.field_direction) {
+        o.field_direction[3 * i] = dir.x;
+        o.field_direction[3 * i + 1] = dir.y;
+        o.field_direction[3 * i + 2] = dir.z;
+    }
+    for (int k = 0; k < W; ++k) {
+        const bool on = k < nh;
+        if (o.interaction_positions) {
+            float* d = o.interaction_positions + (i * W + k) * 3;
+            d[0] = on ? float(hits[k].x) : 0.f;
+            d[1] = on ? float(hits[k].y) : 0.f;
+            d[2] = on ? float(hits[k].z) : 0.f;
+        }
+        if (o.interaction_normals) {
+            float* d = o.interaction_normals + (i * W + k) * 3;
+            d[0] = on ? normals[k].x : 0.f;
+            d[1] = on ? normals[k].y : 0.f;
+            d[2] = on ? normals[k].z : 0.f;
+        }
+    }
+    if (o.phase_rad) {
+        float ph = -atan2f(path_field.im, path_field.re);
+        const float tp = float(kTwoPi);
+        ph = fmodf(ph, tp);
+        if (ph < 0.0f) ph += tp;
+        o.phase_rad[i] = ph;
+    }
+}
+
+// deterministic per-cell accumulation over canonical rows
+__global__ void k_accumulate_rows(const RowRec* rows, const long long* sel, long long n, const float* path_gain,
+                                  const float* path_field, const float* field_xyz, const float* tx_power, int num_tx,
+                                  int num_rx, int coherent,
+                                  float* out_pg, float* out_field, float* out_cp, float* out_cf, float* out_dv) {
+    const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long cells = (long long)num_tx * num_rx;
+    if (cell >= cells) return;
+    const int t = int(cell / num_rx);
+    const int r = int(cell - (long long)t * num_rx);
+    // rows are sorted by (rx, tx): lower bound of (r, t)
+    long long lo = 0, hi = n;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        const RowRec m = rows[sel[mid]];
+        if (m.rx < r || (m.rx == r && m.tx < t)) lo = mid + 1;
+        else hi = mid;
+    }
+    Cx<float> slot[4] = {cx(0.f, 0.f), cx(0.f, 0.f), cx(0.f, 0.f), cx(0.f, 0.f)};
+    float gain[4] = {0.f, 0.f, 0.f, 0.f};
+    Cx<float> dv[3] = {cx(0.f, 0.f), cx(0.f, 0.f), cx(0.f, 0.f)};
+    const float amp = tx_power ? sqrtf(fmaxf(tx_power[t], 0.f)) : 1.f;
+    for (long long q = lo; q < n; ++q) {
+        const RowRec m = rows[sel[q]];
+        if (m.rx != r || m.tx != t) break;
+        const int s = m.component == 0 ? 0 : m.component == 1 ? 1 : m.component == 2 ? 2 : m.component == 5 ? 3 : -1;
+        if (s < 0) continue;
+        const Cx<float> pf = cx(path_field[2 * q], path_field[2 * q + 1]);
+        slot[s] = slot[s] + pf;
+        gain[s] += path_gain[q];
+        if (s == 2 && field_xyz) {
+            // field_xyz is unit excitation; the exact vector sum uses the powered field
+            dv[0] = dv[0] + cx(field_xyz[6 * q + 0], field_xyz[6 * q + 1]) * amp;
+            dv[1] = dv[1] + cx(field_xyz[6 * q + 2], field_xyz[6 * q + 3]) * amp;
+            dv[2] = dv[2] + cx(field_xyz[6 * q + 4], field_xyz[6 * q + 5]) * amp;
+        }
+    }
+    Cx<float> total = cx(0.f, 0.f);
+    float gsum = 0.f;
+    for (int s = 0; s < 4; ++s) {
+        total = total + slot[s];
+        gsum += gain[s];
+    }
+    if (out_pg) out_pg[cell] = coherent ? cabs2(total) : gsum;
+    if (out_field) {
+        out_field[2 * cell] = coherent ? total.re : sqrtf(fmaxf(gsum, 0.f));
+        out_field[2 * cell + 1] = coherent ? total.im : 0.f;
+    }
+    for (int s = 0; s < 6; ++s) {
+        const long long o = s * cells + cell;
+        const Cx<float> v = s < 4 ? slot[s] : cx(0.f, 0.f);
+        if (out_cp) out_cp[o] = s < 4 ? (coherent ? cabs2(v) : gain[s]) : 0.f;
+        if (out_cf) { out_cf[2 * o] = v.re; out_cf[2 * o + 1] = v.im; }
+    }
+    if (out_dv) out_dv[cell] = cabs2(dv[0]) + cabs2(dv[1]) + cabs2(dv[2]);
+}
+
+// ------------------------------------------------------------ field operators
+__global__ void k_field_free_space(long long n, const float* src, const float* tgt, const float* pw, const float* tpol,
+                                   const float* rpol, double freq, float* fv, float* coef, float* pf, float* pg,
+                                   float* plen, float* delay, float* dirout) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const V3<double> S = v3<double>(src[3 * i], src[3 * i + 1], src[3 * i + 2]);
+    const V3<double> R = v3<double>(tgt[3 * i], tgt[3 * i + 1], tgt[3 * i + 2]);
+    const double k = kTwoPi * freq / kC0;
+    const double dist = length(R - S);
+    const PathEval<float> ev = eval_free_space(cast3<float>(S), cast3<float>(R), v3(tpol[3 * i], tpol[3 * i + 1], tpol[3 * i + 2]),
+                                               v3(rpol[3 * i], rpol[3 * i + 1], rpol[3 * i + 2]), k, dist);
+    const float sq = sqrtf(fmaxf(pw[i], 0.f));
+    const Cx<float> p = ev.coefficient * sq;
+    store_c(fv, 3 * i, ev.field.x);
+    store_c(fv, 3 * i + 1, ev.field.y);
+    store_c(fv, 3 * i + 2, ev.field.z);
+    store_c(coef, i, ev.coefficient);
+    store_c(pf, i, p);
+    if (pg) pg[i] = cabs2(p);
+    if (plen) plen[i] = float(dist);
+    if (delay) delay[i] = float(dist / kC0);
+    if (dirout) { dirout[3 * i] = ev.direction.x; dirout[3 * i + 1] = ev.direction.y; dirout[3 * i + 2] = ev.direction.z; }
+}
+
+__global__ void k_field_reflection(long long n, int depth, const float* src, const float* tgt, const float* pos,
+                                   const float* nrm, const float* pw, const float* tpol, const float* rpol,
+                                   const float* eps, const float* sig, const float* mu, const float* gain,
+                                   const float* th, double freq, float* fv, float* coef, float* pf, float* pg,
+                                   float* plen, float* delay, float* dirout) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const V3<float> S = v3(src[3 * i], src[3 * i + 1], src[3 * i + 2]);
+    const V3<float> R = v3(tgt[3 * i], tgt[3 * i + 1], tgt[3 * i + 2]);
+    const V3<float> tx_pol = v3(tpol[3 * i], tpol[3 * i + 1], tpol[3 * i + 2]);
+    const V3<float> rx_pol = v3(rpol[3 * i], rpol[3 * i + 1], rpol[3 * i + 2]);
+    const double k = kTwoPi * freq / kC0;
+    const float wl = float(kC0 / freq);
+    auto hit = [&](int b) { const float* h = pos + (i * depth + b) * 3; return v3(h[0], h[1], h[2]); };
+    V3<float> prev = S;
+    V3<float> incident = safe_normalize(hit(0) - prev, v3(0.f, 0.f, 1.f));
+    C3<float> value = c3_from_real(transverse(incident, tx_pol));
+    V3<float> outgoing = incident;
+    double total = 0.0;
+    V3<double> prevd = cast3<double>(S);
+    for (int b = 0; b < depth; ++b) {
+        const V3<float> h = hit(b);
+        incident = safe_normalize(h - prev, outgoing);
+        total += length(cast3<double>(h) - prevd);
+        const float* nn = nrm + (i * depth + b) * 3;
+        const long long s = i * depth + b;
+        reflect_bounce(value, outgoing, incident, v3(nn[0], nn[1], nn[2]), Slab<float>{eps[s], sig[s], mu[s], gain[s], th[s]}, freq, wl);
+        prev = h;
+        prevd = cast3<double>(h);
+    }
+    const V3<float> fdir = safe_normalize(R - prev, outgoing);
+    total += length(cast3<double>(R) - prevd);
+    const float amp = 1.0f / (2.0f * float(k) * float(fmax(total, kUtdEps)));
+    value = c3_scale(value, phasor_neg_kd<float>(k, total) * amp);
+    const Cx<float> c = project_receiver(value, fdir, rx_pol);
+    const Cx<float> p = c * sqrtf(fmaxf(pw[i], 0.f));
+    store_c(fv, 3 * i, value.x);
+    store_c(fv, 3 * i + 1, value.y);
+    store_c(fv, 3 * i + 2, value.z);
+    store_c(coef, i, c);
+    store_c(pf, i, p);
+    if (pg) pg[i] = cabs2(p);
+    if (plen) plen[i] = float(total);
+    if (delay) delay[i] = float(total / kC0);
+    if (dirout) { dirout[3 * i] = fdir.x; dirout[3 * i + 1] = fdir.y; dirout[3 * i + 2] = fdir.z; }
+}
+
+__global__ void k_field_project(long long n, const float* fv, const float* dir, const float* rpol, float* coef, float* pg) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const C3<float> v = {cx(fv[6 * i], fv[6 * i + 1]), cx(fv[6 * i + 2], fv[6 * i + 3]), cx(fv[6 * i + 4], fv[6 * i + 5])};
+    const Cx<float> c = project_receiver(v, v3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]), v3(rpol[3 * i], rpol[3 * i + 1], rpol[3 * i + 2]));
+    store_c(coef, i, c);
+    if (pg) pg[i] = cabs2(c);
+}
+
+}  // namespace
+
+int rows_evaluate(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m, int fi, const void* rows,
+                  const int64_t* selected, int64_t count, int width, const wcb_row_fields* out, cudaStream_t stream) {
+    if (count <= 0) return 0;
+    if (fi < 0 || fi >= d->num_freq) return 1;
+    EvalParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.sc = h->dev;
+    p.edge_slot = h->edge_slot;
+    p.tx_pos = d->tx_pos;
+    p.tx_power = d->tx_power;
+    p.tx_pol = d->tx_pol;
+    p.rx_kind = d->rx_kind;
+    p.rx_pos = d->rx_pos;
+    for (int k = 0; k < 3; ++k) {
+        p.grid_origin[k] = d->grid_origin[k];
+        p.grid_x[k] = d->grid_x_axis[k];
+        p.grid_y[k] = d->grid_y_axis[k];
+    }
+    p.grid_rows = d->grid_rows;
+    p.grid_cols = d->grid_cols;
+    p.grid_spacing[0] = d->grid_spacing[0];
+    p.grid_spacing[1] = d->grid_spacing[1];
+    p.rx_pol = d->rx_pol;
+    p.rx_pol_stride = d->rx_pol_stride;
+    p.freq = d->frequency_hz[fi];
+    p.k = kTwoPi * p.freq / kC0;
+    const long long mo = (long long)fi * m->num_materials;
+    p.num_materials = m->num_materials;
+    p.eps_r = m->eps_r + mo;
+    p.sigma_e = m->sigma_e + mo;
+    p.mu_r = m->mu_r + mo;
+    p.gain = m->gain + mo;
+    p.thickness = m->thickness + mo;
+    const long long lo = (long long)fi * m->num_layers;
+    p.num_layers = m->num_layers;
+    p.layer_offset = m->layer_offset;
+    p.layer_count = m->layer_count;
+    p.layer_thickness = m->layer_thickness ? m->layer_thickness + lo : nullptr;
+    p.layer_eps_r = m->layer_eps_r ? m->layer_eps_r + lo : nullptr;
+    p.layer_sigma_e = m->layer_sigma_e ? m->layer_sigma_e + lo : nullptr;
+    p.layer_mu_r = m->layer_mu_r ? m->layer_mu_r + lo : nullptr;
+    p.rows = static_cast<const RowRec*>(rows);
+    p.selected = reinterpret_cast<const long long*>(selected);
+    p.count = count;
+    p.width = width;
+    p.out = *out;
+    k_eval_rows<<<int((count + kB - 1) / kB), kB, 0, stream>>>(p);
+    note_launch();
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int rows_accumulate(const void* rows, const int64_t* selected, int64_t n, const float* path_gain, const float* path_field,
+                    const float* field_xyz, const float* tx_power, int num_tx, int num_rx, int coherent,
+                    const wcb_outputs* out, cudaStream_t stream) {
+    const long long cells = (long long)num_tx * num_rx;
+    if (cells <= 0) return 0;
+    k_accumulate_rows<<<int((cells + kB - 1) / kB), kB, 0, stream>>>(
+        static_cast<const RowRec*>(rows), reinterpret_cast<const long long*>(selected), n, path_gain, path_field, field_xyz,
+        tx_power, num_tx, num_rx, coherent, static_cast<float*>(out->path_gain), static_cast<float*>(out->field),
+        static_cast<float*>(out->comp_power), static_cast<float*>(out->comp_field), static_cast<float*>(out->diff_vec_power));
+    note_launch();
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int field_free_space(int64_t n, const float* s, const float* t, const float* pw, const float* tp, const float* rp, double f,
+                     float* fv, float* c, float* pf, float* pg, float* pl, float* dl, float* dr, cudaStream_t stream) {
+    if (n <= 0) return 0;
+    k_field_free_space<<<int((n + kB - 1) / kB), kB, 0, stream>>>(n, s, t, pw, tp, rp, f, fv, c, pf, pg, pl, dl, dr);
+    note_launch();
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int field_reflection(int64_t n, int depth, const float* s, const float* t, const float* pos, const float* nrm, const float* pw,
+                     const float* tp, const float* rp, const float* eps, const float* sig, const float* mu, const float* gain,
+                     const float* th, double f, float* fv, float* c, float* pf, float* pg, float* pl, float* dl, float* dr,
+                     cudaStream_t stream) {
+    if (n <= 0) return 0;
+    if (depth < 1 || depth > kMaxDepth) return 1;
+    k_field_reflection<<<int((n + kB - 1) / kB), kB, 0, stream>>>(n, depth, s, t, pos, nrm, pw, tp, rp, eps, sig, mu, gain, th,
+                                                                   f, fv, c, pf, pg, pl, dl, dr);
+    note_launch();
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int field_project(int64_t n, const float* fv, const float* dir, const float* rp, float* c, float* pg, cudaStream_t stream) {
+    if (n <= 0) return 0;
+    k_field_project<<<int((n + kB - 1) / kB), kB, 0, stream>>>(n, fv, dir, rp, c, pg);
+    note_launch();
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+}  // namespace wcb

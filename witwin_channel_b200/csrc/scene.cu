@@ -1,0 +1,582 @@
+// Scene compile: face planes, coplanar groups, diffraction edges and the
+// GPU LBVH (Morton codes -> radix sort -> Karras radix tree -> AABB refit).
+//
+// Coplanar groups follow native/channel/kernels/paths.cu:3168-3190 (keys) and
+// paths.cu:3768-3912 (ordering); edge selection follows
+// native/channel/kernels/diffraction.cu:803-900 and the shared-boundary merge
+// and policy filter of witwin/channel/scene/resources.py:306-405.  The LBVH is
+// Karras, "Maximizing parallelism in the construction of BVHs, octrees, and
+// k-d trees" (HPG 2012).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <array>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "internal.h"
+
+namespace wcb {
+
+namespace {
+
+constexpr double kPlaneGroupQuant = 1.0e-4;  // propagation/geometry.py:113
+constexpr double kEdgePlaneTol = 1.34e-5;    // propagation/geometry.py:37
+constexpr double kEndpointQuant = 1.0e-4;    // scene/resources.py:296
+constexpr double kNormalCosTol = 1.0 - 1.0e-5;
+constexpr double kPlaneTolerance = 1.0e-3;   // rayd/reflection.cpp:50
+
+// ------------------------------------------------------------ LBVH kernels
+__device__ __forceinline__ unsigned expand_bits(unsigned v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+__global__ void k_morton(int n, const float* vertices, const int* faces, float3 lo, float3 inv_ext,
+                         unsigned long long* keys) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int a = faces[3 * i], b = faces[3 * i + 1], c = faces[3 * i + 2];
+    float cx_ = (vertices[3 * a] + vertices[3 * b] + vertices[3 * c]) * (1.0f / 3.0f);
+    float cy_ = (vertices[3 * a + 1] + vertices[3 * b + 1] + vertices[3 * c + 1]) * (1.0f / 3.0f);
+    float cz_ = (vertices[3 * a + 2] + vertices[3 * b + 2] + vertices[3 * c + 2]) * (1.0f / 3.0f);
+    float x = fminf(fmaxf((cx_ - lo.x) * inv_ext.x * 1024.0f, 0.0f), 1023.0f);
+    float y = fminf(fmaxf((cy_ - lo.y) * inv_ext.y * 1024.0f, 0.0f), 1023.0f);
+    float z = fminf(fmaxf((cz_ - lo.z) * inv_ext.z * 1024.0f, 0.0f), 1023.0f);
+    unsigned code = (expand_bits(unsigned(x)) << 2) | (expand_bits(unsigned(y)) << 1) | expand_bits(unsigned(z));
+    keys[i] = (static_cast<unsigned long long>(code) << 32) | static_cast<unsigned>(i);
+}
+
+__device__ __forceinline__ int delta(const unsigned long long* keys, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    return __clzll(keys[i] ^ keys[j]);
+}
+
+__global__ void k_karras(int n, const unsigned long long* keys, BvhNode* nodes, int* parent_internal,
+                         int* parent_leaf) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2) {
+        if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    }
+    const int j = i + l * d;
+    const int dnode = delta(keys, n, i, j);
+    int s = 0;
+    int div = 2;
+    while (true) {
+        const int t = (l + div - 1) / div;
+        if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+        if (t <= 1) break;
+        div *= 2;
+    }
+    const int gamma = i + s * d + min(d, 0);
+    const int left = (min(i, j) == gamma) ? ~gamma : gamma;
+    const int right = (max(i, j) == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+    nodes[i].d = make_int4(left, right, 0, 0);
+    if (left < 0) parent_leaf[~left] = i; else parent_internal[left] = i;
+    if (right < 0) parent_leaf[~right] = i; else parent_internal[right] = i;
+}
+
+__global__ void k_leaves(int n, const unsigned long long* keys, const float* vertices, const int* faces,
+                         const int* face_group, float4* tri, float* leaf_box) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int f = static_cast<int>(keys[s] & 0xffffffffull);
+    const int a = faces[3 * f], b = faces[3 * f + 1], c = faces[3 * f + 2];
+    const float ax = vertices[3 * a], ay = vertices[3 * a + 1], az = vertices[3 * a + 2];
+    const float bx = vertices[3 * b], by = vertices[3 * b + 1], bz = vertices[3 * b + 2];
+    const float cx_ = vertices[3 * c], cy_ = vertices[3 * c + 1], cz_ = vertices[3 * c + 2];
+    tri[3 * s + 0] = make_float4(ax, ay, az, __int_as_float(f));
+    tri[3 * s + 1] = make_float4(bx, by, bz, __int_as_float(face_group[f]));
+    tri[3 * s + 2] = make_float4(cx_, cy_, cz_, 0.0f);
+    leaf_box[6 * s + 0] = fminf(ax, fminf(bx, cx_));
+    leaf_box[6 * s + 1] = fminf(ay, fminf(by, cy_));
+    leaf_box[6 * s + 2] = fminf(az, fminf(bz, cz_));
+    leaf_box[6 * s + 3] = fmaxf(ax, fmaxf(bx, cx_));
+    leaf_box[6 * s + 4] = fmaxf(ay, fmaxf(by, cy_));
+    leaf_box[6 * s + 5] = fmaxf(az, fmaxf(bz, cz_));
+}
+
+__device__ void child_box(const BvhNode* nodes, const float* leaf_box, int ref, float* out) {
+    if (ref < 0) {
+        const int s = ~ref;
+        for (int k = 0; k < 6; ++k) out[k] = __ldcg(leaf_box + 6 * s + k);
+        return;
+    }
+    const float4 a = __ldcg(&nodes[ref].a);
+    const float4 b = __ldcg(&nodes[ref].b);
+    const float4 c = __ldcg(&nodes[ref].c);
+    out[0] = fminf(a.x, b.z);
+    out[1] = fminf(a.y, b.w);
+    out[2] = fminf(a.z, c.x);
+    out[3] = fmaxf(a.w, c.y);
+    out[4] = fmaxf(b.x, c.z);
+    out[5] = fmaxf(b.y, c.w);
+}
+
+__global__ void k_refit(int n, BvhNode* nodes, const int* parent_internal, const int* parent_leaf,
+                        const float* leaf_box, int* flags, int* depth_out) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int p = parent_leaf[s];
+    int depth = 0;
+    // depth: count internal ancestors of this leaf
+    for (int q = p; q >= 0; q = parent_internal[q]) ++depth;
+    atomicMax(depth_out, depth);
+    while (p >= 0) {
+        __threadfence();
+        const int old = atomicAdd(flags + p, 1);
+        if (old == 0) return;  // first arrival: the sibling finishes this node
+        const int4 d = __ldcg(&nodes[p].d);
+        float l[6], r[6];
+        child_box(nodes, leaf_box, d.x, l);
+        child_box(nodes, leaf_box, d.y, r);
+        nodes[p].a = make_float4(l[0], l[1], l[2], l[3]);
+        nodes[p].b = make_float4(l[4], l[5], r[0], r[1]);
+        nodes[p].c = make_float4(r[2], r[3], r[4], r[5]);
+        __threadfence();
+        p = parent_internal[p];
+    }
+}
+
+__global__ void k_fill_int(int n, int* p, int v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// ------------------------------------------------------------ host helpers
+inline long long llround_f32(float x) { return std::llround(x); }
+
+struct HostFacePlane {
+    double n[3];
+    double off;
+};
+
+std::array<double, 3> sub3(const float* a, const float* b) {
+    return {double(a[0]) - double(b[0]), double(a[1]) - double(b[1]), double(a[2]) - double(b[2])};
+}
+
+std::array<double, 3> cross3(const std::array<double, 3>& a, const std::array<double, 3>& b) {
+    return {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+}
+double dot3(const std::array<double, 3>& a, const std::array<double, 3>& b) {
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+std::array<double, 3> norm3(const std::array<double, 3>& a, double eps = 1e-6) {
+    double l = std::sqrt(dot3(a, a));
+    l = std::max(l, eps);
+    return {a[0] / l, a[1] / l, a[2] / l};
+}
+double unsigned_angle(const std::array<double, 3>& a, const std::array<double, 3>& b, const std::array<double, 3>& axis) {
+    auto c = cross3(a, b);
+    double s = dot3(c, axis);
+    double sn = (s > 0 ? 1.0 : (s < 0 ? -1.0 : 0.0)) * std::sqrt(dot3(c, c));
+    double ang = std::atan2(sn, dot3(a, b));
+    return ang < 0 ? ang + 2.0 * M_PI : ang;
+}
+
+template <typename T>
+T* upload(SceneHandle* h, const std::vector<T>& v, cudaStream_t stream) {
+    T* d = nullptr;
+    size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
+    if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
+    h->owned.push_back(d);
+    if (!v.empty()) cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream);
+    return d;
+}
+
+void* alloc_owned(SceneHandle* h, size_t bytes) {
+    void* d = nullptr;
+    if (cudaMalloc(&d, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
+    h->owned.push_back(d);
+    return d;
+}
+
+}  // namespace
+
+int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, int64_t nf, const int32_t* d_surface,
+                 const int32_t* d_structure, const int32_t* d_material, int boundary_half_plane, int vertical_only,
+                 double vertical_ratio, cudaStream_t stream, SceneHandle** out) {
+    if (nv < 0 || nf < 0 || out == nullptr) return 1;
+    if (nf > INT_MAX / 3 || nv > INT_MAX / 3) return 1;
+    auto* h = new SceneHandle();
+    const int F = static_cast<int>(nf);
+    const int V = static_cast<int>(nv);
+    std::vector<float> verts(size_t(V) * 3);
+    std::vector<int> faces(size_t(F) * 3), surface(F), structure(F), material(F);
+    if (V) cudaMemcpyAsync(verts.data(), d_vertices, verts.size() * 4, cudaMemcpyDeviceToHost, stream);
+    if (F) {
+        cudaMemcpyAsync(faces.data(), d_faces, faces.size() * 4, cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(surface.data(), d_surface, F * 4, cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(structure.data(), d_structure, F * 4, cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(material.data(), d_material, F * 4, cudaMemcpyDeviceToHost, stream);
+    }
+    if (cudaStreamSynchronize(stream) != cudaSuccess) { delete h; return 2; }
+    for (int i = 0; i < F * 3; ++i) {
+        if (faces[i] < 0 || faces[i] >= V) { delete h; return 1; }
+    }
+    // ---- face planes (fp64) and fp32 unit normals
+    std::vector<double> face_plane(size_t(F) * 4);
+    std::vector<float> face_normal(size_t(F) * 3);
+    std::vector<float> nrm32(size_t(F) * 3);
+    for (int f = 0; f < F; ++f) {
+        const float* a = &verts[3 * faces[3 * f]];
+        const float* b = &verts[3 * faces[3 * f + 1]];
+        const float* c = &verts[3 * faces[3 * f + 2]];
+        auto n = norm3(cross3(sub3(b, a), sub3(c, a)));
+        face_plane[4 * f + 0] = n[0];
+        face_plane[4 * f + 1] = n[1];
+        face_plane[4 * f + 2] = n[2];
+        face_plane[4 * f + 3] = n[0] * a[0] + n[1] * a[1] + n[2] * a[2];
+        face_normal[3 * f + 0] = float(n[0]);
+        face_normal[3 * f + 1] = float(n[1]);
+        face_normal[3 * f + 2] = float(n[2]);
+        // fp32 normal as the reference's group keys see it
+        float e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+        float e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+        float cxv[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        float l = std::sqrt(cxv[0] * cxv[0] + cxv[1] * cxv[1] + cxv[2] * cxv[2]);
+        l = std::max(l, 1e-6f);
+        for (int k = 0; k < 3; ++k) nrm32[3 * f + k] = cxv[k] / l;
+    }
+    // ---- coplanar groups (fp32 keys, lexicographic order, stable by face)
+    std::vector<std::array<long long, 5>> keys(F);
+    for (int f = 0; f < F; ++f) {
+        float nx = nrm32[3 * f], ny = nrm32[3 * f + 1], nz = nrm32[3 * f + 2];
+        float norm = std::sqrt(nx * nx + ny * ny + nz * nz);
+        float inv = norm > 1e-6f ? 1.0f / norm : 0.0f;
+        nx *= inv; ny *= inv; nz *= inv;
+        float major_abs = std::fabs(nx), major = nx;
+        if (std::fabs(ny) > major_abs) { major_abs = std::fabs(ny); major = ny; }
+        if (std::fabs(nz) > major_abs) { major = nz; }
+        float sgn = major < 0.0f ? -1.0f : 1.0f;
+        nx *= sgn; ny *= sgn; nz *= sgn;
+        const float* a = &verts[3 * faces[3 * f]];
+        float offset = nx * a[0] + ny * a[1] + nz * a[2];
+        float scale = float(1.0 / kPlaneGroupQuant);
+        keys[f] = {static_cast<long long>(surface[f]), llround_f32(nx * scale), llround_f32(ny * scale),
+                   llround_f32(nz * scale), llround_f32(offset * scale)};
+    }
+    std::vector<int> order(F);
+    for (int f = 0; f < F; ++f) order[f] = f;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return keys[x] < keys[y]; });
+    std::vector<int> face_group(F), group_rep;
+    std::vector<std::vector<int>> members;
+    for (int i = 0; i < F; ++i) {
+        const int f = order[i];
+        if (i == 0 || keys[f] != keys[order[i - 1]]) {
+            group_rep.push_back(f);
+            members.emplace_back();
+        }
+        face_group[f] = int(group_rep.size()) - 1;
+        members.back().push_back(f);
+    }
+    const int G = int(group_rep.size());
+    std::vector<int> member_off(G + 1, 0), member_list;
+    std::vector<double> group_plane(size_t(G) * 4);
+    std::vector<float> group_box(size_t(G) * 6);
+    for (int g = 0; g < G; ++g) {
+        std::sort(members[g].begin(), members[g].end());
+        member_off[g] = int(member_list.size());
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int f : members[g]) {
+            member_list.push_back(f);
+            for (int k = 0; k < 3; ++k) {
+                const float* p = &verts[3 * faces[3 * f + k]];
+                for (int ax = 0; ax < 3; ++ax) {
+                    lo[ax] = std::min(lo[ax], p[ax]);
+                    hi[ax] = std::max(hi[ax], p[ax]);
+                }
+            }
+        }
+        for (int ax = 0; ax < 3; ++ax) {
+            const float pad = float(kPlaneTolerance) + 1e-6f * std::max(std::fabs(lo[ax]), std::fabs(hi[ax]));
+            group_box[6 * g + ax] = lo[ax] - pad;
+            group_box[6 * g + 3 + ax] = hi[ax] + pad;
+        }
+        const int rep = group_rep[g];
+        for (int k = 0; k < 4; ++k) group_plane[4 * g + k] = face_plane[4 * rep + k];
+    }
+    member_off[G] = int(member_list.size());
+    // ---- diffraction edges: per-structure unique undirected edges
+    struct Rec { int v0, v1, f0, f1; };
+    std::vector<Rec> recs;
+    {
+        std::vector<int> structs(structure.begin(), structure.end());
+        std::sort(structs.begin(), structs.end());
+        structs.erase(std::unique(structs.begin(), structs.end()), structs.end());
+        std::vector<std::vector<int>> faces_of(structs.size());
+        for (int f = 0; f < F; ++f) {
+            auto it = std::lower_bound(structs.begin(), structs.end(), structure[f]);
+            faces_of[it - structs.begin()].push_back(f);
+        }
+        for (auto& fl : faces_of) {
+            std::map<std::pair<int, int>, std::vector<int>> table;
+            for (int f : fl) {
+                int vv[3] = {faces[3 * f], faces[3 * f + 1], faces[3 * f + 2]};
+                for (int k = 0; k < 3; ++k) {
+                    int u = vv[k], w = vv[(k + 1) % 3];
+                    table[{std::min(u, w), std::max(u, w)}].push_back(f);
+                }
+            }
+            for (auto& kv : table) {
+                auto v = kv.second;
+                std::sort(v.begin(), v.end());
+                recs.push_back({kv.first.first, kv.first.second, v[0], v.size() > 1 ? v[1] : -1});
+            }
+        }
+    }
+    const int NE = int(recs.size());
+    std::vector<char> sel(NE, 0), boundary(NE, 0);
+    std::vector<std::array<double, 3>> epos(NE), edir(NE), n0o(NE), n1o(NE), opp0(NE);
+    std::vector<double> elen(NE), ext(NE);
+    std::vector<int> face0(NE), face1(NE), mat0(NE), mat1(NE);
+    auto fnormal = [&](int f) { return std::array<double, 3>{face_plane[4 * f], face_plane[4 * f + 1], face_plane[4 * f + 2]}; };
+    auto opposite = [&](int f, int a, int b) {
+        for (int k = 0; k < 3; ++k) {
+            int v = faces[3 * f + k];
+            if (v != a && v != b) return v;
+        }
+        return faces[3 * f + 2];
+    };
+    for (int e = 0; e < NE; ++e) {
+        const Rec& r = recs[e];
+        const bool bnd = r.f0 >= 0 && r.f1 < 0;
+        const bool interior = r.f0 >= 0 && r.f1 >= 0;
+        const int s0 = std::max(r.f0, 0), s1 = std::max(r.f1, 0);
+        const float* st = &verts[3 * r.v0];
+        const float* en = &verts[3 * r.v1];
+        auto vec = sub3(en, st);
+        double L = std::max(std::sqrt(dot3(vec, vec)), 1e-12);
+        std::array<double, 3> d = {vec[0] / L, vec[1] / L, vec[2] / L};
+        auto n0c = norm3(fnormal(s0));
+        auto n1c = norm3(fnormal(s1));
+        auto to1 = norm3(cross3(n0c, d));
+        auto tn1 = norm3(cross3(n1c, d));
+        const bool first = unsigned_angle(to1, tn1, d) < unsigned_angle(tn1, to1, d);
+        auto on0 = first ? n0c : n1c;
+        auto on1 = first ? n1c : n0c;
+        auto out0 = interior ? on0 : n0c;
+        auto out1 = interior ? on1 : n1c;
+        if (r.f1 < 0) out1 = {-n0c[0], -n0c[1], -n0c[2]};
+        double inter = std::acos(std::min(std::max(-dot3(out0, out1), -1.0), 1.0));
+        ext[e] = interior ? (2.0 * M_PI - inter) : 2.0 * M_PI;
+        bool coplanar = false;
+        if (interior) {
+            const bool aligned = std::fabs(dot3(n0c, n1c)) >= kNormalCosTol;
+            auto pa = sub3(&verts[3 * opposite(s0, r.v0, r.v1)], st);
+            auto pb = sub3(&verts[3 * opposite(s1, r.v0, r.v1)], st);
+            coplanar = aligned && std::fabs(dot3(pa, n0c)) <= kEdgePlaneTol && std::fabs(dot3(pb, n0c)) <= kEdgePlaneTol;
+        }
+        const bool wedge_ok = bnd || (interior && dot3(n0c, n1c) < 1.0);
+        sel[e] = (interior || bnd) && !coplanar && L > 1e-6 && wedge_ok;
+        boundary[e] = r.f1 < 0;
+        epos[e] = {0.5 * (double(st[0]) + en[0]), 0.5 * (double(st[1]) + en[1]), 0.5 * (double(st[2]) + en[2])};
+        edir[e] = d;
+        elen[e] = L;
+        n0o[e] = out0;
+        n1o[e] = out1;
+        const bool swapped = interior && !first;
+        const int of = swapped ? s1 : s0;
+        const float* op = &verts[3 * opposite(of, r.v0, r.v1)];
+        opp0[e] = {double(op[0]), double(op[1]), double(op[2])};
+        face0[e] = r.f0;
+        face1[e] = r.f1;
+        mat0[e] = swapped ? r.f1 : r.f0;
+        mat1[e] = swapped ? r.f0 : r.f1;
+    }
+    // shared boundary merge: group boundary records by quantized endpoints
+    {
+        std::map<std::array<long long, 6>, std::vector<int>> groups;
+        for (int e = 0; e < NE; ++e) {
+            if (!(sel[e] && boundary[e])) continue;
+            const float* a = &verts[3 * recs[e].v0];
+            const float* b = &verts[3 * recs[e].v1];
+            std::array<long long, 3> pa, pb;
+            for (int k = 0; k < 3; ++k) {
+                pa[k] = std::llround(double(a[k]) / kEndpointQuant);
+                pb[k] = std::llround(double(b[k]) / kEndpointQuant);
+            }
+            std::array<long long, 6> key;
+            if (pa <= pb) key = {pa[0], pa[1], pa[2], pb[0], pb[1], pb[2]};
+            else key = {pb[0], pb[1], pb[2], pa[0], pa[1], pa[2]};
+            groups[key].push_back(e);
+        }
+        int candidates = 0;
+        for (auto& kv : groups) candidates += int(kv.second.size());
+        if (candidates >= 2) {
+            for (auto& kv : groups) {
+                auto& g = kv.second;
+                if (g.size() < 2) continue;
+                const int a = g[0], b = g[1];
+                double nd = std::min(std::max(dot3(n0o[a], n0o[b]), -1.0), 1.0);
+                double interior_angle = std::acos(std::min(std::max(-nd, -1.0), 1.0));
+                double merged = 2.0 * M_PI - interior_angle;
+                bool copl = std::fabs(nd) >= kNormalCosTol;
+                sel[a] = (merged > M_PI * (1.0 + 1e-6)) && !copl;
+                sel[b] = 0;
+                n1o[a] = n0o[b];
+                face1[a] = face0[b];
+                mat1[a] = mat0[b];
+                ext[a] = merged;
+                boundary[a] = 0;
+                for (size_t x = 2; x < g.size(); ++x) sel[g[x]] = 0;
+            }
+        }
+    }
+    std::vector<EdgeDev> edges;
+    std::vector<int> edge_ids;
+    for (int e = 0; e < NE; ++e) {
+        if (!boundary_half_plane && boundary[e]) sel[e] = 0;
+        if (vertical_only) {
+            auto dv = sub3(&verts[3 * recs[e].v1], &verts[3 * recs[e].v0]);
+            double lz = std::max(std::sqrt(dot3(dv, dv)), 1e-6);
+            if (!(std::fabs(dv[2]) / lz > vertical_ratio)) sel[e] = 0;
+        }
+        if (!sel[e]) continue;
+        EdgeDev ed;
+        std::memset(&ed, 0, sizeof(ed));
+        auto dir = edir[e];
+        auto t0 = norm3(cross3(n0o[e], dir));
+        std::array<double, 3> to_opp = {opp0[e][0] - epos[e][0], opp0[e][1] - epos[e][1], opp0[e][2] - epos[e][2]};
+        if (dot3(to_opp, t0) < 0.0) {
+            dir = {-dir[0], -dir[1], -dir[2]};
+            t0 = {-t0[0], -t0[1], -t0[2]};
+        }
+        std::array<double, 3> bis = {n0o[e][0] + n1o[e][0], n0o[e][1] + n1o[e][1], n0o[e][2] + n1o[e][2]};
+        double bl = std::sqrt(dot3(bis, bis));
+        if (bl > 1e-6) bis = {bis[0] / bl, bis[1] / bl, bis[2] / bl};
+        else bis = {-t0[0], -t0[1], -t0[2]};
+        for (int k = 0; k < 3; ++k) {
+            ed.pos[k] = epos[e][k];
+            ed.dir[k] = dir[k];
+            ed.t0[k] = t0[k];
+            ed.n0[k] = n0o[e][k];
+            ed.n1[k] = n1o[e][k];
+            ed.bisector[k] = bis[k];
+        }
+        ed.half_length = 0.5 * elen[e];
+        ed.n = ext[e] / M_PI;
+        ed.face0 = face0[e];
+        ed.face1 = face1[e];
+        ed.mat_face0 = mat0[e];
+        ed.mat_face1 = mat1[e] >= 0 ? mat1[e] : mat0[e];
+        ed.edge_id = e;
+        edges.push_back(ed);
+        edge_ids.push_back(e);
+    }
+    // ---- upload tables
+    SceneDev& sd = h->dev;
+    std::memset(&sd, 0, sizeof(sd));
+    sd.num_vertices = V;
+    sd.num_faces = F;
+    sd.num_groups = G;
+    sd.num_edges = int(edges.size());
+    sd.vertices = upload(h, verts, stream);
+    sd.faces = upload(h, faces, stream);
+    sd.face_normal = upload(h, face_normal, stream);
+    sd.face_plane = upload(h, face_plane, stream);
+    sd.face_group = upload(h, face_group, stream);
+    sd.face_material = upload(h, material, stream);
+    sd.group_rep = upload(h, group_rep, stream);
+    sd.group_member_off = upload(h, member_off, stream);
+    sd.group_members = upload(h, member_list, stream);
+    sd.group_plane = upload(h, group_plane, stream);
+    sd.group_box = upload(h, group_box, stream);
+    sd.edges = upload(h, edges, stream);
+    h->edge_ids = upload(h, edge_ids, stream);
+    {
+        std::vector<int> slot(std::max(NE, 1), -1);
+        for (size_t i = 0; i < edge_ids.size(); ++i) slot[edge_ids[i]] = int(i);
+        h->edge_slot = upload(h, slot, stream);
+    }
+    h->group_rep_host = group_rep;
+    h->face_group_host = face_group;
+    h->num_edges_total = NE;
+    // bounds
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = 0; i < V; ++i)
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], verts[3 * i + k]);
+            hi[k] = std::max(hi[k], verts[3 * i + k]);
+        }
+    sd.diagonal = V ? std::sqrt(double(hi[0] - lo[0]) * (hi[0] - lo[0]) + double(hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                                double(hi[2] - lo[2]) * (hi[2] - lo[2]))
+                    : 0.0;
+    // ---- LBVH
+    sd.root = INT_MIN;
+    sd.max_depth = 0;
+    if (F > 0) {
+        float4* tri = static_cast<float4*>(alloc_owned(h, size_t(F) * 3 * sizeof(float4)));
+        BvhNode* nodes = static_cast<BvhNode*>(alloc_owned(h, size_t(std::max(F - 1, 1)) * sizeof(BvhNode)));
+        unsigned long long* keys = nullptr;
+        unsigned long long* keys_sorted = nullptr;
+        int *parent_internal = nullptr, *parent_leaf = nullptr, *flags = nullptr, *depth = nullptr;
+        float* leaf_box = nullptr;
+        cudaMalloc(&keys, size_t(F) * 8);
+        cudaMalloc(&keys_sorted, size_t(F) * 8);
+        cudaMalloc(&parent_internal, size_t(std::max(F - 1, 1)) * 4);
+        cudaMalloc(&parent_leaf, size_t(F) * 4);
+        cudaMalloc(&flags, size_t(std::max(F - 1, 1)) * 4);
+        cudaMalloc(&leaf_box, size_t(F) * 24);
+        cudaMalloc(&depth, 4);
+        const int B = 256;
+        float3 flo = make_float3(lo[0], lo[1], lo[2]);
+        float3 inv = make_float3(1.0f / std::max(hi[0] - lo[0], 1e-6f), 1.0f / std::max(hi[1] - lo[1], 1e-6f),
+                                 1.0f / std::max(hi[2] - lo[2], 1e-6f));
+        k_morton<<<(F + B - 1) / B, B, 0, stream>>>(F, sd.vertices, sd.faces, flo, inv, keys);
+        note_launch();
+        size_t temp = 0;
+        cub::DeviceRadixSort::SortKeys(nullptr, temp, keys, keys_sorted, F, 0, 64, stream);
+        void* tmp = nullptr;
+        cudaMalloc(&tmp, std::max<size_t>(temp, 16));
+        cub::DeviceRadixSort::SortKeys(tmp, temp, keys, keys_sorted, F, 0, 64, stream);
+        k_fill_int<<<(F + B - 1) / B, B, 0, stream>>>(std::max(F - 1, 1), parent_internal, -1);
+        k_fill_int<<<(F + B - 1) / B, B, 0, stream>>>(F, parent_leaf, -1);
+        k_fill_int<<<(F + B - 1) / B, B, 0, stream>>>(std::max(F - 1, 1), flags, 0);
+        k_fill_int<<<1, 1, 0, stream>>>(1, depth, 0);
+        note_launch(4);
+        k_leaves<<<(F + B - 1) / B, B, 0, stream>>>(F, keys_sorted, sd.vertices, sd.faces, sd.face_group, tri, leaf_box);
+        note_launch();
+        if (F > 1) {
+            k_karras<<<(F - 1 + B - 1) / B, B, 0, stream>>>(F, keys_sorted, nodes, parent_internal, parent_leaf);
+            k_refit<<<(F + B - 1) / B, B, 0, stream>>>(F, nodes, parent_internal, parent_leaf, leaf_box, flags, depth);
+            note_launch(2);
+        }
+        int hdepth = 0;
+        cudaMemcpyAsync(&hdepth, depth, 4, cudaMemcpyDeviceToHost, stream);
+        cudaError_t err = cudaStreamSynchronize(stream);
+        cudaFree(keys); cudaFree(keys_sorted); cudaFree(parent_internal); cudaFree(parent_leaf);
+        cudaFree(flags); cudaFree(leaf_box); cudaFree(depth); cudaFree(tmp);
+        if (err != cudaSuccess) { scene_destroy(h); return 2; }
+        sd.tri = tri;
+        sd.nodes = nodes;
+        sd.root = F > 1 ? 0 : ~0;
+        sd.max_depth = hdepth;
+        h->num_nodes = std::max(F - 1, 0);
+        if (hdepth >= kStackDepth) { scene_destroy(h); return 4; }
+    }
+    if (cudaStreamSynchronize(stream) != cudaSuccess) { scene_destroy(h); return 2; }
+    *out = h;
+    return 0;
+}
+
+void scene_destroy(SceneHandle* h) {
+    if (!h) return;
+    for (void* p : h->owned) cudaFree(p);
+    delete h;
+}
+
+}  // namespace wcb

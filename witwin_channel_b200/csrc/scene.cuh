@@ -1,0 +1,49 @@
+// Device-resident scene: triangles in Morton order, the LBVH, per-face
+// tables, coplanar face groups and the selected diffraction edges.
+#pragma once
+
+#include "common.cuh"
+#include "utd.cuh"
+
+namespace wcb {
+
+constexpr int kStackDepth = 64;  // per-thread traversal stack entries (shared memory)
+
+// BVH node: both child boxes plus the child references (64 bytes, four
+// 16-byte loads).  child >= 0: internal node; child < 0: leaf ~slot.
+struct __align__(16) BvhNode {
+    float4 a;  // c0.lo.xyz, c0.hi.x
+    float4 b;  // c0.hi.yz, c1.lo.xy
+    float4 c;  // c1.lo.z, c1.hi.xyz
+    int4 d;    // left, right, -, -
+};
+
+struct SceneDev {
+    int num_vertices;
+    int num_faces;
+    int num_groups;
+    int num_edges;        // selected edges
+    int root;             // root child reference (internal node index, or ~slot, or INT_MIN when empty)
+    int max_depth;        // BVH depth (root = 0)
+    // geometry
+    const float* vertices;     // (V,3)
+    const int* faces;          // (F,3)
+    const float4* tri;         // (F*3) Morton order: v0|face, v1|group, v2|pad
+    const BvhNode* nodes;      // (F-1)
+    // per face (original order)
+    const float* face_normal;  // (F,3) unit, fp32
+    const double* face_plane;  // (F,4) unit normal + offset n.v0, fp64
+    const int* face_group;     // (F)
+    const int* face_material;  // (F)
+    // groups
+    const int* group_rep;          // (G)
+    const int* group_member_off;   // (G+1)
+    const int* group_members;      // (F) ascending face index within a group
+    const double* group_plane;     // (G,4) representative normal + offset (anchor = rep's v0)
+    const float* group_box;        // (G,6) lo.xyz hi.xyz padded by the plane tolerance
+    // edges
+    const EdgeDev* edges;          // (E)
+    double diagonal;               // scene bounding-box diagonal
+};
+
+}  // namespace wcb

@@ -1,0 +1,906 @@
+// Fused deterministic radiomap solve.
+//
+// Candidate preparation (per transmitter):
+//   * reflection chains of coplanar groups per depth: exhaustive
+//     (adjacent-distinct, paths.cu:364-406) when the reference's planning
+//     guard allows it, otherwise discovered by tracing the FP64 Fibonacci
+//     sphere (montecarlo.cu:713-731) with specular bounces and keeping the
+//     unique group chains per depth (interactions/reflection.py:186-293,
+//     541-569); FP64 image points are precomputed per chain;
+//   * diffraction edges the source sees (exterior test + sampled-point
+//     visibility prefilter, rayd/diffraction.cpp:380-403).
+// Main kernel: one thread per (transmitter, receiver cell).  Each thread walks
+// every candidate of its transmitter, traces the visibility segments through
+// the LBVH, evaluates the complex fields for every solve frequency and keeps
+// the per-slot coherent sums in registers; each output cell is written once.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <vector>
+
+#include "em.cuh"
+#include "internal.h"
+#include "paths.cuh"
+#include "solve.h"
+#include "utd.cuh"
+
+namespace wcb {
+
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kMaxNF = 4;
+constexpr long long kOrder1ExhaustiveLimit = 4096;      // interactions/reflection.py:30
+constexpr long long kMultibounceExhaustiveLimit = 100000;  // interactions/reflection.py:31
+
+// ------------------------------------------------------------ discovery
+__global__ void k_fibonacci(int count, float* dirs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const double golden = 1.618033988749894848204586834365638118;
+    const double idx = double(i);
+    const double az = idx / golden;
+    const double az_u = az - floor(az);
+    const double ev = count == 1 ? 0.0 : idx / double(count - 1);
+    const double phi = 2.0 * kPi * az_u;
+    const double z = 1.0 - 2.0 * ev;
+    const double radial = sqrt(fmax(1.0 - z * z, 0.0));
+    dirs[3 * i + 0] = float(radial * cos(phi));
+    dirs[3 * i + 1] = float(radial * sin(phi));
+    dirs[3 * i + 2] = float(z);
+}
+
+template <typename G>
+__global__ void __launch_bounds__(kBlock) k_discovery_trace(SceneDev sc, int count, int depth, const float* dirs,
+                                                            const float* tx, int* groups_out, int* err) {
+    extern __shared__ int stack[];
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    V3<G> o = v3<G>(G(tx[0]), G(tx[1]), G(tx[2]));
+    V3<G> d = v3<G>(G(dirs[3 * i]), G(dirs[3 * i + 1]), G(dirs[3 * i + 2]));
+    int last = -1;
+    bool alive = true;
+    for (int k = 0; k < depth; ++k) {
+        int hit_group = -1;
+        if (alive) {
+            const G inf = sizeof(G) == 4 ? G(3e38) : G(1e300);
+            Ray<G> r = make_ray<G>(o, d, G(1e-6), inf);
+            Ignore ig = ignore_none();
+            ig.f0 = last;
+            G bt = inf;
+            int bf = -1, bg = -1;
+            traverse<1, G>(sc, r, ig, stack, err, &bt, &bf, &bg, NoSink{});
+            if (bf >= 0) {
+                hit_group = bg;
+                const float* n = sc.face_normal + 3 * bf;
+                const V3<G> nn = v3<G>(G(n[0]), G(n[1]), G(n[2]));
+                o = o + d * bt;
+                d = d - nn * (G(2) * dot(d, nn));
+                last = bf;
+            } else {
+                alive = false;
+            }
+        }
+        groups_out[size_t(i) * depth + k] = hit_group;
+    }
+}
+
+// key for unique chains at depth k: (prefix rank << 21) | group
+__global__ void k_chain_keys(int count, int depth, int k, const int* groups, const int* prefix_rank,
+                             unsigned long long* keys, int* vals) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int g = groups[size_t(i) * depth + k];
+    const int pr = k == 0 ? 0 : prefix_rank[i];
+    unsigned long long key;
+    if (g < 0 || pr < 0) key = ~0ull;
+    else key = (static_cast<unsigned long long>(pr) << 21) | static_cast<unsigned long long>(g);
+    keys[i] = key;
+    vals[i] = i;
+}
+
+__global__ void k_chain_flags(int count, const unsigned long long* keys, int* flags) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const bool valid = keys[i] != ~0ull;
+    flags[i] = valid && (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
+}
+
+// rank of each ray's chain after the inclusive scan of flags; the first ray
+// of each run writes the chain's group ids into the chain table (when one is
+// given) and the last valid element writes the chain count.
+__global__ void k_chain_emit(int count, int depth, int k, const unsigned long long* keys, const int* vals,
+                             const int* flags, const int* scan, const int* groups, int* rank_out, int* chain_groups,
+                             int chain_cap, int* chain_count) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int ray = vals[i];
+    if (keys[i] == ~0ull) {
+        rank_out[ray] = -1;
+        return;
+    }
+    const int rank = scan[i] - 1;
+    rank_out[ray] = rank;
+    if (chain_groups != nullptr && flags[i] && rank < chain_cap) {
+        for (int c = 0; c <= k; ++c) chain_groups[size_t(rank) * (k + 1) + c] = groups[size_t(ray) * depth + c];
+    }
+    if (chain_count != nullptr && (i == count - 1 || keys[i + 1] == ~0ull)) {
+        *chain_count = min(rank + 1, chain_cap);
+    }
+}
+
+// exhaustive adjacent-distinct sequences (paths.cu:364-406)
+__global__ void k_exhaustive_chains(long long total, int depth, int groups_n, int* chain_groups) {
+    long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (row >= total) return;
+    long long value = row;
+    const long long base = depth > 1 ? groups_n - 1 : groups_n;
+    long long div = 1;
+    for (int p = 1; p < depth; ++p) div *= base;
+    long long prev = -1;
+    for (int col = 0; col < depth; ++col) {
+        long long digit;
+        if (depth > 1) {
+            const long long raw = value / div;
+            value -= raw * div;
+            div = div > 1 ? div / base : 1;
+            digit = col == 0 ? raw : (raw < prev ? raw : raw + 1);
+            prev = digit;
+        } else {
+            digit = value;
+        }
+        chain_groups[row * depth + col] = int(digit);
+    }
+}
+
+// FP64 images of the source through each chain's group planes.
+__global__ void k_chain_images(SceneDev sc, const float* tx, int depth, const int* count_ptr, long long count_fixed,
+                               const int* chain_groups, double* planes_out, double* images_out) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long count = count_ptr ? *count_ptr : count_fixed;
+    if (c >= count) return;
+    V3<double> p = v3<double>(tx[0], tx[1], tx[2]);
+    for (int k = 0; k < depth; ++k) {
+        const int g = chain_groups[c * depth + k];
+        const double* pl = sc.group_plane + 4 * g;
+        const V3<double> n = v3(pl[0], pl[1], pl[2]);
+        p = p - n * (2.0 * (dot(p, n) - pl[3]));
+        double* po = planes_out + (c * depth + k) * 4;
+        po[0] = pl[0]; po[1] = pl[1]; po[2] = pl[2]; po[3] = pl[3];
+        double* io = images_out + (c * depth + k) * 3;
+        io[0] = p.x; io[1] = p.y; io[2] = p.z;
+    }
+}
+
+// ------------------------------------------------------------ edge prefilter
+template <typename G>
+__global__ void __launch_bounds__(kBlock) k_edge_flags(SceneDev sc, const float* tx_pos, int t, double wavelength,
+                                                       int* flags, int* err) {
+    extern __shared__ int stack[];
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= sc.num_edges) return;
+    const EdgeDev ed = sc.edges[j];
+    const V3<double> S = v3<double>(tx_pos[3 * t], tx_pos[3 * t + 1], tx_pos[3 * t + 2]);
+    const V3<double> c = v3(ed.pos[0], ed.pos[1], ed.pos[2]);
+    const V3<double> e = v3(ed.dir[0], ed.dir[1], ed.dir[2]);
+    V3<double> ds = S - c;
+    ds = ds - e * dot(ds, e);
+    const double phi_p = double(wedge_angle(ds, v3(ed.t0[0], ed.t0[1], ed.t0[2]), v3(ed.n0[0], ed.n0[1], ed.n0[2])));
+    int ok = 0;
+    if (phi_p <= ed.n * kPi) {
+        const double L = 2.0 * ed.half_length;
+        int n = int(ceil(L / wavelength));
+        n = n < 4 ? 4 : (n > 16 ? 16 : n);
+        Ignore ig = ignore_none();
+        ig.f0 = ed.face0;
+        ig.f1 = ed.face1;
+        const V3<double> bis = v3(ed.bisector[0], ed.bisector[1], ed.bisector[2]);
+        for (int i = 0; i < n && !ok; ++i) {
+            const double tt = -0.5 * L + (i + 0.5) / n * L;
+            const V3<double> p = c + e * tt + bis * kDiffractionRayBias;
+            if (!segment_blocked<G>(sc, cast3<G>(S), cast3<G>(p), ig, stack, err)) ok = 1;
+        }
+    }
+    flags[j] = ok;
+}
+
+// ordered compaction of edge flags (one block per call)
+__global__ void k_compact_flags(int n, const int* flags, int* list, int* count) {
+    typedef cub::BlockScan<int, 256> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ int base;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    for (int start = 0; start < n; start += 256) {
+        const int i = start + threadIdx.x;
+        const int f = i < n ? flags[i] : 0;
+        int pos, total;
+        Scan(tmp).ExclusiveSum(f, pos, total);
+        if (f) list[base + pos] = i;
+        __syncthreads();
+        if (threadIdx.x == 0) base += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *count = base;
+}
+
+// ------------------------------------------------------------ main kernel
+template <typename T>
+struct Accum {
+    Cx<T> slot[4];   // los, reflection, diffraction, transmission
+    T gain[4];
+    Cx<T> dv[3];     // diffraction vector sum (powered)
+};
+
+template <typename T>
+WCB_D Slab<T> face_slab(const MainParams& p, int f_index, int face) {
+    const int m = p.sc.face_material[face];
+    const long long o = (long long)f_index * p.num_materials + m;
+    return Slab<T>{T(p.mat_eps_r[o]), T(p.mat_sigma_e[o]), T(p.mat_mu_r[o]), T(p.mat_gain[o]), T(p.mat_thickness[o])};
+}
+
+template <typename T>
+WCB_D LayerTable<T> layer_table_f(const MainParams& p, int f_index);
+
+template <>
+WCB_D LayerTable<float> layer_table_f<float>(const MainParams& p, int f_index) {
+    const long long o = (long long)f_index * p.num_layers;
+    return LayerTable<float>{p.layer_offset, p.layer_count, p.layer_thickness + o, p.layer_eps_r + o,
+                             p.layer_sigma_e + o, p.layer_mu_r + o};
+}
+
+template <>
+WCB_D LayerTable<double> layer_table_f<double>(const MainParams& p, int f_index) {
+    // FP64 precision mode reads the float layer tables through a converting view
+    const long long o = (long long)f_index * p.num_layers;
+    return LayerTable<double>{p.layer_offset, p.layer_count, p.layer_thickness64 + o, p.layer_eps_r64 + o,
+                              p.layer_sigma_e64 + o, p.layer_mu_r64 + o};
+}
+
+WCB_D void emit_row(const MainParams& p, int t, int r, int cid, int depth, const int* seq, int edge, float length) {
+    if (p.rows == nullptr) return;
+    const unsigned long long idx = atomicAdd(p.row_counter, 1ull);
+    if (idx >= (unsigned long long)p.row_capacity) return;
+    RowRec rec;
+    rec.tx = t;
+    rec.rx = r;
+    rec.component = short(cid);
+    rec.depth = short(depth);
+    for (int k = 0; k < kMaxDepth; ++k) rec.seq[k] = k < depth && seq ? seq[k] : -1;
+    rec.edge = edge;
+    rec.length = length;
+    rec.pad = 0;
+    rec.pad2 = 0;
+    p.rows[idx] = rec;
+}
+
+template <typename T>
+WCB_D V3<T> rx_position(const MainParams& p, int r) {
+    if (p.rx_kind == 1) {
+        const int row = r / p.grid_cols;
+        const int col = r - row * p.grid_cols;
+        const float u = __fmul_rn(float(row), p.grid_spacing[0]);
+        const float v = __fmul_rn(float(col), p.grid_spacing[1]);
+        // (origin + x_axis*u) + y_axis*v, rounded per operation (los.cu:391-420)
+        return v3<T>(T(__fadd_rn(__fadd_rn(p.grid_origin[0], __fmul_rn(p.grid_x[0], u)), __fmul_rn(p.grid_y[0], v))),
+                     T(__fadd_rn(__fadd_rn(p.grid_origin[1], __fmul_rn(p.grid_x[1], u)), __fmul_rn(p.grid_y[1], v))),
+                     T(__fadd_rn(__fadd_rn(p.grid_origin[2], __fmul_rn(p.grid_x[2], u)), __fmul_rn(p.grid_y[2], v))));
+    }
+    return v3<T>(T(p.rx_pos[3 * r]), T(p.rx_pos[3 * r + 1]), T(p.rx_pos[3 * r + 2]));
+}
+
+// cell index of lane `i` (warps cover 8x4 receiver-grid patches)
+WCB_D bool cell_of(const MainParams& p, long long i, int* t, int* r) {
+    if (p.rx_kind == 1) {
+        const int tiles_r = (p.grid_rows + 7) / 8;
+        const int tiles_c = (p.grid_cols + 3) / 4;
+        const long long per_tx = (long long)tiles_r * tiles_c * 32;
+        const long long tt = i / per_tx;
+        if (tt >= p.num_tx) return false;
+        const long long rem = i - tt * per_tx;
+        const long long tile = rem / 32;
+        const int lane = int(rem - tile * 32);
+        const int tr = int(tile / tiles_c), tc = int(tile - (long long)tr * tiles_c);
+        const int row = tr * 8 + lane / 4;
+        const int col = tc * 4 + (lane & 3);
+        if (row >= p.grid_rows || col >= p.grid_cols) return false;
+        *t = int(tt);
+        *r = row * p.grid_cols + col;
+        return true;
+    }
+    const long long tt = i / p.num_rx;
+    if (tt >= p.num_tx) return false;
+    *t = int(tt);
+    *r = int(i - tt * p.num_rx);
+    return true;
+}
+
+template <typename T, int NF>
+__global__ void __launch_bounds__(kBlock) k_main(MainParams p) {
+    extern __shared__ int stack[];
+    const long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int t, r;
+    if (!cell_of(p, gi, &t, &r)) return;
+    const SceneDev& sc = p.sc;
+    const V3<double> S = v3<double>(p.tx_pos[3 * t], p.tx_pos[3 * t + 1], p.tx_pos[3 * t + 2]);
+    const V3<float> Rf = rx_position<float>(p, r);
+    const V3<double> R = cast3<double>(Rf);
+    const V3<T> ST = cast3<T>(S), RT = cast3<T>(R);
+    const V3<T> tx_pol = v3<T>(T(p.tx_pol[3 * t]), T(p.tx_pol[3 * t + 1]), T(p.tx_pol[3 * t + 2]));
+    const float* rp = p.rx_pol + (long long)r * p.rx_pol_stride;
+    const V3<T> rx_pol = v3<T>(T(rp[0]), T(rp[1]), T(rp[2]));
+    const T sqrt_p = s_sqrt(s_max(T(p.tx_power[t]), T(0)));
+    Accum<T> acc[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        for (int s = 0; s < 4; ++s) { acc[f].slot[s] = cx(T(0), T(0)); acc[f].gain[s] = T(0); }
+        for (int s = 0; s < 3; ++s) acc[f].dv[s] = cx(T(0), T(0));
+    }
+    int* err = p.status;
+    // -------------------------------------------------------------- LoS
+    if (p.components & 1) {
+        const bool blocked = sc.num_faces > 0 && segment_blocked<T>(sc, ST, RT, ignore_none(), stack, err);
+        if (!blocked) {
+            const double dist = length(R - S);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const PathEval<T> ev = eval_free_space(ST, RT, tx_pol, rx_pol, p.k[f], dist);
+                const Cx<T> pf = ev.coefficient * sqrt_p;
+                acc[f].slot[0] = acc[f].slot[0] + pf;
+                acc[f].gain[0] = acc[f].gain[0] + cabs2(pf);
+            }
+            emit_row(p, t, r, 0, 0, nullptr, -1, float(dist));
+        }
+    }
+    // -------------------------------------------------------------- reflection
+    if ((p.components & 2) && sc.num_faces > 0) {
+        for (int d = 1; d <= p.max_depth; ++d) {
+            const int cnt = p.chain_count[t * kMaxDepth + (d - 1)];
+            const long long base = p.chain_offset[t * kMaxDepth + (d - 1)];
+            const int* cg = p.chain_groups + base * 1;  // offsets are in int units (chain * depth)
+            const double* cpl = p.chain_planes + base * 4;
+            const double* cim = p.chain_images + base * 3;
+            for (int c = 0; c < cnt; ++c) {
+                const int* groups = cg + (long long)c * d;
+                const double* planes = cpl + (long long)c * d * 4;
+                const double* images = cim + (long long)c * d * 3;
+                if (sizeof(T) == 4 && !back_project_prefilter(sc, Rf, groups, planes, images, d)) continue;
+                V3<double> hits[kMaxDepth];
+                if (!back_project(R, planes, images, d, hits)) continue;
+                int faces[kMaxDepth];
+                bool ok = true;
+                for (int k = d - 1; k >= 0 && ok; --k) {
+                    faces[k] = resolve_in_group(sc, groups[k], hits[k]);
+                    ok = faces[k] >= 0;
+                }
+                if (!ok) continue;
+                // visibility of the d+1 segments
+                for (int s = 0; s <= d && ok; ++s) {
+                    const V3<double> a = s == 0 ? S : hits[s - 1];
+                    const V3<double> b = s == d ? R : hits[s];
+                    Ignore ig = ignore_none();
+                    ig.g0 = s > 0 ? groups[s - 1] : -1;
+                    ig.g1 = s < d ? groups[s] : -1;
+                    if (segment_blocked<T>(sc, cast3<T>(a), cast3<T>(b), ig, stack, err)) ok = false;
+                }
+                if (!ok) continue;
+                const V3<double> img = v3(images[3 * (d - 1)], images[3 * (d - 1) + 1], images[3 * (d - 1) + 2]);
+                const double total = length(R - img);
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    const double freq = p.freq[f];
+                    const T wl = T(kC0 / freq);
+                    const V3<T> ez = v3<T>(T(0), T(0), T(1));
+                    V3<T> prev = ST;
+                    V3<T> incident = safe_normalize(cast3<T>(hits[0]) - prev, ez);
+                    C3<T> value = c3_from_real(transverse(incident, tx_pol));
+                    V3<T> outgoing = incident;
+                    for (int k = 0; k < d; ++k) {
+                        const V3<T> hit = cast3<T>(hits[k]);
+                        incident = safe_normalize(hit - prev, outgoing);
+                        const float* nf = sc.face_normal + 3 * faces[k];
+                        reflect_bounce(value, outgoing, incident, v3<T>(T(nf[0]), T(nf[1]), T(nf[2])),
+                                       face_slab<T>(p, f, faces[k]), freq, wl);
+                        prev = hit;
+                    }
+                    const V3<T> fdir = safe_normalize(RT - prev, outgoing);
+                    const T amp = T(1) / (T(2) * T(p.k[f]) * T(fmax(total, kUtdEps)));
+                    const Cx<T> prop = phasor_neg_kd<T>(p.k[f], total) * amp;
+                    value = c3_scale(value, prop);
+                    const Cx<T> pf = project_receiver(value, fdir, rx_pol) * sqrt_p;
+                    acc[f].slot[1] = acc[f].slot[1] + pf;
+                    acc[f].gain[1] = acc[f].gain[1] + cabs2(pf);
+                }
+                emit_row(p, t, r, 1, d, faces, -1, float(total));
+            }
+        }
+    }
+    // -------------------------------------------------------------- diffraction
+    if ((p.components & 4) && sc.num_edges > 0 && p.max_depth >= 1) {
+        const int cnt = p.edge_count[t];
+        const int* list = p.edge_list + (long long)t * sc.num_edges;
+        for (int j = 0; j < cnt; ++j) {
+            const EdgeDev& ed = sc.edges[list[j]];
+            C3<T> fields[NF];
+            bool any = false;
+            bool valid = false;
+            DiffractionResult<T> res;
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const int m0 = ed.mat_face0, mn = ed.mat_face1;
+                res = utd_field<T>(ed, S, R, tx_pol, face_slab<T>(p, f, m0), face_slab<T>(p, f, mn), p.freq[f]);
+                valid = res.valid;
+                fields[f] = res.field;
+                if (res.valid && value_of(c3_power(res.field)) * value_of(sqrt_p * sqrt_p) >= kUtdGainFloor) any = true;
+            }
+            if (!valid || !any) continue;
+            Ignore ig = ignore_none();
+            ig.f0 = ed.face0;
+            ig.f1 = ed.face1;
+            const V3<double> qv = v3(res.q_vis[0], res.q_vis[1], res.q_vis[2]);
+            if (segment_blocked<T>(sc, ST, cast3<T>(qv), ig, stack, err)) continue;
+            if (segment_blocked<T>(sc, cast3<T>(qv), RT, ig, stack, err)) continue;
+            const V3<double> q = v3(res.q[0], res.q[1], res.q[2]);
+            const V3<T> arrival = safe_normalize(cast3<T>(R - q), v3<T>(T(0), T(0), T(1)));
+            bool emitted = false;
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const C3<T> powered = c3_scale(fields[f], cx(sqrt_p, T(0)));
+                if (value_of(c3_power(powered)) < kUtdGainFloor) continue;
+                const Cx<T> pf = project_receiver(powered, arrival, rx_pol);
+                acc[f].slot[2] = acc[f].slot[2] + pf;
+                acc[f].gain[2] = acc[f].gain[2] + cabs2(pf);
+                acc[f].dv[0] = acc[f].dv[0] + powered.x;
+                acc[f].dv[1] = acc[f].dv[1] + powered.y;
+                acc[f].dv[2] = acc[f].dv[2] + powered.z;
+                if (!emitted) {
+                    emit_row(p, t, r, 2, 1, nullptr, ed.edge_id, float(res.length));
+                    emitted = true;
+                }
+            }
+        }
+    }
+    // -------------------------------------------------------------- transmission
+    if ((p.components & 8) && sc.num_faces > 0 && p.max_depth >= 1) {
+        HitList hl;
+        segment_hits<T>(sc, ST, RT, p.max_depth, &hl, stack, err);
+        if (hl.count > p.max_depth) {
+            if (p.overflow_counter) atomicAdd(p.overflow_counter, 1ull);
+        } else if (hl.count >= 1) {
+            bool ok = true;
+            for (int i = 0; i < hl.count; ++i) {
+                const int m = sc.face_material[hl.face[i]];
+                if (p.mat_volumetric && p.mat_volumetric[m]) ok = false;
+            }
+            if (ok) {
+                const double dist = length(R - S);
+                const V3<T> dir = safe_normalize(RT - ST, v3<T>(T(0), T(0), T(1)));
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    C3<T> value = c3_from_real(transverse(dir, tx_pol));
+                    T shorten = T(0);
+                    const LayerTable<T> lt = layer_table_f<T>(p, f);
+                    for (int i = 0; i < hl.count; ++i) {
+                        const float* nf = sc.face_normal + 3 * hl.face[i];
+                        transmit_wall(value, shorten, dir, v3<T>(T(nf[0]), T(nf[1]), T(nf[2])),
+                                      sc.face_material[hl.face[i]], lt, p.freq[f]);
+                    }
+                    const T amp = T(1) / (T(2) * T(p.k[f]) * T(fmax(dist, kUtdEps)));
+                    const Cx<T> prop = phasor_neg_kd<T>(p.k[f], dist - double(value_of(shorten))) * amp;
+                    value = c3_scale(value, prop);
+                    const Cx<T> pf = project_receiver(value, dir, rx_pol) * sqrt_p;
+                    acc[f].slot[3] = acc[f].slot[3] + pf;
+                    acc[f].gain[3] = acc[f].gain[3] + cabs2(pf);
+                }
+                emit_row(p, t, r, 5, hl.count, hl.face, -1, float(dist));
+            }
+        }
+    }
+    // -------------------------------------------------------------- outputs
+    const long long cells = (long long)p.num_tx * p.num_rx;
+    const long long cell = (long long)t * p.num_rx + r;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        const long long fc = (long long)(p.freq_base + f) * cells + cell;
+        const long long slot_stride = (long long)p.num_freq_total * cells;
+        Cx<T> total = cx(T(0), T(0));
+        T gsum = T(0);
+        for (int s = 0; s < 4; ++s) {
+            total = total + acc[f].slot[s];
+            gsum = gsum + acc[f].gain[s];
+        }
+        T* pg = static_cast<T*>(p.out_path_gain);
+        T* fl = static_cast<T*>(p.out_field);
+        T* cp = static_cast<T*>(p.out_comp_power);
+        T* cf = static_cast<T*>(p.out_comp_field);
+        T* dvp = static_cast<T*>(p.out_diff_vec_power);
+        if (p.coherent) {
+            if (pg) pg[fc] = cabs2(total);
+            if (fl) { fl[2 * fc] = total.re; fl[2 * fc + 1] = total.im; }
+        } else {
+            if (pg) pg[fc] = gsum;
+            if (fl) { fl[2 * fc] = s_sqrt(s_max(gsum, T(0))); fl[2 * fc + 1] = T(0); }
+        }
+        for (int s = 0; s < 6; ++s) {
+            const long long o = s * slot_stride + fc;
+            const Cx<T> v = s < 4 ? acc[f].slot[s] : cx(T(0), T(0));
+            if (cp) cp[o] = s < 4 ? (p.coherent ? cabs2(v) : acc[f].gain[s]) : T(0);
+            if (cf) { cf[2 * o] = v.re; cf[2 * o + 1] = v.im; }
+        }
+        if (dvp) dvp[fc] = cabs2(acc[f].dv[0]) + cabs2(acc[f].dv[1]) + cabs2(acc[f].dv[2]);
+    }
+}
+
+__global__ void k_to_double(long long n, const float* in, double* out) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[i];
+}
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+// ------------------------------------------------------------ host side
+struct ChainPlan {
+    bool exhaustive_o1;
+    bool exhaustive_mb;
+    long long cap[kMaxDepth];      // chains capacity per depth
+    long long offset_int[kMaxDepth];
+};
+
+static long long seq_count(long long g, int d) {
+    if (d > 1) {
+        if (g <= 1) return 0;
+        long long v = g;
+        for (int i = 1; i < d; ++i) {
+            if (v > LLONG_MAX / (g - 1)) return LLONG_MAX;
+            v *= (g - 1);
+        }
+        return v;
+    }
+    return g;
+}
+
+static ChainPlan make_plan(const SceneDev& sc, int max_depth, int rays) {
+    ChainPlan pl;
+    const long long G = sc.num_groups;
+    pl.exhaustive_o1 = G <= kOrder1ExhaustiveLimit;
+    pl.exhaustive_mb = true;
+    for (int d = 2; d <= max_depth; ++d)
+        if (seq_count(G, d) > kMultibounceExhaustiveLimit) pl.exhaustive_mb = false;
+    long long off = 0;
+    for (int d = 1; d <= kMaxDepth; ++d) {
+        long long cap = 0;
+        if (d <= max_depth) {
+            if (d == 1) cap = pl.exhaustive_o1 ? G : rays;
+            else cap = pl.exhaustive_mb ? seq_count(G, d) : rays;
+        }
+        pl.cap[d - 1] = cap;
+        pl.offset_int[d - 1] = off;
+        off += cap * d;
+    }
+    return pl;
+}
+
+struct WorkspaceLayout {
+    size_t chain_counts, chain_offsets, chain_groups, chain_planes, chain_images;
+    size_t disc_dirs, disc_groups, disc_keys, disc_keys2, disc_vals, disc_vals2, disc_flags, disc_scan, disc_rank,
+        disc_temp;
+    size_t disc_temp_bytes;
+    size_t edge_flags, edge_list, edge_count;
+    size_t overflow;
+    size_t layers64;
+    size_t total;
+    long long chain_ints_per_tx;
+};
+
+static WorkspaceLayout layout_for(const SceneDev& sc, const wcb_solve_desc& d, const ChainPlan& pl, int rays) {
+    WorkspaceLayout L;
+    const int T = d.num_tx;
+    long long ints = 0;
+    for (int k = 0; k < kMaxDepth; ++k) ints += pl.cap[k] * (k + 1);
+    L.chain_ints_per_tx = ints;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { size_t at = o; o = align_up(o + bytes); return at; };
+    L.chain_counts = take(size_t(T) * kMaxDepth * 4);
+    L.chain_offsets = take(size_t(T) * kMaxDepth * 8);
+    L.chain_groups = take(size_t(T) * ints * 4);
+    L.chain_planes = take(size_t(T) * ints * 4 * 8);
+    L.chain_images = take(size_t(T) * ints * 3 * 8);
+    const bool disc = !(pl.exhaustive_o1 && pl.exhaustive_mb) && (d.components & 2);
+    const size_t nr = disc ? size_t(rays) : 0;
+    const int md = std::max(d.max_depth, 1);
+    L.disc_dirs = take(nr * 3 * 4);
+    L.disc_groups = take(nr * md * 4);
+    L.disc_keys = take(nr * 8);
+    L.disc_keys2 = take(nr * 8);
+    L.disc_vals = take(nr * 4);
+    L.disc_vals2 = take(nr * 4);
+    L.disc_flags = take(nr * 4);
+    L.disc_scan = take(nr * 4);
+    L.disc_rank = take(nr * 4);
+    size_t tb = 0;
+    if (nr) {
+        size_t a = 0, b = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, a, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                        (int*)nullptr, (int*)nullptr, int(nr), 0, 64);
+        cub::DeviceScan::InclusiveSum(nullptr, b, (int*)nullptr, (int*)nullptr, int(nr));
+        tb = std::max(a, b);
+    }
+    L.disc_temp_bytes = tb;
+    L.disc_temp = take(tb);
+    L.edge_flags = take(size_t(std::max(sc.num_edges, 1)) * 4);
+    L.edge_list = take(size_t(T) * std::max(sc.num_edges, 1) * 4);
+    L.edge_count = take(size_t(T) * 4);
+    L.overflow = take(8);
+    L.layers64 = 0;
+    L.total = o;
+    return L;
+}
+
+int solve_workspace_size(const SceneHandle* h, const wcb_solve_desc* d, int64_t* bytes) {
+    const int rays = d->discovery_rays > 0 ? d->discovery_rays : 262144;
+    const ChainPlan pl = make_plan(h->dev, d->max_depth, rays);
+    const WorkspaceLayout L = layout_for(h->dev, *d, pl, rays);
+    *bytes = int64_t(L.total);
+    return 0;
+}
+
+int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m, const wcb_outputs* out, void* ws,
+          int64_t ws_bytes, cudaStream_t stream) {
+    const SceneDev& sc = h->dev;
+    if (d->num_tx < 0 || d->num_freq < 1 || d->max_depth < 0 || d->max_depth > kMaxDepth) return 1;
+    const int rays = d->discovery_rays > 0 ? d->discovery_rays : 262144;
+    const int T = d->num_tx;
+    const int R = d->rx_kind == 1 ? d->grid_rows * d->grid_cols : d->num_rx;
+    if (R < 0) return 1;
+    const ChainPlan pl = make_plan(sc, d->max_depth, rays);
+    const WorkspaceLayout L = layout_for(sc, *d, pl, rays);
+    if (ws_bytes < int64_t(L.total)) return 3;
+    char* base = static_cast<char*>(ws);
+    int* chain_counts = reinterpret_cast<int*>(base + L.chain_counts);
+    long long* chain_offsets = reinterpret_cast<long long*>(base + L.chain_offsets);
+    int* chain_groups = reinterpret_cast<int*>(base + L.chain_groups);
+    double* chain_planes = reinterpret_cast<double*>(base + L.chain_planes);
+    double* chain_images = reinterpret_cast<double*>(base + L.chain_images);
+    int* edge_flags = reinterpret_cast<int*>(base + L.edge_flags);
+    int* edge_list = reinterpret_cast<int*>(base + L.edge_list);
+    int* edge_count = reinterpret_cast<int*>(base + L.edge_count);
+    unsigned long long* overflow = reinterpret_cast<unsigned long long*>(base + L.overflow);
+    const bool fp64 = d->precision == 1;
+    if (T == 0 || R == 0) return 0;
+    cudaMemsetAsync(chain_counts, 0, size_t(T) * kMaxDepth * 4, stream);
+    cudaMemsetAsync(edge_count, 0, size_t(T) * 4, stream);
+    cudaMemsetAsync(overflow, 0, 8, stream);
+    if (out->status) cudaMemsetAsync(out->status, 0, 4, stream);
+    if (out->row_count) cudaMemsetAsync(out->row_count, 0, 8, stream);
+    // chain offsets (in chain-int units, per tx)
+    std::vector<long long> offs(size_t(T) * kMaxDepth);
+    std::vector<int> fixed_counts(size_t(T) * kMaxDepth, 0);
+    for (int t = 0; t < T; ++t)
+        for (int k = 0; k < kMaxDepth; ++k) offs[t * kMaxDepth + k] = t * L.chain_ints_per_tx + pl.offset_int[k];
+    cudaMemcpyAsync(chain_offsets, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, stream);
+    const int B = 256;
+    const size_t smem = size_t(kStackDepth) * kBlock * 4;
+    int* err = out->status;
+    // ---------------- reflection candidates
+    if ((d->components & 2) && sc.num_faces > 0 && d->max_depth >= 1) {
+        const bool need_disc = !(pl.exhaustive_o1 && (d->max_depth < 2 || pl.exhaustive_mb));
+        float* dirs = reinterpret_cast<float*>(base + L.disc_dirs);
+        if (need_disc) {
+            k_fibonacci<<<(rays + B - 1) / B, B, 0, stream>>>(rays, dirs);
+            note_launch();
+        }
+        // exhaustive tables are identical for every tx: generate per tx
+        for (int t = 0; t < T; ++t) {
+            const float* txp = d->tx_pos + 3 * t;
+            if (need_disc) {
+                int* dg = reinterpret_cast<int*>(base + L.disc_groups);
+                const int md = d->max_depth;
+                if (fp64)
+                    k_discovery_trace<double><<<(rays + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, rays, md, dirs, txp, dg, err);
+                else
+                    k_discovery_trace<float><<<(rays + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, rays, md, dirs, txp, dg, err);
+                note_launch();
+                unsigned long long* keys = reinterpret_cast<unsigned long long*>(base + L.disc_keys);
+                unsigned long long* keys2 = reinterpret_cast<unsigned long long*>(base + L.disc_keys2);
+                int* vals = reinterpret_cast<int*>(base + L.disc_vals);
+                int* vals2 = reinterpret_cast<int*>(base + L.disc_vals2);
+                int* flags = reinterpret_cast<int*>(base + L.disc_flags);
+                int* scan = reinterpret_cast<int*>(base + L.disc_scan);
+                int* rank = reinterpret_cast<int*>(base + L.disc_rank);
+                void* temp = base + L.disc_temp;
+                for (int k = 0; k < md; ++k) {
+                    const int depth = k + 1;
+                    const bool use_disc = depth == 1 ? !pl.exhaustive_o1 : !pl.exhaustive_mb;
+                    // ranks are needed for the next depth even when this depth is exhaustive
+                    k_chain_keys<<<(rays + B - 1) / B, B, 0, stream>>>(rays, md, k, dg, rank, keys, vals);
+                    size_t tb = L.disc_temp_bytes;
+                    cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys2, vals, vals2, rays, 0, 64, stream);
+                    k_chain_flags<<<(rays + B - 1) / B, B, 0, stream>>>(rays, keys2, flags);
+                    tb = L.disc_temp_bytes;
+                    cub::DeviceScan::InclusiveSum(temp, tb, flags, scan, rays, stream);
+                    int* cgrp = use_disc ? chain_groups + offs[t * kMaxDepth + k] : nullptr;
+                    int* ccount = use_disc ? chain_counts + t * kMaxDepth + k : nullptr;
+                    k_chain_emit<<<(rays + B - 1) / B, B, 0, stream>>>(rays, md, k, keys2, vals2, flags, scan, dg, rank,
+                                                                       cgrp, use_disc ? int(pl.cap[k]) : 0, ccount);
+                    note_launch(3);
+                }
+            }
+            for (int k = 0; k < d->max_depth; ++k) {
+                const int depth = k + 1;
+                const bool exh = depth == 1 ? pl.exhaustive_o1 : pl.exhaustive_mb;
+                int* cgrp = chain_groups + offs[t * kMaxDepth + k];
+                double* cpl = chain_planes + offs[t * kMaxDepth + k] * 4;
+                double* cim = chain_images + offs[t * kMaxDepth + k] * 3;
+                if (exh) {
+                    const long long total = pl.cap[k];
+                    fixed_counts[t * kMaxDepth + k] = int(total);
+                    if (total > 0) {
+                        k_exhaustive_chains<<<int((total + B - 1) / B), B, 0, stream>>>(total, depth, sc.num_groups, cgrp);
+                        k_chain_images<<<int((total + B - 1) / B), B, 0, stream>>>(sc, txp, depth, nullptr, total, cgrp, cpl, cim);
+                        note_launch(2);
+                    }
+                    cudaMemcpyAsync(chain_counts + t * kMaxDepth + k, &fixed_counts[t * kMaxDepth + k], 4,
+                                    cudaMemcpyHostToDevice, stream);
+                } else {
+                    const long long cap = pl.cap[k];
+                    k_chain_images<<<int((cap + B - 1) / B), B, 0, stream>>>(sc, txp, depth, chain_counts + t * kMaxDepth + k,
+                                                                           0, cgrp, cpl, cim);
+                    note_launch();
+                }
+            }
+        }
+    }
+    // ---------------- diffraction edge prefilter
+    if ((d->components & 4) && sc.num_edges > 0 && d->max_depth >= 1) {
+        const double wavelength = kC0 / d->frequency_hz[0];
+        for (int t = 0; t < T; ++t) {
+            if (fp64)
+                k_edge_flags<double><<<(sc.num_edges + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, d->tx_pos, t, wavelength, edge_flags, err);
+            else
+                k_edge_flags<float><<<(sc.num_edges + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, d->tx_pos, t, wavelength, edge_flags, err);
+            k_compact_flags<<<1, 256, 0, stream>>>(sc.num_edges, edge_flags, edge_list + size_t(t) * sc.num_edges, edge_count + t);
+            note_launch(2);
+        }
+    }
+    // ---------------- main kernel
+    MainParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.sc = sc;
+    p.num_tx = T;
+    p.num_rx = R;
+    p.rx_kind = d->rx_kind;
+    p.rx_pos = d->rx_pos;
+    for (int k = 0; k < 3; ++k) {
+        p.grid_origin[k] = d->grid_origin[k];
+        p.grid_x[k] = d->grid_x_axis[k];
+        p.grid_y[k] = d->grid_y_axis[k];
+    }
+    p.grid_rows = d->grid_rows;
+    p.grid_cols = d->grid_cols;
+    p.grid_spacing[0] = d->grid_spacing[0];
+    p.grid_spacing[1] = d->grid_spacing[1];
+    p.rx_pol = d->rx_pol;
+    p.rx_pol_stride = d->rx_pol_stride;
+    p.tx_pos = d->tx_pos;
+    p.tx_power = d->tx_power;
+    p.tx_pol = d->tx_pol;
+    p.num_materials = m->num_materials;
+    p.mat_eps_r = m->eps_r;
+    p.mat_sigma_e = m->sigma_e;
+    p.mat_mu_r = m->mu_r;
+    p.mat_gain = m->gain;
+    p.mat_thickness = m->thickness;
+    p.mat_volumetric = m->volumetric;
+    p.num_layers = m->num_layers;
+    p.layer_offset = m->layer_offset;
+    p.layer_count = m->layer_count;
+    p.layer_thickness = m->layer_thickness;
+    p.layer_eps_r = m->layer_eps_r;
+    p.layer_sigma_e = m->layer_sigma_e;
+    p.layer_mu_r = m->layer_mu_r;
+    p.components = d->components;
+    p.max_depth = d->max_depth;
+    p.coherent = d->coherent;
+    p.chain_count = chain_counts;
+    p.chain_offset = chain_offsets;
+    p.chain_groups = chain_groups;
+    p.chain_planes = chain_planes;
+    p.chain_images = chain_images;
+    p.edge_count = edge_count;
+    p.edge_list = edge_list;
+    p.out_path_gain = out->path_gain;
+    p.out_field = out->field;
+    p.out_comp_power = out->comp_power;
+    p.out_comp_field = out->comp_field;
+    p.out_diff_vec_power = out->diff_vec_power;
+    p.rows = static_cast<RowRec*>(out->rows);
+    p.row_capacity = out->rows ? out->row_capacity : 0;
+    p.row_counter = reinterpret_cast<unsigned long long*>(out->row_count);
+    p.status = out->status;
+    p.overflow_counter = overflow;
+    p.num_freq_total = d->num_freq;
+    // FP64 mode: double copies of the layer tables
+    double* layers64 = nullptr;
+    if (fp64 && m->num_layers > 0) {
+        const long long n = (long long)m->num_layers * d->num_freq;
+        if (cudaMallocAsync(&layers64, size_t(n) * 4 * 8, stream) != cudaSuccess) return 2;
+        const float* src[4] = {m->layer_thickness, m->layer_eps_r, m->layer_sigma_e, m->layer_mu_r};
+        for (int q = 0; q < 4; ++q) {
+            k_to_double<<<int((n + B - 1) / B), B, 0, stream>>>(n, src[q], layers64 + q * n);
+            note_launch();
+        }
+        p.layer_thickness64 = layers64;
+        p.layer_eps_r64 = layers64 + n;
+        p.layer_sigma_e64 = layers64 + 2 * n;
+        p.layer_mu_r64 = layers64 + 3 * n;
+    }
+    long long threads;
+    if (d->rx_kind == 1) {
+        const long long tiles = (long long)((d->grid_rows + 7) / 8) * ((d->grid_cols + 3) / 4);
+        threads = tiles * 32 * T;
+    } else {
+        threads = (long long)R * T;
+    }
+    const long long blocks = (threads + kBlock - 1) / kBlock;
+    for (int fb = 0; fb < d->num_freq; fb += kMaxNF) {
+        const int nf = std::min(kMaxNF, d->num_freq - fb);
+        p.freq_base = fb;
+        for (int f = 0; f < nf; ++f) {
+            p.freq[f] = d->frequency_hz[fb + f];
+            p.k[f] = kTwoPi * p.freq[f] / kC0;
+        }
+        MainParams q = p;
+        // material tables are addressed relative to this frequency chunk
+        const long long mo = (long long)fb * m->num_materials;
+        q.mat_eps_r = m->eps_r + mo;
+        q.mat_sigma_e = m->sigma_e + mo;
+        q.mat_mu_r = m->mu_r + mo;
+        q.mat_gain = m->gain + mo;
+        q.mat_thickness = m->thickness + mo;
+        const long long lo = (long long)fb * m->num_layers;
+        q.layer_thickness = m->layer_thickness ? m->layer_thickness + lo : nullptr;
+        q.layer_eps_r = m->layer_eps_r ? m->layer_eps_r + lo : nullptr;
+        q.layer_sigma_e = m->layer_sigma_e ? m->layer_sigma_e + lo : nullptr;
+        q.layer_mu_r = m->layer_mu_r ? m->layer_mu_r + lo : nullptr;
+        if (layers64) {
+            q.layer_thickness64 = p.layer_thickness64 + lo;
+            q.layer_eps_r64 = p.layer_eps_r64 + lo;
+            q.layer_sigma_e64 = p.layer_sigma_e64 + lo;
+            q.layer_mu_r64 = p.layer_mu_r64 + lo;
+        }
+        if (fb > 0) q.rows = nullptr;  // geometry rows are emitted once
+        if (blocks > 0) {
+            if (fp64) {
+                switch (nf) {
+                    case 1: k_main<double, 1><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
+                    case 2: k_main<double, 2><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
+                    case 3: k_main<double, 3><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
+                    default: k_main<double, 4><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
+                }
+            } else {
+                switch (nf) {
+                    case 1: k_main<float, 1><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
+                    case 2: k_main<float, 2><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
+                    case 3: k_main<float, 3><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
+                    default: k_main<float, 4><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
+                }
+            }
+            note_launch();
+        }
+    }
+    if (layers64) cudaFreeAsync(layers64, stream);
+    if (cudaGetLastError() != cudaSuccess) return 2;
+    return 0;
+}
+
+int solve_set_smem_limits() {
+    const int smem = kStackDepth * kBlock * 4;
+    cudaFuncSetAttribute(k_main<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return 0;
+}
+
+}  // namespace wcb

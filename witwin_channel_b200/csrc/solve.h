@@ -1,0 +1,92 @@
+// Kernel parameter blocks shared by the solve and row translation units.
+#pragma once
+
+#include <stdint.h>
+
+#include "../../include/witwin_channel_b200.h"
+#include "scene.cuh"
+
+namespace wcb {
+
+// Device layout of wcb_row (48 bytes).
+struct RowRec {
+    int tx;
+    int rx;
+    short component;
+    short depth;
+    int seq[5];
+    int edge;
+    float length;
+    int pad;
+    int pad2;
+};
+static_assert(sizeof(RowRec) == 48, "RowRec must match wcb_row");
+static_assert(sizeof(wcb_row) == 48, "wcb_row must be 48 bytes");
+
+struct MainParams {
+    SceneDev sc;
+    int num_tx, num_rx;
+    int rx_kind;
+    const float* rx_pos;
+    float grid_origin[3], grid_x[3], grid_y[3];
+    int grid_rows, grid_cols;
+    float grid_spacing[2];
+    const float* rx_pol;
+    int rx_pol_stride;
+    const float* tx_pos;
+    const float* tx_power;
+    const float* tx_pol;
+    // frequencies of this launch (chunk of at most four)
+    double freq[4];
+    double k[4];
+    int freq_base;
+    int num_freq_total;
+    // materials (already offset to this chunk's first frequency)
+    int num_materials;
+    const float* mat_eps_r;
+    const float* mat_sigma_e;
+    const float* mat_mu_r;
+    const float* mat_gain;
+    const float* mat_thickness;
+    const int* mat_volumetric;
+    int num_layers;
+    const int* layer_offset;
+    const int* layer_count;
+    const float* layer_thickness;
+    const float* layer_eps_r;
+    const float* layer_sigma_e;
+    const float* layer_mu_r;
+    const double* layer_thickness64;
+    const double* layer_eps_r64;
+    const double* layer_sigma_e64;
+    const double* layer_mu_r64;
+    int components;
+    int max_depth;
+    int coherent;
+    // candidates
+    const int* chain_count;          // (T, 5)
+    const long long* chain_offset;   // (T, 5) in chain-int units
+    const int* chain_groups;
+    const double* chain_planes;
+    const double* chain_images;
+    const int* edge_count;           // (T)
+    const int* edge_list;            // (T, E)
+    // outputs
+    void* out_path_gain;
+    void* out_field;
+    void* out_comp_power;
+    void* out_comp_field;
+    void* out_diff_vec_power;
+    RowRec* rows;
+    long long row_capacity;
+    unsigned long long* row_counter;
+    int* status;
+    unsigned long long* overflow_counter;
+};
+
+struct SceneHandle;
+int solve_workspace_size(const SceneHandle* h, const wcb_solve_desc* d, int64_t* bytes);
+int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m, const wcb_outputs* out, void* ws,
+          int64_t ws_bytes, cudaStream_t stream);
+
+}  // namespace wcb

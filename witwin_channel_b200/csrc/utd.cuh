@@ -1,0 +1,285 @@
+// First-order UTD wedge diffraction (device).
+//
+// The reference computes this in RayD (rayd/diffraction.cpp:405-455), whose
+// source is not shipped.  This is the published Kouyoumjian-Pathak UTD with
+// Luebbers' finite-conductivity face factors and the finite-edge rules the
+// reference documents in docs/dev/audit/utd-continuity-fix-design.md (F1 vector
+// field with unnormalised transverse Tx polarization, F2 1e-4 m distance
+// guard, F3 receiver-angle clamp, F4 biased visibility point, F5e/F5f monotone
+// truncation with the odd/even corner mend, C_BLEND = 0.35).
+//
+// Fresnel integrals C(x) + jS(x) (pi/2 convention) use the power series for
+// |x| < 1.5 and, above, the continued fraction of erfc evaluated with the
+// modified Lentz method (Press et al., Numerical Recipes, section 6.9):
+//   C + jS = (1+j)/2 * (1 - erfc(z)),  z = sqrt(pi)/2 (1-j) x,
+//   erfc(z) = (2z/sqrt(pi)) e^{-z^2} h,  h = 1/(b1 - 2/(b2 - 12/(b3 - ...))),
+//   b_k = 1 - j pi x^2 + 4(k-1),  a_k = -(2k-1)(2k),
+// which gives the complement (1+j)/2 - (C + jS) = x e^{j pi x^2/2} h without
+// cancellation.
+#pragma once
+
+#include "common.cuh"
+#include "em.cuh"
+
+namespace wcb {
+
+constexpr double kCBlend = 0.35;
+constexpr double kGammaScale = 0.1;
+constexpr double kWindowCutoff = 1.0e-3;
+constexpr double kUtdGainFloor = 1.0e-30;
+constexpr double kDiffractionRayBias = 1.0e-4;
+constexpr double kUtdMinDistance = 1.0e-4;
+
+template <typename T>
+struct FresnelPair {
+    Cx<T> value;       // C(x) + jS(x)
+    Cx<T> complement;  // (1+j)/2 - (C(x) + jS(x))
+};
+
+template <typename T>
+WCB_HD FresnelPair<T> fresnel_pos(T x) {
+    FresnelPair<T> out;
+    const Cx<T> half = cx(T(0.5), T(0.5));
+    const T eps = sizeof(T) == 4 ? T(1e-7) : T(1e-15);
+    if (value_of(x) < 1.5) {
+        const T t = T(kPi / 2) * x * x;
+        T sum_c = T(0), sum_s = T(0);
+        T fact = T(1);  // t^k / k!
+        for (int kk = 0; kk < 60; ++kk) {
+            if (kk > 0) fact = fact * t / T(kk);
+            const T term = fact * x / T(2 * kk + 1);
+            const int r = kk & 3;
+            if (r == 0) sum_c = sum_c + term;
+            else if (r == 1) sum_s = sum_s + term;
+            else if (r == 2) sum_c = sum_c - term;
+            else sum_s = sum_s - term;
+            if (kk > 2 && value_of(term) < value_of(eps) * (value_of(sum_c) + value_of(sum_s) + T(1e-30))) break;
+        }
+        out.value = cx(sum_c, sum_s);
+        out.complement = half - out.value;
+        return out;
+    }
+    const Cx<T> b1 = cx(T(1), -T(kPi) * x * x);
+    Cx<T> b = b1;
+    const T big = sizeof(T) == 4 ? T(1e30) : T(1e300);
+    Cx<T> cc = cx(big, T(0));
+    Cx<T> d = cx(T(1), T(0)) / b;
+    Cx<T> h = d;
+    for (int kk = 1; kk < 200; ++kk) {
+        const T a = -T((2 * kk - 1) * (2 * kk));
+        b = b + cx(T(4), T(0));
+        d = cx(T(1), T(0)) / (d * a + b);
+        cc = b + cx(a, T(0)) / cc;
+        const Cx<T> del = cc * d;
+        h = h * del;
+        if (value_of(s_abs(del.re - T(1)) + s_abs(del.im)) < value_of(eps)) break;
+    }
+    const Cx<T> e = cexpj<T>(T(kPi / 2) * x * x);
+    out.complement = e * h * x;
+    out.value = half - out.complement;
+    return out;
+}
+
+template <typename T>
+WCB_HD FresnelPair<T> fresnel(T x) {
+    if (value_of(x) >= 0) return fresnel_pos(x);
+    FresnelPair<T> p = fresnel_pos(-x);
+    // F(-x) = -F(x); complement(-x) = (1+j)/2 + F(x) = (1+j) - complement(x)
+    FresnelPair<T> out;
+    out.value = -p.value;
+    out.complement = cx(T(1), T(1)) - p.complement;
+    return out;
+}
+
+// KP transition function F(x) = 2j sqrt(x) e^{jx} int_{sqrt x}^inf e^{-j t^2} dt, x >= 0.
+template <typename T>
+WCB_HD Cx<T> transition(T x) {
+    if (value_of(x) <= 0) return cx(T(0), T(0));
+    const T u = s_sqrt(T(2) * x / T(kPi));
+    const FresnelPair<T> p = fresnel_pos(u);
+    // int = sqrt(pi/2) * conj(complement); F = 2j sqrt(x) e^{jx} * int
+    const Cx<T> integral = cconj(p.complement) * T(s_sqrt(kPi / 2));
+    const Cx<T> pre = cexpj<T>(x) * (T(2) * s_sqrt(x));
+    return cx(T(0), T(1)) * pre * integral;
+}
+
+// One KP term cot((pi + s*beta)/(2n)) F(kL a^s(beta)) written in the distance
+// eps to the term's own singular point: cot(eps/(2n)) F(2 kL sin^2(eps/2)).
+template <typename T>
+WCB_HD Cx<T> kp_term(T beta, T n, T kl, int s) {
+    const T two_n_pi = T(2) * n * T(kPi);
+    const T arg = T(kPi) + T(s) * beta;
+    const T m = s_round(arg / two_n_pi);
+    const T eps = arg - two_n_pi * m;
+    const T small = sizeof(T) == 4 ? T(1e-5) : T(1e-9);
+    const Cx<T> ej = cx(T(0.70710678118654752440), T(0.70710678118654752440));
+    if (value_of(s_abs(eps)) < value_of(small)) {
+        const T sg = value_of(eps) < 0 ? T(-1) : T(1);
+        const Cx<T> inner = cx(sg * s_sqrt(T(kTwoPi) * kl), T(0)) - ej * (T(2) * kl * eps);
+        return inner * ej * n;
+    }
+    const T half = eps / (T(2) * n);
+    T sh, ch;
+    s_sincos(half, &sh, &ch);
+    const T se = s_sin(eps / T(2));
+    return transition(T(2) * kl * se * se) * (ch / sh);
+}
+
+// Selected diffraction edge (device layout, FP64 geometry).
+struct EdgeDev {
+    double pos[3];     // midpoint
+    double dir[3];     // unit edge direction, oriented so t0 = n0 x dir points into face 0
+    double t0[3];      // unit face-0 tangent
+    double n0[3];      // ordered outward normal of face 0
+    double n1[3];      // ordered outward normal of face n
+    double half_length;
+    double n;          // exterior angle / pi
+    double bisector[3];  // unit exterior bisector used for the visibility bias
+    int face0, face1;    // reference face ids (visibility ignore set)
+    int mat_face0, mat_face1;  // faces whose slab gives R_0 and R_n
+    int edge_id;         // reference edge id
+    int pad;
+};
+
+template <typename T>
+WCB_HD T wedge_angle(V3<T> d, V3<T> t0, V3<T> n0) {
+    T a = s_atan2(dot(d, n0), dot(d, t0));
+    if (value_of(a) < 0) a = a + T(kTwoPi);
+    return a;
+}
+
+template <typename T>
+struct DiffractionResult {
+    bool valid;        // source outside the wedge
+    C3<T> field;       // unit-excitation field at the receiver (phase included)
+    double q[3];       // unclamped stationary point (FP64)
+    double q_vis[3];   // clamped + biased visibility point
+    double length;     // s' + s (FP64)
+};
+
+// Per-frequency face slab lookup callback is provided as two Slab values.
+template <typename T>
+WCB_HD DiffractionResult<T> utd_field(const EdgeDev& ed, V3<double> S, V3<double> R, V3<T> tx_pol, const Slab<T>& m0,
+                                      const Slab<T>& mn, double frequency) {
+    DiffractionResult<T> out;
+    out.valid = false;
+    const double k = kTwoPi * frequency / kC0;
+    const V3<double> c = v3(ed.pos[0], ed.pos[1], ed.pos[2]);
+    const V3<double> e = v3(ed.dir[0], ed.dir[1], ed.dir[2]);
+    const V3<double> t0d = v3(ed.t0[0], ed.t0[1], ed.t0[2]);
+    const V3<double> n0d = v3(ed.n0[0], ed.n0[1], ed.n0[2]);
+    const double n = ed.n;
+    // Keller stationary point (unfolding); FP64
+    const V3<double> ds = S - c;
+    const double ts = dot(ds, e);
+    const V3<double> ps = ds - e * ts;
+    const double rs = length(ps);
+    const V3<double> dr = R - c;
+    const double tr = dot(dr, e);
+    const V3<double> pr = dr - e * tr;
+    const double rr = length(pr);
+    const double t_star = (rs + rr) > 0.0 ? ts + (tr - ts) * rs / (rs + rr) : ts;
+    const V3<double> q = c + e * t_star;
+    const double tc = fmin(fmax(t_star, -ed.half_length), ed.half_length);
+    const V3<double> qv = c + e * tc + v3(ed.bisector[0], ed.bisector[1], ed.bisector[2]) * kDiffractionRayBias;
+    out.q[0] = q.x; out.q[1] = q.y; out.q[2] = q.z;
+    out.q_vis[0] = qv.x; out.q_vis[1] = qv.y; out.q_vis[2] = qv.z;
+    const V3<double> sp_vec = q - S;
+    const V3<double> s_vec = R - q;
+    const double s_p = fmax(length(sp_vec), kUtdMinDistance);
+    const double s = fmax(length(s_vec), kUtdMinDistance);
+    out.length = s_p + s;
+    // angles in the edge frame
+    const T phi_p = wedge_angle(cast3<T>(ps), cast3<T>(t0d), cast3<T>(n0d));
+    T phi = wedge_angle(cast3<T>(pr), cast3<T>(t0d), cast3<T>(n0d));
+    const T nn = T(n);
+    const T npi = nn * T(kPi);
+    if (value_of(phi_p) > value_of(npi)) return out;
+    if (value_of(phi) > value_of(npi)) {
+        phi = (value_of(phi - npi) < value_of(T(kTwoPi) - phi)) ? npi : T(0);
+    }
+    out.valid = true;
+    const V3<T> sh_p = cast3<T>(sp_vec * (1.0 / s_p));
+    const V3<T> sh = cast3<T>(s_vec * (1.0 / s));
+    const V3<T> ef = cast3<T>(e);
+    T cos_b = dot(sh_p, ef);
+    cos_b = s_min(s_max(cos_b, T(-1)), T(1));
+    const T sin_b = s_max(s_sqrt(s_max(T(1) - cos_b * cos_b, T(0))), T(1e-6));
+    const T sT = T(s), spT = T(s_p);
+    const T kT = T(k);
+    const T kl = kT * sT * spT * sin_b * sin_b / (sT + spT);
+    // finite-edge truncation
+    const T rho_p = spT * sin_b;
+    const T rho = sT * sin_b;
+    const T kappa = rho_p * rho_p / (spT * spT * spT) + rho * rho / (sT * sT * sT);
+    const T sigma = s_sqrt(kT * kappa / T(kPi));
+    const T tsT = T(t_star);
+    const T tmax = T(ed.half_length), tmin = -T(ed.half_length);
+    const FresnelPair<T> hi = fresnel(sigma * (tmax - tsT));
+    const FresnelPair<T> lo = fresnel(-(sigma * (tmin - tsT)));
+    const T inv_sqrt2 = T(0.70710678118654752440);
+    const T t_mono = s_min(s_max(T(1) - inv_sqrt2 * cabs(lo.complement) - inv_sqrt2 * cabs(hi.complement), T(0)), T(1));
+    T u;
+    if (value_of(s_abs(tsT - tmax)) < value_of(s_abs(tsT - tmin))) u = sigma * (tsT - tmax);
+    else u = sigma * (tmin - tsT);
+    const T gamma = T(1) / (T(1) + s_exp(s_min(u / T(kGammaScale), T(80))));
+    const T unit = s_sqrt(T(kTwoPi) / kl);
+    const T delta_w = T(4) * unit;
+    const T delta_b = T(kCBlend) * unit;
+    // face factors
+    const T wavelength = T(kC0 / frequency);
+    Cx<T> r0_te, r0_tm, rn_te, rn_tm;
+    slab_fresnel(s_sin(phi_p), m0, frequency, wavelength, &r0_te, &r0_tm);
+    slab_fresnel(s_sin(npi - phi), mn, frequency, wavelength, &rn_te, &rn_tm);
+    const T bm = phi - phi_p;
+    const T bp = phi + phi_p;
+    auto mended = [&](T beta, int sgn, bool incident_group) -> Cx<T> {
+        const Cx<T> value = kp_term(beta, nn, kl, sgn);
+        T b_star;
+        if (incident_group) {
+            b_star = value_of(s_abs(beta - T(kPi))) <= value_of(s_abs(beta + T(kPi))) ? T(kPi) : T(-kPi);
+        } else {
+            const T other = (T(2) * nn - T(1)) * T(kPi);
+            b_star = value_of(s_abs(beta - T(kPi))) <= value_of(s_abs(beta - other)) ? T(kPi) : other;
+        }
+        const T delta = beta - b_star;
+        const T rw = delta / delta_w;
+        T w = s_exp(-rw * rw);
+        if (value_of(w) <= kWindowCutoff) w = T(0);
+        const Cx<T> mirrored = kp_term(T(2) * b_star - beta, nn, kl, sgn);
+        const Cx<T> odd = (value - mirrored) * (T(0.5) * w);
+        const T rb = delta / delta_b;
+        const T wb = s_exp(-rb * rb);
+        const T blend = wb + (T(1) - wb) * t_mono;
+        return (value - odd) * t_mono + odd * (gamma * blend);
+    };
+    const Cx<T> t1 = mended(bm, +1, true);
+    const Cx<T> t2 = mended(bm, -1, true);
+    const Cx<T> t3 = mended(bp, +1, false);
+    const Cx<T> t4 = mended(bp, -1, false);
+    // pre = -exp(-j pi/4) / (2 n sqrt(2 pi k) sin_b)
+    const T pre_mag = T(1) / (T(2) * nn * s_sqrt(T(kTwoPi) * kT) * sin_b);
+    const Cx<T> pre = cx(-inv_sqrt2 * pre_mag, inv_sqrt2 * pre_mag);
+    const Cx<T> inc = t1 + t2;
+    const Cx<T> d_soft = pre * (inc + rn_te * t3 + r0_te * t4);
+    const Cx<T> d_hard = pre * (inc + rn_tm * t3 + r0_tm * t4);
+    // ray-fixed bases
+    V3<T> phi_hat_p = cross(ef, sh_p);
+    phi_hat_p = phi_hat_p * (T(1) / s_max(length(phi_hat_p), T(1e-12)));
+    const V3<T> beta_hat_p = cross(sh_p, phi_hat_p);
+    V3<T> phi_hat = cross(ef, sh);
+    phi_hat = phi_hat * (T(1) / s_max(length(phi_hat), T(1e-12)));
+    const V3<T> beta_hat = cross(sh, phi_hat);
+    const V3<T> tx_axis = transverse(sh_p, tx_pol);
+    const T inc_amp = T(1) / (T(2) * kT * spT);
+    const T e_beta = dot(tx_axis, beta_hat_p) * inc_amp;
+    const T e_phi = dot(tx_axis, phi_hat_p) * inc_amp;
+    const T spread = s_sqrt(spT / (sT * (spT + sT)));
+    const Cx<T> ph = phasor_neg_kd<T>(k, s_p + s);
+    const Cx<T> cb = -(d_soft * (e_beta * spread)) * ph;
+    const Cx<T> cf = -(d_hard * (e_phi * spread)) * ph;
+    out.field = c3_axis(beta_hat, cb) + c3_axis(phi_hat, cf);
+    return out;
+}
+
+}  // namespace wcb

@@ -1,0 +1,278 @@
+"""Minimal logical scene model for the deterministic solver.
+
+The reference takes its scene objects from ``witwin.core`` (``witwin==0.4.0``),
+which is a separate package.  This module defines the subset of that model the
+deterministic path reads, duck-type compatible with it, so that user code
+written against ``witwin.core`` (``Scene``, ``Structure``, ``Mesh``,
+``PhysicalMaterial``, ``MaterialLayer``, ``AntennaState``, ``ReceiverGrid``)
+keeps working.  Field usage follows the reference's fixtures
+(``tests/support/core_world.py:9-75``, ``tests/support/scenes.py``) and its
+compiler (``witwin/channel/scene/compiler.py:967-1035``).
+
+Material parameters may be Python floats, callables of the frequency in Hz
+(dispersive ITU-style laws), or 0-d torch tensors; a tensor that requires
+grad receives a gradient from a ``vjp`` solve.
+"""
+
+from __future__ import annotations
+
+import itertools
+from dataclasses import dataclass, field
+from typing import Any, Callable, Sequence
+
+import torch
+
+_ids = itertools.count(1)
+
+
+def new_antenna_id() -> int:
+    return next(_ids)
+
+
+MaterialValue = float | torch.Tensor | Callable[[float], float]
+
+
+def evaluate_material_value(value: MaterialValue, frequency_hz: float) -> Any:
+    """Return a float or a 0-d tensor for a material parameter at ``frequency_hz``."""
+
+    if callable(value) and not isinstance(value, torch.Tensor):
+        return value(frequency_hz)
+    return value
+
+
+@dataclass(frozen=True)
+class MaterialLayer:
+    """One physical layer of a thin-sheet stack (entry side first)."""
+
+    thickness_m: MaterialValue
+    eps_r: MaterialValue
+    sigma_e: MaterialValue = 0.0
+    mu_r: MaterialValue = 1.0
+
+
+_GEOMETRY_MODES = ("thin_sheet", "volumetric")
+
+
+@dataclass(frozen=True)
+class PhysicalMaterial:
+    """Per-structure electromagnetic material.
+
+    Without explicit ``layers`` the material is one layer of
+    ``(thickness_m, eps_r, sigma_e, mu_r)``; with layers, the first layer is the
+    scalar Fresnel view used by reflection and the whole stack is used by
+    transmission (``witwin/channel/scene/compiler.py:967-1035``).
+    """
+
+    eps_r: MaterialValue = 1.0
+    sigma_e: MaterialValue = 0.0
+    mu_r: MaterialValue = 1.0
+    gain: MaterialValue = 1.0
+    thickness_m: MaterialValue = 0.2
+    layers: tuple[MaterialLayer, ...] = ()
+    conductor_model: str | None = None
+    geometry_mode: str = "thin_sheet"
+    name: str = ""
+
+    def __post_init__(self) -> None:
+        if self.geometry_mode not in _GEOMETRY_MODES:
+            raise ValueError(f"geometry_mode must be one of {_GEOMETRY_MODES}")
+
+    @classmethod
+    def perfect_conductor(cls, *, thickness_m: float = 0.2, name: str = "pec") -> "PhysicalMaterial":
+        return cls(eps_r=1.0, sigma_e=0.0, conductor_model="perfect", thickness_m=thickness_m, name=name)
+
+    def stack(self) -> tuple[MaterialLayer, ...]:
+        if self.layers:
+            return tuple(self.layers)
+        return (
+            MaterialLayer(
+                thickness_m=self.thickness_m,
+                eps_r=self.eps_r,
+                sigma_e=self.sigma_e,
+                mu_r=self.mu_r,
+            ),
+        )
+
+
+@dataclass
+class Mesh:
+    vertices: torch.Tensor
+    faces: torch.Tensor
+
+    def __post_init__(self) -> None:
+        if not isinstance(self.vertices, torch.Tensor):
+            self.vertices = torch.as_tensor(self.vertices, dtype=torch.float32)
+        if not isinstance(self.faces, torch.Tensor):
+            self.faces = torch.as_tensor(self.faces, dtype=torch.int64)
+        if self.vertices.ndim != 2 or self.vertices.shape[-1] != 3:
+            raise ValueError("vertices must have shape (V, 3)")
+        if self.faces.ndim != 2 or self.faces.shape[-1] != 3:
+            raise ValueError("faces must have shape (F, 3)")
+
+
+class Structure:
+    """A triangle mesh with one material.  ``surface_id`` keys coplanar grouping."""
+
+    def __init__(
+        self,
+        geometry: Mesh | None = None,
+        material: PhysicalMaterial | None = None,
+        *,
+        vertices: torch.Tensor | None = None,
+        faces: torch.Tensor | None = None,
+        surface_id: int | None = None,
+        name: str = "",
+        **_: Any,
+    ) -> None:
+        if geometry is None:
+            if vertices is None or faces is None:
+                raise ValueError("Structure needs a Mesh or vertices and faces")
+            geometry = Mesh(vertices, faces)
+        if material is None:
+            raise ValueError("Structure needs a material")
+        self.geometry = geometry
+        self.material = material
+        self.surface_id = surface_id
+        self.name = name
+
+    @property
+    def vertices(self) -> torch.Tensor:
+        return self.geometry.vertices
+
+    @property
+    def faces(self) -> torch.Tensor:
+        return self.geometry.faces
+
+
+def _vec3(value: Any) -> torch.Tensor:
+    if isinstance(value, torch.Tensor):
+        return value.reshape(3)
+    return torch.tensor(tuple(float(v) for v in value), dtype=torch.float32)
+
+
+class AntennaState:
+    """A transmitter (``role="tx"``) or point receiver (``role="rx"``)."""
+
+    def __init__(
+        self,
+        id: int,
+        role: str,
+        position: Any,
+        *,
+        polarization: Any = None,
+        power_w: float | torch.Tensor = 1.0,
+        **_: Any,
+    ) -> None:
+        if role not in ("tx", "rx"):
+            raise ValueError("role must be 'tx' or 'rx'")
+        self.id = id
+        self.role = role
+        self.position = _vec3(position)
+        self.polarization = (
+            torch.tensor((0.0, 0.0, 1.0)) if polarization is None else _vec3(polarization)
+        )
+        self.power_w = 1.0 if power_w is None else power_w
+
+
+ReceiverPoint = AntennaState
+
+
+class ReceiverGrid:
+    """A planar receiver grid.
+
+    Point ``(row, col)`` sits at ``origin + x_axis*row*spacing[0] +
+    y_axis*col*spacing[1]``; results come back as ``(T, shape[1], shape[0])``
+    (``witwin/channel/propagation/geometry.py:71-89``; ``los.cu:391-420``).
+    """
+
+    role = "rx"
+
+    def __init__(
+        self,
+        id: int,
+        origin: Any,
+        x_axis: Any,
+        y_axis: Any,
+        shape: Sequence[int],
+        spacing: Sequence[float],
+        *,
+        polarization: Any = None,
+        **_: Any,
+    ) -> None:
+        rows, cols = (int(shape[0]), int(shape[1]))
+        if rows < 0 or cols < 0:
+            raise ValueError("shape entries must be non-negative")
+        if float(spacing[0]) <= 0.0 or float(spacing[1]) <= 0.0:
+            raise ValueError("spacing entries must be positive")
+        self.id = id
+        self.origin = _vec3(origin)
+        self.x_axis = _vec3(x_axis)
+        self.y_axis = _vec3(y_axis)
+        self.shape = (rows, cols)
+        self.spacing = (float(spacing[0]), float(spacing[1]))
+        self.polarization = (
+            torch.tensor((0.0, 0.0, 1.0)) if polarization is None else _vec3(polarization)
+        )
+        self.position = self.origin
+
+    @property
+    def count(self) -> int:
+        return self.shape[0] * self.shape[1]
+
+    def points(self) -> torch.Tensor:
+        """Grid points in float32, row-major over ``(row, col)``."""
+
+        rows, cols = self.shape
+        r = torch.arange(rows, dtype=torch.float32).repeat_interleave(cols) * self.spacing[0]
+        c = torch.arange(cols, dtype=torch.float32).repeat(rows) * self.spacing[1]
+        o = self.origin.detach().float()
+        return o[None, :] + self.x_axis.float()[None, :] * r[:, None] + self.y_axis.float()[None, :] * c[:, None]
+
+
+@dataclass
+class Scene:
+    structures: list[Structure] = field(default_factory=list)
+    endpoints: list[Any] = field(default_factory=list)
+    metadata: dict[str, Any] = field(default_factory=dict)
+    versions: Any = None
+
+    @property
+    def transmitters(self) -> list[AntennaState]:
+        return [e for e in self.endpoints if getattr(e, "role", None) == "tx"]
+
+    @property
+    def receivers(self) -> list[Any]:
+        return [e for e in self.endpoints if getattr(e, "role", None) == "rx"]
+
+
+def make_transmitter(position: Any, *, polarization: Any = None, power_w: float = 1.0, **kw: Any) -> AntennaState:
+    return AntennaState(new_antenna_id(), "tx", position, polarization=polarization, power_w=power_w)
+
+
+def make_receiver(position: Any, *, polarization: Any = None, **kw: Any) -> AntennaState:
+    return AntennaState(new_antenna_id(), "rx", position, polarization=polarization)
+
+
+def make_receiver_grid(*, origin: Any, x_axis: Any, y_axis: Any, shape: Sequence[int], spacing: Sequence[float], polarization: Any = None, **kw: Any) -> ReceiverGrid:
+    return ReceiverGrid(new_antenna_id(), origin, x_axis, y_axis, shape, spacing, polarization=polarization)
+
+
+def make_mesh_structure(*, vertices: Any, faces: Any, material: PhysicalMaterial, surface_id: int | None = None, name: str = "", **kw: Any) -> Structure:
+    return Structure(Mesh(vertices, faces), material, surface_id=surface_id, name=name)
+
+
+__all__ = [
+    "AntennaState",
+    "MaterialLayer",
+    "Mesh",
+    "PhysicalMaterial",
+    "ReceiverGrid",
+    "ReceiverPoint",
+    "Scene",
+    "Structure",
+    "evaluate_material_value",
+    "make_mesh_structure",
+    "make_receiver",
+    "make_receiver_grid",
+    "make_transmitter",
+]
