@@ -211,8 +211,25 @@ int wcb_field_reflection_sequence(int64_t n, int32_t depth, const float* source,
                                   const float* thickness, double frequency_hz, float* field_vector,
                                   float* coefficient, float* path_field, float* path_gain, float* path_length,
                                   float* delay, float* direction, void* stream);
+/* Straight thin-sheet chain: normals (N,D,3), material ids (N,D) i32 and
+ * per-row wall count (N) i32; materials as in wcb_materials (NF = 1). */
+int wcb_field_transmission_sequence(int64_t n, int32_t depth, const float* source, const float* target,
+                                    const float* normals, const int32_t* material_ids, const int32_t* wall_count,
+                                    const float* tx_power, const float* tx_pol, const float* rx_pol,
+                                    const wcb_materials* materials, double frequency_hz, float* field_vector,
+                                    float* coefficient, float* path_field, float* path_gain, float* path_length,
+                                    float* delay, float* direction, void* stream);
 int wcb_field_project_complex3(int64_t n, const float* field_vector, const float* direction, const float* rx_pol,
                                float* coefficient, float* path_gain, void* stream);
+
+/* Measurement: when enabled, wcb_solve brackets its candidate preparation and
+ * its main kernel with CUDA events on the solve stream and counts the rays
+ * (segment visibility / penetration queries) the main kernel traces.
+ * wcb_profile_read returns the last solve's figures: values[0] main-kernel ms,
+ * values[1] preparation ms, values[2] main-kernel rays, values[3] main-kernel
+ * launches, values[4] preparation rays (discovery bounces, edge prefilter). */
+int wcb_profile_enable(int32_t enabled);
+int wcb_profile_read(double* values);
 
 /* Runtime info: writes a NUL-terminated description (architecture, build). */
 int wcb_build_info(char* buffer, int64_t capacity);

@@ -14,6 +14,9 @@ BARY_EPS = 1.0e-7
 SEGMENT_T_EPS = 1.0e-6
 EDGE_PLANE_TOL = 1.34e-5  # propagation/geometry.py:37 (_RAYD_EDGE_INFO_PLANE_TOL)
 ENDPOINT_QUANTIZATION = 1.0e-4  # scene/resources.py:296
+
+# Rays traced (segment queries and discovery bounces), for throughput figures.
+RAY_COUNTER = [0]
 NORMAL_COS_TOL = 1.0 - 1.0e-5  # scene/resources.py:297
 
 
@@ -294,6 +297,7 @@ def segment_blocked(tris: Triangles, p0: np.ndarray, p1: np.ndarray, ignore: np.
     """True where segment p0->p1 hits a triangle at ``t`` in
     ``[SEGMENT_T_EPS, 1 - SEGMENT_T_EPS]``; ``ignore`` is an ``(N, F)`` bool mask."""
     out = np.zeros(p0.shape[0], dtype=bool)
+    RAY_COUNTER[0] += int(p0.shape[0])
     for s in range(0, p0.shape[0], chunk):
         e = min(s + chunk, p0.shape[0])
         t = tris.intersect(p0[s:e], p1[s:e] - p0[s:e])
@@ -307,6 +311,7 @@ def segment_hits(tris: Triangles, p0: np.ndarray, p1: np.ndarray, groups: np.nda
                  ) -> list[list[tuple[float, int]]]:
     """All hits ``(t, face)`` per segment, ascending in ``t``."""
     t = tris.intersect(p0, p1 - p0)
+    RAY_COUNTER[0] += int(p0.shape[0])
     out = []
     for row in t:
         idx = np.nonzero((row >= SEGMENT_T_EPS) & (row <= 1.0 - SEGMENT_T_EPS))[0]
@@ -406,6 +411,7 @@ def trace_reflections(tris: Triangles, normals: np.ndarray, origin: np.ndarray, 
         last = np.full(e - s, -1, dtype=np.int64)
         alive = np.ones(e - s, dtype=bool)
         for depth in range(max_depth):
+            RAY_COUNTER[0] += int(alive.sum())
             t = tris.intersect(o, d)
             rows = np.arange(e - s)
             t[rows[last >= 0], last[last >= 0]] = np.inf

@@ -167,9 +167,31 @@ def _exhaustive_chains(g: int, d: int) -> list[tuple[int, ...]]:
     return out
 
 
+def discover(arrays: dict, *, max_depth: int, discovery_rays: int = DISCOVERY_RAYS) -> list | None:
+    """Per-transmitter discovered group chains (``interactions/reflection.py:541-569``),
+    or ``None`` when the exhaustive plan applies at every depth."""
+    V, Fc = arrays["vertices"], arrays["faces"]
+    if Fc.shape[0] == 0 or max_depth < 1:
+        return None
+    groups = geom.coplanar_groups(V[Fc[:, 0]], geom.face_normals_f32(V, Fc), arrays["face_surface"])
+    G = groups["group_count"]
+    need = G > ORDER1_EXHAUSTIVE_GROUP_LIMIT or (max_depth >= 2 and not all(
+        _face_sequence_count(G, d) <= MAX_MULTIBOUNCE_FACE_SEQUENCES for d in range(2, max_depth + 1)))
+    if not need:
+        return None
+    tris = geom.Triangles(V, Fc)
+    normals = geom.face_normals(V, Fc)
+    dirs = geom.fibonacci_directions(discovery_rays)
+    out = []
+    for t in range(arrays["tx_pos"].shape[0]):
+        prims = geom.trace_reflections(tris, normals, arrays["tx_pos"][t], dirs, max(max_depth, 1))
+        out.append(np.where(prims >= 0, groups["face_group_id"][np.maximum(prims, 0)], -1))
+    return out
+
+
 def solve(arrays: dict, *, components, max_depth: int, coherent: bool = True, max_paths=None,
           max_paths_scope: str = "global", frequency: float, discovery_rays: int = DISCOVERY_RAYS,
-          edge_policy=None) -> dict:
+          edge_policy=None, discovered: list | None = None) -> dict:
     V, Fc = arrays["vertices"], arrays["faces"]
     fm = arrays["face_mats"]
     tx_pos, tx_pow, tx_pol = arrays["tx_pos"], arrays["tx_power"], arrays["tx_pol"]
@@ -198,6 +220,7 @@ def solve(arrays: dict, *, components, max_depth: int, coherent: bool = True, ma
                          length=float(np.linalg.norm(rx_pos[r] - tx_pos[t])))
 
     # ---- reflection --------------------------------------------------------
+    discovered_all = discovered
     if "reflection" in components and max_depth >= 1 and has_struct and R > 0:
         G = groups["group_count"]
         face_group = groups["face_group_id"]
@@ -209,9 +232,12 @@ def solve(arrays: dict, *, components, max_depth: int, coherent: bool = True, ma
                 _face_sequence_count(G, d) <= MAX_MULTIBOUNCE_FACE_SEQUENCES for d in range(2, max_depth + 1))
             chain_sets = {}
             if need_disc_o1 or need_disc_mb:
-                dirs = geom.fibonacci_directions(discovery_rays)
-                prims = geom.trace_reflections(tris, normals, S, dirs, max(max_depth, 1))
-                discovered = np.where(prims >= 0, face_group[np.maximum(prims, 0)], -1)
+                if discovered_all is not None:
+                    discovered = discovered_all[t]
+                else:
+                    dirs = geom.fibonacci_directions(discovery_rays)
+                    prims = geom.trace_reflections(tris, normals, S, dirs, max(max_depth, 1))
+                    discovered = np.where(prims >= 0, face_group[np.maximum(prims, 0)], -1)
             if need_disc_o1:
                 firsts = np.unique(discovered[discovered[:, 0] >= 0, 0])
                 chain_sets[1] = [(int(g),) for g in firsts]

@@ -129,7 +129,10 @@ EXPORTED_SYMBOLS = (
     "wcb_rows_accumulate",
     "wcb_field_free_space",
     "wcb_field_reflection_sequence",
+    "wcb_field_transmission_sequence",
     "wcb_field_project_complex3",
+    "wcb_profile_enable",
+    "wcb_profile_read",
     "wcb_build_info",
     "wcb_launch_count",
 )
@@ -172,7 +175,11 @@ def load() -> ctypes.CDLL:
                                         ctypes.c_int32, ctypes.POINTER(Outputs), _vp]
     lib.wcb_field_free_space.argtypes = [ctypes.c_int64] + [_vp] * 5 + [ctypes.c_double] + [_vp] * 7 + [_vp]
     lib.wcb_field_reflection_sequence.argtypes = [ctypes.c_int64, ctypes.c_int32] + [_vp] * 12 + [ctypes.c_double] + [_vp] * 7 + [_vp]
+    lib.wcb_field_transmission_sequence.argtypes = [ctypes.c_int64, ctypes.c_int32] + [_vp] * 8 + [
+        ctypes.POINTER(Materials), ctypes.c_double] + [_vp] * 7 + [_vp]
     lib.wcb_field_project_complex3.argtypes = [ctypes.c_int64] + [_vp] * 5 + [_vp]
+    lib.wcb_profile_enable.argtypes = [ctypes.c_int32]
+    lib.wcb_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double)]
     lib.wcb_build_info.argtypes = [ctypes.c_char_p, ctypes.c_int64]
     lib.wcb_launch_count.restype = ctypes.c_int64
     for name in EXPORTED_SYMBOLS:
@@ -215,6 +222,17 @@ def stream_handle(device: torch.device | None = None) -> int:
 
 def launch_count() -> int:
     return int(load().wcb_launch_count())
+
+
+def profile_enable(enabled: bool) -> None:
+    check(load().wcb_profile_enable(int(bool(enabled))), "wcb_profile_enable")
+
+
+def profile_read() -> dict:
+    vals = (ctypes.c_double * 5)()
+    check(load().wcb_profile_read(vals), "wcb_profile_read")
+    return {"main_ms": vals[0], "prep_ms": vals[1], "rays": int(vals[2]), "main_launches": int(vals[3]),
+            "prep_rays": int(vals[4])}
 
 
 def build_info() -> str:

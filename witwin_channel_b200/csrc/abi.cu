@@ -156,9 +156,37 @@ int wcb_field_reflection_sequence(int64_t n, int32_t depth, const float* source,
                                  path_length, delay, direction, as_stream(stream));
 }
 
+int wcb_field_transmission_sequence(int64_t n, int32_t depth, const float* source, const float* target,
+                                    const float* normals, const int32_t* material_ids, const int32_t* wall_count,
+                                    const float* tx_power, const float* tx_pol, const float* rx_pol,
+                                    const wcb_materials* materials, double frequency_hz, float* field_vector,
+                                    float* coefficient, float* path_field, float* path_gain, float* path_length,
+                                    float* delay, float* direction, void* stream) {
+    if (!(frequency_hz > 0.0) || materials == nullptr) return WCB_ERR_INVALID_ARGUMENT;
+    return wcb::field_transmission(n, depth, source, target, normals, material_ids, wall_count, tx_power, tx_pol,
+                                   rx_pol, materials, frequency_hz, field_vector, coefficient, path_field, path_gain,
+                                   path_length, delay, direction, as_stream(stream));
+}
+
 int wcb_field_project_complex3(int64_t n, const float* field_vector, const float* direction, const float* rx_pol,
                                float* coefficient, float* path_gain, void* stream) {
     return wcb::field_project(n, field_vector, direction, rx_pol, coefficient, path_gain, as_stream(stream));
+}
+
+int wcb_profile_enable(int32_t enabled) {
+    wcb::profile_state().enabled = enabled != 0;
+    return WCB_OK;
+}
+
+int wcb_profile_read(double* values) {
+    if (values == nullptr) return WCB_ERR_INVALID_ARGUMENT;
+    const wcb::ProfileState& st = wcb::profile_state();
+    values[0] = st.main_ms;
+    values[1] = st.prep_ms;
+    values[2] = double(st.rays);
+    values[3] = double(st.main_launches);
+    values[4] = double(st.prep_rays);
+    return WCB_OK;
 }
 
 int wcb_build_info(char* buffer, int64_t capacity) {

@@ -148,14 +148,20 @@ WCB_HD Cx<T> operator/(Cx<T> a, Cx<T> b) {
     T den = b.re * r + b.im;
     return {(a.re * r + a.im) / den, (a.im * r - a.re) / den};
 }
-// principal square root (branch cut on the negative real axis)
+// principal square root (branch cut on the negative real axis).  The
+// component computed from (|z| +- Re z)/2 is the one without cancellation;
+// the other follows from Im z = 2 Re(w) Im(w).
 template <typename T>
 WCB_HD Cx<T> csqrt(Cx<T> z) {
-    T m = cabs(z);
-    T re = s_sqrt(s_max(T(0), T(0.5) * (m + z.re)));
-    T im = s_sqrt(s_max(T(0), T(0.5) * (m - z.re)));
+    const T m = cabs(z);
+    if (value_of(m) == 0) return {T(0), T(0)};
+    if (value_of(z.re) >= 0) {
+        const T re = s_sqrt(T(0.5) * (m + z.re));
+        return {re, z.im / (T(2) * re)};
+    }
+    T im = s_sqrt(T(0.5) * (m - z.re));
     if (value_of(z.im) < 0) im = -im;
-    return {re, im};
+    return {z.im / (T(2) * im), im};
 }
 template <typename T>
 WCB_HD Cx<T> cexp(Cx<T> z) {

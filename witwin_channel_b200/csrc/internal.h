@@ -41,6 +41,10 @@ int field_reflection(int64_t n, int depth, const float* s, const float* t, const
                      const float* tp, const float* rp, const float* eps, const float* sig, const float* mu, const float* gain,
                      const float* th, double f, float* fv, float* c, float* pf, float* pg, float* pl, float* dl, float* dr,
                      cudaStream_t stream);
+int field_transmission(int64_t n, int depth, const float* s, const float* t, const float* nrm, const int* mids,
+                       const int* counts, const float* pw, const float* tp, const float* rp, const wcb_materials* m,
+                       double f, float* fv, float* c, float* pf, float* pg, float* pl, float* dl, float* dr,
+                       cudaStream_t stream);
 int field_project(int64_t n, const float* fv, const float* dir, const float* rp, float* c, float* pg, cudaStream_t stream);
 
 extern std::atomic<long long> g_launch_count;

@@ -566,6 +566,39 @@ __global__ void k_field_reflection(long long n, int depth, const float* src, con
     if (dirout) { dirout[3 * i] = fdir.x; dirout[3 * i + 1] = fdir.y; dirout[3 * i + 2] = fdir.z; }
 }
 
+__global__ void k_field_transmission(long long n, int depth, const float* src, const float* tgt, const float* nrm,
+                                     const int* mids, const int* counts, const float* pw, const float* tpol,
+                                     const float* rpol, LayerTable<float> lt, double freq, float* fv, float* coef,
+                                     float* pf, float* pg, float* plen, float* delay, float* dirout) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const V3<double> S = v3<double>(src[3 * i], src[3 * i + 1], src[3 * i + 2]);
+    const V3<double> R = v3<double>(tgt[3 * i], tgt[3 * i + 1], tgt[3 * i + 2]);
+    const double k = kTwoPi * freq / kC0;
+    const double dist = length(R - S);
+    const V3<float> dir = safe_normalize(cast3<float>(R) - cast3<float>(S), v3(0.f, 0.f, 1.f));
+    C3<float> value = c3_from_real(transverse(dir, v3(tpol[3 * i], tpol[3 * i + 1], tpol[3 * i + 2])));
+    float shorten = 0.f;
+    const int cnt = counts[i] < depth ? counts[i] : depth;
+    for (int w = 0; w < cnt; ++w) {
+        const float* nn = nrm + (i * depth + w) * 3;
+        transmit_wall(value, shorten, dir, v3(nn[0], nn[1], nn[2]), mids[i * depth + w], lt, freq);
+    }
+    const float amp = 1.0f / (2.0f * float(k) * float(fmax(dist, kUtdEps)));
+    value = c3_scale(value, phasor_neg_kd<float>(k, dist - double(shorten)) * amp);
+    const Cx<float> c = project_receiver(value, dir, v3(rpol[3 * i], rpol[3 * i + 1], rpol[3 * i + 2]));
+    const Cx<float> p = c * sqrtf(fmaxf(pw[i], 0.f));
+    store_c(fv, 3 * i, value.x);
+    store_c(fv, 3 * i + 1, value.y);
+    store_c(fv, 3 * i + 2, value.z);
+    store_c(coef, i, c);
+    store_c(pf, i, p);
+    if (pg) pg[i] = cabs2(p);
+    if (plen) plen[i] = float(dist);
+    if (delay) delay[i] = float(dist / kC0);
+    if (dirout) { dirout[3 * i] = dir.x; dirout[3 * i + 1] = dir.y; dirout[3 * i + 2] = dir.z; }
+}
+
 __global__ void k_field_project(long long n, const float* fv, const float* dir, const float* rpol, float* coef, float* pg) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -657,6 +690,20 @@ int field_reflection(int64_t n, int depth, const float* s, const float* t, const
     if (depth < 1 || depth > kMaxDepth) return 1;
     k_field_reflection<<<int((n + kB - 1) / kB), kB, 0, stream>>>(n, depth, s, t, pos, nrm, pw, tp, rp, eps, sig, mu, gain, th,
                                                                    f, fv, c, pf, pg, pl, dl, dr);
+    note_launch();
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int field_transmission(int64_t n, int depth, const float* s, const float* t, const float* nrm, const int* mids,
+                       const int* counts, const float* pw, const float* tp, const float* rp, const wcb_materials* m,
+                       double f, float* fv, float* c, float* pf, float* pg, float* pl, float* dl, float* dr,
+                       cudaStream_t stream) {
+    if (n <= 0) return 0;
+    if (depth < 1 || depth > kMaxDepth) return 1;
+    const LayerTable<float> lt{m->layer_offset, m->layer_count, m->layer_thickness, m->layer_eps_r, m->layer_sigma_e,
+                               m->layer_mu_r};
+    k_field_transmission<<<int((n + kB - 1) / kB), kB, 0, stream>>>(n, depth, s, t, nrm, mids, counts, pw, tp, rp, lt, f,
+                                                                     fv, c, pf, pg, pl, dl, dr);
     note_launch();
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }

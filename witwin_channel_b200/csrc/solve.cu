@@ -54,7 +54,8 @@ __global__ void k_fibonacci(int count, float* dirs) {
 
 template <typename G>
 __global__ void __launch_bounds__(kBlock) k_discovery_trace(SceneDev sc, int count, int depth, const float* dirs,
-                                                            const float* tx, int* groups_out, int* err) {
+                                                            const float* tx, int* groups_out, int* err,
+                                                            unsigned long long* ray_counter) {
     extern __shared__ int stack[];
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
@@ -62,9 +63,11 @@ __global__ void __launch_bounds__(kBlock) k_discovery_trace(SceneDev sc, int cou
     V3<G> d = v3<G>(G(dirs[3 * i]), G(dirs[3 * i + 1]), G(dirs[3 * i + 2]));
     int last = -1;
     bool alive = true;
+    unsigned long long traced = 0;
     for (int k = 0; k < depth; ++k) {
         int hit_group = -1;
         if (alive) {
+            ++traced;
             const G inf = sizeof(G) == 4 ? G(3e38) : G(1e300);
             Ray<G> r = make_ray<G>(o, d, G(1e-6), inf);
             Ignore ig = ignore_none();
@@ -85,6 +88,7 @@ __global__ void __launch_bounds__(kBlock) k_discovery_trace(SceneDev sc, int cou
         }
         groups_out[size_t(i) * depth + k] = hit_group;
     }
+    if (ray_counter) atomicAdd(ray_counter, traced);
 }
 
 // key for unique chains at depth k: (prefix rank << 21) | group
@@ -177,7 +181,7 @@ __global__ void k_chain_images(SceneDev sc, const float* tx, int depth, const in
 // ------------------------------------------------------------ edge prefilter
 template <typename G>
 __global__ void __launch_bounds__(kBlock) k_edge_flags(SceneDev sc, const float* tx_pos, int t, double wavelength,
-                                                       int* flags, int* err) {
+                                                       int* flags, int* err, unsigned long long* ray_counter) {
     extern __shared__ int stack[];
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= sc.num_edges) return;
@@ -197,11 +201,14 @@ __global__ void __launch_bounds__(kBlock) k_edge_flags(SceneDev sc, const float*
         ig.f0 = ed.face0;
         ig.f1 = ed.face1;
         const V3<double> bis = v3(ed.bisector[0], ed.bisector[1], ed.bisector[2]);
+        unsigned long long traced = 0;
         for (int i = 0; i < n && !ok; ++i) {
             const double tt = -0.5 * L + (i + 0.5) / n * L;
             const V3<double> p = c + e * tt + bis * kDiffractionRayBias;
+            ++traced;
             if (!segment_blocked<G>(sc, cast3<G>(S), cast3<G>(p), ig, stack, err)) ok = 1;
         }
+        if (ray_counter) atomicAdd(ray_counter, traced);
     }
     flags[j] = ok;
 }
@@ -339,9 +346,11 @@ __global__ void __launch_bounds__(kBlock) k_main(MainParams p) {
         for (int s = 0; s < 3; ++s) acc[f].dv[s] = cx(T(0), T(0));
     }
     int* err = p.status;
+    unsigned long long rays = 0;
     // -------------------------------------------------------------- LoS
     if (p.components & 1) {
         const bool blocked = sc.num_faces > 0 && segment_blocked<T>(sc, ST, RT, ignore_none(), stack, err);
+        if (sc.num_faces > 0) ++rays;
         if (!blocked) {
             const double dist = length(R - S);
 #pragma unroll
@@ -383,6 +392,7 @@ __global__ void __launch_bounds__(kBlock) k_main(MainParams p) {
                     Ignore ig = ignore_none();
                     ig.g0 = s > 0 ? groups[s - 1] : -1;
                     ig.g1 = s < d ? groups[s] : -1;
+                    ++rays;
                     if (segment_blocked<T>(sc, cast3<T>(a), cast3<T>(b), ig, stack, err)) ok = false;
                 }
                 if (!ok) continue;
@@ -440,7 +450,9 @@ __global__ void __launch_bounds__(kBlock) k_main(MainParams p) {
             ig.f0 = ed.face0;
             ig.f1 = ed.face1;
             const V3<double> qv = v3(res.q_vis[0], res.q_vis[1], res.q_vis[2]);
+            ++rays;
             if (segment_blocked<T>(sc, ST, cast3<T>(qv), ig, stack, err)) continue;
+            ++rays;
             if (segment_blocked<T>(sc, cast3<T>(qv), RT, ig, stack, err)) continue;
             const V3<double> q = v3(res.q[0], res.q[1], res.q[2]);
             const V3<T> arrival = safe_normalize(cast3<T>(R - q), v3<T>(T(0), T(0), T(1)));
@@ -465,6 +477,7 @@ __global__ void __launch_bounds__(kBlock) k_main(MainParams p) {
     // -------------------------------------------------------------- transmission
     if ((p.components & 8) && sc.num_faces > 0 && p.max_depth >= 1) {
         HitList hl;
+        ++rays;
         segment_hits<T>(sc, ST, RT, p.max_depth, &hl, stack, err);
         if (hl.count > p.max_depth) {
             if (p.overflow_counter) atomicAdd(p.overflow_counter, 1ull);
@@ -499,6 +512,7 @@ __global__ void __launch_bounds__(kBlock) k_main(MainParams p) {
         }
     }
     // -------------------------------------------------------------- outputs
+    if (p.ray_counter && p.freq_base == 0 && rays) atomicAdd(p.ray_counter, rays);
     const long long cells = (long long)p.num_tx * p.num_rx;
     const long long cell = (long long)t * p.num_rx + r;
 #pragma unroll
@@ -543,6 +557,11 @@ size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 }  // namespace
 
 // ------------------------------------------------------------ host side
+ProfileState& profile_state() {
+    static ProfileState st;
+    return st;
+}
+
 struct ChainPlan {
     bool exhaustive_o1;
     bool exhaustive_mb;
@@ -634,7 +653,7 @@ static WorkspaceLayout layout_for(const SceneDev& sc, const wcb_solve_desc& d, c
     L.edge_flags = take(size_t(std::max(sc.num_edges, 1)) * 4);
     L.edge_list = take(size_t(T) * std::max(sc.num_edges, 1) * 4);
     L.edge_count = take(size_t(T) * 4);
-    L.overflow = take(8);
+    L.overflow = take(32);
     L.layers64 = 0;
     L.total = o;
     return L;
@@ -669,11 +688,25 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     int* edge_list = reinterpret_cast<int*>(base + L.edge_list);
     int* edge_count = reinterpret_cast<int*>(base + L.edge_count);
     unsigned long long* overflow = reinterpret_cast<unsigned long long*>(base + L.overflow);
+    unsigned long long* ray_counter = overflow + 1;       // preparation rays (discovery, edge prefilter)
+    unsigned long long* main_ray_counter = overflow + 2;  // main-kernel rays
     const bool fp64 = d->precision == 1;
+    ProfileState& prof = profile_state();
+    cudaEvent_t ev_prep = nullptr, ev_main0 = nullptr, ev_main1 = nullptr;
+    if (prof.enabled) {
+        cudaEventCreate(&ev_prep);
+        cudaEventCreate(&ev_main0);
+        cudaEventCreate(&ev_main1);
+        cudaEventRecord(ev_prep, stream);
+        prof.main_ms = prof.prep_ms = 0.0;
+        prof.rays = 0;
+        prof.prep_rays = 0;
+        prof.main_launches = 0;
+    }
     if (T == 0 || R == 0) return 0;
     cudaMemsetAsync(chain_counts, 0, size_t(T) * kMaxDepth * 4, stream);
     cudaMemsetAsync(edge_count, 0, size_t(T) * 4, stream);
-    cudaMemsetAsync(overflow, 0, 8, stream);
+    cudaMemsetAsync(overflow, 0, 32, stream);
     if (out->status) cudaMemsetAsync(out->status, 0, 4, stream);
     if (out->row_count) cudaMemsetAsync(out->row_count, 0, 8, stream);
     // chain offsets (in chain-int units, per tx)
@@ -700,9 +733,9 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                 int* dg = reinterpret_cast<int*>(base + L.disc_groups);
                 const int md = d->max_depth;
                 if (fp64)
-                    k_discovery_trace<double><<<(rays + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, rays, md, dirs, txp, dg, err);
+                    k_discovery_trace<double><<<(rays + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, rays, md, dirs, txp, dg, err, prof.enabled ? ray_counter : nullptr);
                 else
-                    k_discovery_trace<float><<<(rays + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, rays, md, dirs, txp, dg, err);
+                    k_discovery_trace<float><<<(rays + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, rays, md, dirs, txp, dg, err, prof.enabled ? ray_counter : nullptr);
                 note_launch();
                 unsigned long long* keys = reinterpret_cast<unsigned long long*>(base + L.disc_keys);
                 unsigned long long* keys2 = reinterpret_cast<unsigned long long*>(base + L.disc_keys2);
@@ -759,9 +792,9 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         const double wavelength = kC0 / d->frequency_hz[0];
         for (int t = 0; t < T; ++t) {
             if (fp64)
-                k_edge_flags<double><<<(sc.num_edges + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, d->tx_pos, t, wavelength, edge_flags, err);
+                k_edge_flags<double><<<(sc.num_edges + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, d->tx_pos, t, wavelength, edge_flags, err, prof.enabled ? ray_counter : nullptr);
             else
-                k_edge_flags<float><<<(sc.num_edges + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, d->tx_pos, t, wavelength, edge_flags, err);
+                k_edge_flags<float><<<(sc.num_edges + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, d->tx_pos, t, wavelength, edge_flags, err, prof.enabled ? ray_counter : nullptr);
             k_compact_flags<<<1, 256, 0, stream>>>(sc.num_edges, edge_flags, edge_list + size_t(t) * sc.num_edges, edge_count + t);
             note_launch(2);
         }
@@ -822,6 +855,7 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     p.row_counter = reinterpret_cast<unsigned long long*>(out->row_count);
     p.status = out->status;
     p.overflow_counter = overflow;
+    p.ray_counter = prof.enabled ? main_ray_counter : nullptr;
     p.num_freq_total = d->num_freq;
     // FP64 mode: double copies of the layer tables
     double* layers64 = nullptr;
@@ -846,6 +880,7 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         threads = (long long)R * T;
     }
     const long long blocks = (threads + kBlock - 1) / kBlock;
+    if (prof.enabled) cudaEventRecord(ev_main0, stream);
     for (int fb = 0; fb < d->num_freq; fb += kMaxNF) {
         const int nf = std::min(kMaxNF, d->num_freq - fb);
         p.freq_base = fb;
@@ -891,6 +926,24 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
             }
             note_launch();
         }
+    }
+    if (prof.enabled) {
+        cudaEventRecord(ev_main1, stream);
+        unsigned long long nr[2] = {0, 0};
+        cudaMemcpyAsync(nr, ray_counter, 16, cudaMemcpyDeviceToHost, stream);
+        cudaEventSynchronize(ev_main1);
+        cudaStreamSynchronize(stream);
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, ev_prep, ev_main0);
+        cudaEventElapsedTime(&b, ev_main0, ev_main1);
+        prof.prep_ms = a;
+        prof.main_ms = b;
+        prof.prep_rays = (long long)nr[0];
+        prof.rays = (long long)nr[1];
+        prof.main_launches = (d->num_freq + kMaxNF - 1) / kMaxNF;
+        cudaEventDestroy(ev_prep);
+        cudaEventDestroy(ev_main0);
+        cudaEventDestroy(ev_main1);
     }
     if (layers64) cudaFreeAsync(layers64, stream);
     if (cudaGetLastError() != cudaSuccess) return 2;

@@ -82,7 +82,20 @@ struct MainParams {
     unsigned long long* row_counter;
     int* status;
     unsigned long long* overflow_counter;
+    unsigned long long* ray_counter;  // segment/ray queries traced (optional)
 };
+
+// Optional measurement of the main kernel: CUDA events bracket each launch
+// and the ray counter is read back after the solve.
+struct ProfileState {
+    bool enabled = false;
+    double main_ms = 0.0;        // summed main-kernel time of the last solve
+    double prep_ms = 0.0;        // candidate preparation time of the last solve
+    long long rays = 0;          // rays traced by the main kernel in the last solve
+    long long prep_rays = 0;     // rays traced while preparing candidates (discovery, edge prefilter)
+    long long main_launches = 0;
+};
+ProfileState& profile_state();
 
 struct SceneHandle;
 int solve_workspace_size(const SceneHandle* h, const wcb_solve_desc* d, int64_t* bytes);

@@ -34,10 +34,16 @@ template <typename T>
 struct FresnelPair {
     Cx<T> value;       // C(x) + jS(x)
     Cx<T> complement;  // (1+j)/2 - (C(x) + jS(x))
+    Cx<T> h;           // continued-fraction value (x >= 1.5), complement = x e^{j pi x^2/2} h
+    bool has_h;
 };
 
+// Fresnel integrals for x >= 0.  For x >= 1.5 the complement is kept in the
+// factored form x e^{j pi x^2/2} h so callers that need only its modulus or
+// that cancel the exponential never evaluate e^{j pi x^2/2} at a large
+// argument.
 template <typename T>
-WCB_HD FresnelPair<T> fresnel_pos(T x) {
+WCB_HD FresnelPair<T> fresnel_pos(T x, bool want_value = true) {
     FresnelPair<T> out;
     const Cx<T> half = cx(T(0.5), T(0.5));
     const T eps = sizeof(T) == 4 ? T(1e-7) : T(1e-15);
@@ -57,6 +63,7 @@ WCB_HD FresnelPair<T> fresnel_pos(T x) {
         }
         out.value = cx(sum_c, sum_s);
         out.complement = half - out.value;
+        out.has_h = false;
         return out;
     }
     const Cx<T> b1 = cx(T(1), -T(kPi) * x * x);
@@ -74,9 +81,16 @@ WCB_HD FresnelPair<T> fresnel_pos(T x) {
         h = h * del;
         if (value_of(s_abs(del.re - T(1)) + s_abs(del.im)) < value_of(eps)) break;
     }
-    const Cx<T> e = cexpj<T>(T(kPi / 2) * x * x);
-    out.complement = e * h * x;
-    out.value = half - out.complement;
+    out.h = h;
+    out.has_h = true;
+    if (want_value) {
+        // the exponential argument is reduced in FP64 before the T-precision sincos
+        double ph = kPi / 2 * double(value_of(x)) * double(value_of(x));
+        ph = ph - kTwoPi * floor(ph / kTwoPi);
+        const Cx<T> e = cexpj<T>(T(ph));
+        out.complement = e * h * x;
+        out.value = half - out.complement;
+    }
     return out;
 }
 
@@ -88,16 +102,33 @@ WCB_HD FresnelPair<T> fresnel(T x) {
     FresnelPair<T> out;
     out.value = -p.value;
     out.complement = cx(T(1), T(1)) - p.complement;
+    out.has_h = false;
     return out;
 }
 
+// |(1+j)/2 - (C(x) + jS(x))| for any real x.
+template <typename T>
+WCB_HD T fresnel_complement_abs(T x) {
+    if (value_of(x) >= 0) {
+        const FresnelPair<T> p = fresnel_pos(x, false);
+        return p.has_h ? x * cabs(p.h) : cabs(p.complement);
+    }
+    const FresnelPair<T> p = fresnel_pos(-x);
+    return cabs(cx(T(1), T(1)) - p.complement);
+}
+
 // KP transition function F(x) = 2j sqrt(x) e^{jx} int_{sqrt x}^inf e^{-j t^2} dt, x >= 0.
+// With u = sqrt(2x/pi): int = sqrt(pi/2) conj(complement(u)); for u >= 1.5 the
+// exponentials cancel exactly and F = 2j x conj(h(u)).
 template <typename T>
 WCB_HD Cx<T> transition(T x) {
     if (value_of(x) <= 0) return cx(T(0), T(0));
     const T u = s_sqrt(T(2) * x / T(kPi));
-    const FresnelPair<T> p = fresnel_pos(u);
-    // int = sqrt(pi/2) * conj(complement); F = 2j sqrt(x) e^{jx} * int
+    const FresnelPair<T> p = fresnel_pos(u, false);
+    if (p.has_h) {
+        const Cx<T> ch = cconj(p.h);
+        return cx(-ch.im * T(2) * x, ch.re * T(2) * x);
+    }
     const Cx<T> integral = cconj(p.complement) * T(s_sqrt(kPi / 2));
     const Cx<T> pre = cexpj<T>(x) * (T(2) * s_sqrt(x));
     return cx(T(0), T(1)) * pre * integral;
@@ -215,10 +246,10 @@ WCB_HD DiffractionResult<T> utd_field(const EdgeDev& ed, V3<double> S, V3<double
     const T sigma = s_sqrt(kT * kappa / T(kPi));
     const T tsT = T(t_star);
     const T tmax = T(ed.half_length), tmin = -T(ed.half_length);
-    const FresnelPair<T> hi = fresnel(sigma * (tmax - tsT));
-    const FresnelPair<T> lo = fresnel(-(sigma * (tmin - tsT)));
     const T inv_sqrt2 = T(0.70710678118654752440);
-    const T t_mono = s_min(s_max(T(1) - inv_sqrt2 * cabs(lo.complement) - inv_sqrt2 * cabs(hi.complement), T(0)), T(1));
+    const T hi_abs = fresnel_complement_abs(sigma * (tmax - tsT));
+    const T lo_abs = fresnel_complement_abs(-(sigma * (tmin - tsT)));
+    const T t_mono = s_min(s_max(T(1) - inv_sqrt2 * lo_abs - inv_sqrt2 * hi_abs, T(0)), T(1));
     T u;
     if (value_of(s_abs(tsT - tmax)) < value_of(s_abs(tsT - tmin))) u = sigma * (tsT - tmax);
     else u = sigma * (tmin - tsT);
