@@ -1,0 +1,659 @@
+// Per-component solve kernels with in-warp compaction.
+//
+// A warp owns a tile of 32 receiver cells of one transmitter (an 8x4 patch of
+// a receiver grid, or 32 consecutive points).  Lanes test candidates for
+// their own cells; the survivors are appended to a per-warp queue in shared
+// memory (ballot + popc) and processed 32 at a time with every lane busy.  A
+// processed item's contribution is written to a per-warp buffer and gathered
+// by the lane that owns the item's cell in item order, so every cell sums its
+// paths in a fixed order (deterministic) and each slot of each cell is written
+// once.  Each component runs in its own kernel so the code a warp executes
+// stays small.
+#pragma once
+
+#include "em.cuh"
+#include "paths.cuh"
+#include "solve.h"
+#include "utd.cuh"
+
+namespace wcb {
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kCompBlock = kWarpsPerBlock * 32;
+constexpr int kQueueCap = 64;
+constexpr unsigned kFull = 0xffffffffu;
+
+// ------------------------------------------------------------------ common
+template <typename T>
+WCB_D Slab<T> face_slab(const MainParams& p, int f_index, int face) {
+    const int m = p.sc.face_material[face];
+    const long long o = (long long)f_index * p.num_materials + m;
+    return Slab<T>{T(p.mat_eps_r[o]), T(p.mat_sigma_e[o]), T(p.mat_mu_r[o]), T(p.mat_gain[o]), T(p.mat_thickness[o])};
+}
+
+template <typename T>
+WCB_D LayerTable<T> layer_table_f(const MainParams& p, int f_index);
+
+template <>
+WCB_D LayerTable<float> layer_table_f<float>(const MainParams& p, int f_index) {
+    const long long o = (long long)f_index * p.num_layers;
+    return LayerTable<float>{p.layer_offset, p.layer_count, p.layer_thickness + o, p.layer_eps_r + o,
+                             p.layer_sigma_e + o, p.layer_mu_r + o};
+}
+
+template <>
+WCB_D LayerTable<double> layer_table_f<double>(const MainParams& p, int f_index) {
+    const long long o = (long long)f_index * p.num_layers;
+    return LayerTable<double>{p.layer_offset, p.layer_count, p.layer_thickness64 + o, p.layer_eps_r64 + o,
+                              p.layer_sigma_e64 + o, p.layer_mu_r64 + o};
+}
+
+WCB_D void emit_row(const MainParams& p, int t, int r, int cid, int depth, const int* seq, int edge, float length) {
+    if (p.rows == nullptr) return;
+    const unsigned long long idx = atomicAdd(p.row_counter, 1ull);
+    if (idx >= (unsigned long long)p.row_capacity) return;
+    RowRec rec;
+    rec.tx = t;
+    rec.rx = r;
+    rec.component = short(cid);
+    rec.depth = short(depth);
+    for (int k = 0; k < kMaxDepth; ++k) rec.seq[k] = k < depth && seq ? seq[k] : -1;
+    rec.edge = edge;
+    rec.length = length;
+    rec.pad = 0;
+    rec.pad2 = 0;
+    p.rows[idx] = rec;
+}
+
+// receiver point (float, formed like the reference's grid kernel)
+WCB_D V3<float> rx_point(const MainParams& p, int r) {
+    if (p.rx_kind == 1) {
+        const int row = r / p.grid_cols;
+        const int col = r - row * p.grid_cols;
+        const float u = __fmul_rn(float(row), p.grid_spacing[0]);
+        const float v = __fmul_rn(float(col), p.grid_spacing[1]);
+        return v3(__fadd_rn(__fadd_rn(p.grid_origin[0], __fmul_rn(p.grid_x[0], u)), __fmul_rn(p.grid_y[0], v)),
+                  __fadd_rn(__fadd_rn(p.grid_origin[1], __fmul_rn(p.grid_x[1], u)), __fmul_rn(p.grid_y[1], v)),
+                  __fadd_rn(__fadd_rn(p.grid_origin[2], __fmul_rn(p.grid_x[2], u)), __fmul_rn(p.grid_y[2], v)));
+    }
+    return v3(p.rx_pos[3 * r], p.rx_pos[3 * r + 1], p.rx_pos[3 * r + 2]);
+}
+
+// number of 32-cell tiles per transmitter
+WCB_HD long long tiles_per_tx(const MainParams& p) {
+    if (p.rx_kind == 1) return (long long)((p.grid_rows + 7) / 8) * ((p.grid_cols + 3) / 4);
+    return (p.num_rx + 31) / 32;
+}
+
+// cell of (tile, lane); false for lanes past the grid edge
+WCB_D bool tile_cell(const MainParams& p, long long tile_global, int lane, int* t, int* r) {
+    const long long per_tx = tiles_per_tx(p);
+    const long long tt = tile_global / per_tx;
+    if (tt >= p.num_tx) return false;
+    const long long tile = tile_global - tt * per_tx;
+    *t = int(tt);
+    if (p.rx_kind == 1) {
+        const int tiles_c = (p.grid_cols + 3) / 4;
+        const int tr = int(tile / tiles_c), tc = int(tile - (long long)tr * tiles_c);
+        const int row = tr * 8 + lane / 4;
+        const int col = tc * 4 + (lane & 3);
+        if (row >= p.grid_rows || col >= p.grid_cols) return false;
+        *r = row * p.grid_cols + col;
+        return true;
+    }
+    const long long r64 = tile * 32 + lane;
+    if (r64 >= p.num_rx) return false;
+    *r = int(r64);
+    return true;
+}
+
+WCB_D unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Append (lane, cand, aux) for every lane with `pass`; returns the new size.
+WCB_D int queue_push(int* q, int size, bool pass, int a, int b, int c) {
+    const unsigned mask = __ballot_sync(kFull, pass);
+    if (pass) {
+        const int pos = size + __popc(mask & lanemask_lt());
+        q[3 * pos] = a;
+        q[3 * pos + 1] = b;
+        q[3 * pos + 2] = c;
+    }
+    __syncwarp();
+    return size + __popc(mask);
+}
+
+// Remove the first `n` items (n <= 32) from a queue of `size` items.
+WCB_D int queue_pop(int* q, int size, int n, int lane) {
+    const int rem = size - n;
+    int a = 0, b = 0, c = 0;
+    if (lane < rem) {
+        a = q[3 * (n + lane)];
+        b = q[3 * (n + lane) + 1];
+        c = q[3 * (n + lane) + 2];
+    }
+    __syncwarp();
+    if (lane < rem) {
+        q[3 * lane] = a;
+        q[3 * lane + 1] = b;
+        q[3 * lane + 2] = c;
+    }
+    __syncwarp();
+    return rem;
+}
+
+template <typename T>
+WCB_D void store_slot(const MainParams& p, int slot, int f, long long cell, Cx<T> v, T gain, bool coherent) {
+    const long long cells = (long long)p.num_tx * p.num_rx;
+    const long long fc = (long long)(p.freq_base + f) * cells + cell;
+    const long long o = (long long)slot * p.num_freq_total * cells + fc;
+    T* cp = static_cast<T*>(p.out_comp_power);
+    T* cf = static_cast<T*>(p.out_comp_field);
+    if (cp) cp[o] = coherent ? cabs2(v) : gain;
+    if (cf) {
+        cf[2 * o] = v.re;
+        cf[2 * o + 1] = v.im;
+    }
+}
+
+// ------------------------------------------------------------------ LoS + transmission
+template <typename T, int NF>
+__global__ void __launch_bounds__(kCompBlock) k_los_trans(MainParams p) {
+    extern __shared__ int smem[];
+    int* stack = smem;
+    const int lane = threadIdx.x & 31;
+    const long long tile = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+    int t, r;
+    if (!tile_cell(p, tile, lane, &t, &r)) return;
+    const SceneDev& sc = p.sc;
+    int* err = p.status;
+    const V3<double> S = v3<double>(p.tx_pos[3 * t], p.tx_pos[3 * t + 1], p.tx_pos[3 * t + 2]);
+    const V3<float> Rf = rx_point(p, r);
+    const V3<double> R = cast3<double>(Rf);
+    const V3<T> ST = cast3<T>(S), RT = cast3<T>(R);
+    const V3<T> tx_pol = v3<T>(T(p.tx_pol[3 * t]), T(p.tx_pol[3 * t + 1]), T(p.tx_pol[3 * t + 2]));
+    const float* rp = p.rx_pol + (long long)r * p.rx_pol_stride;
+    const V3<T> rx_pol = v3<T>(T(rp[0]), T(rp[1]), T(rp[2]));
+    const T sqrt_p = s_sqrt(s_max(T(p.tx_power[t]), T(0)));
+    const long long cell = (long long)t * p.num_rx + r;
+    unsigned long long rays = 0;
+    if (p.components & 1) {
+        Cx<T> acc[NF];
+        T gain[NF];
+        for (int f = 0; f < NF; ++f) { acc[f] = cx(T(0), T(0)); gain[f] = T(0); }
+        const bool blocked = sc.num_faces > 0 && segment_blocked<T>(sc, ST, RT, ignore_none(), stack, err);
+        if (sc.num_faces > 0) ++rays;
+        if (!blocked) {
+            const double dist = length(R - S);
+#pragma unroll 1
+            for (int f = 0; f < NF; ++f) {
+                const PathEval<T> ev = eval_free_space(ST, RT, tx_pol, rx_pol, p.k[f], dist);
+                const Cx<T> pf = ev.coefficient * sqrt_p;
+                acc[f] = pf;
+                gain[f] = cabs2(pf);
+            }
+            emit_row(p, t, r, 0, 0, nullptr, -1, float(dist));
+        }
+        for (int f = 0; f < NF; ++f) store_slot(p, 0, f, cell, acc[f], gain[f], p.coherent);
+    }
+    if ((p.components & 8) && p.max_depth >= 1) {
+        Cx<T> acc[NF];
+        T gain[NF];
+        for (int f = 0; f < NF; ++f) { acc[f] = cx(T(0), T(0)); gain[f] = T(0); }
+        if (sc.num_faces > 0) {
+            HitList hl;
+            ++rays;
+            segment_hits<T>(sc, ST, RT, p.max_depth, &hl, stack, err);
+            if (hl.count > p.max_depth) {
+                if (p.overflow_counter) atomicAdd(p.overflow_counter, 1ull);
+            } else if (hl.count >= 1) {
+                bool ok = true;
+                for (int i = 0; i < hl.count; ++i) {
+                    const int m = sc.face_material[hl.face[i]];
+                    if (p.mat_volumetric && p.mat_volumetric[m]) ok = false;
+                }
+                if (ok) {
+                    const double dist = length(R - S);
+                    const V3<T> dir = safe_normalize(RT - ST, v3<T>(T(0), T(0), T(1)));
+#pragma unroll 1
+                    for (int f = 0; f < NF; ++f) {
+                        C3<T> value = c3_from_real(transverse(dir, tx_pol));
+                        T shorten = T(0);
+                        const LayerTable<T> lt = layer_table_f<T>(p, f);
+                        for (int i = 0; i < hl.count; ++i) {
+                            const float* nf = sc.face_normal + 3 * hl.face[i];
+                            transmit_wall(value, shorten, dir, v3<T>(T(nf[0]), T(nf[1]), T(nf[2])),
+                                          sc.face_material[hl.face[i]], lt, p.freq[f]);
+                        }
+                        const T amp = T(1) / (T(2) * T(p.k[f]) * T(fmax(dist, kUtdEps)));
+                        value = c3_scale(value, phasor_neg_kd<T>(p.k[f], dist - double(value_of(shorten))) * amp);
+                        const Cx<T> pf = project_receiver(value, dir, rx_pol) * sqrt_p;
+                        acc[f] = pf;
+                        gain[f] = cabs2(pf);
+                    }
+                    emit_row(p, t, r, 5, hl.count, hl.face, -1, float(dist));
+                }
+            }
+        }
+        for (int f = 0; f < NF; ++f) store_slot(p, 3, f, cell, acc[f], gain[f], p.coherent);
+    }
+    if (p.ray_counter && p.freq_base == 0 && rays) atomicAdd(p.ray_counter, rays);
+}
+
+// ------------------------------------------------------------------ reflection
+// Per-warp shared layout: queue A (3 ints/item), queue B (3 + 5 ints/item),
+// contribution buffer (32 items x NF x 3 floats).
+template <int NF>
+struct ReflShared {
+    int qa[3 * kQueueCap];
+    int qb[3 * kQueueCap];
+    int qbf[kMaxDepth * kQueueCap];
+    float contrib[32 * NF * 3];
+    int owner[32];
+};
+
+template <typename T, int NF>
+__global__ void __launch_bounds__(kCompBlock) k_reflect(MainParams p, int stack_depth) {
+    extern __shared__ int smem[];
+    int* stack = smem;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    ReflShared<NF>* sh = reinterpret_cast<ReflShared<NF>*>(smem + stack_depth * kCompBlock) + warp;
+    const long long tile = (long long)blockIdx.x * kWarpsPerBlock + warp;
+    int t = 0, r = 0;
+    const bool active = tile_cell(p, tile, lane, &t, &r);
+    // the whole warp shares the tile's transmitter
+    const long long per_tx = tiles_per_tx(p);
+    const int tw = int(tile / per_tx);
+    if (tw >= p.num_tx) return;
+    t = tw;
+    const SceneDev& sc = p.sc;
+    int* err = p.status;
+    const V3<double> S = v3<double>(p.tx_pos[3 * t], p.tx_pos[3 * t + 1], p.tx_pos[3 * t + 2]);
+    const V3<T> ST = cast3<T>(S);
+    const V3<T> tx_pol = v3<T>(T(p.tx_pol[3 * t]), T(p.tx_pol[3 * t + 1]), T(p.tx_pol[3 * t + 2]));
+    const V3<float> Rf = active ? rx_point(p, r) : v3(0.f, 0.f, 0.f);
+    const float* rp = p.rx_pol + (long long)(active ? r : 0) * p.rx_pol_stride;
+    const V3<float> rpol = v3(rp[0], rp[1], rp[2]);
+    const T sqrt_p = s_sqrt(s_max(T(p.tx_power[t]), T(0)));
+    Cx<T> acc[NF];
+    T gain[NF];
+    for (int f = 0; f < NF; ++f) { acc[f] = cx(T(0), T(0)); gain[f] = T(0); }
+    unsigned long long rays = 0;
+    int qa = 0, qb = 0;
+
+    // stage B: visibility + field for 32 items (FP64 hits recomputed)
+    auto process_b = [&](int n) {
+        int it_lane = 0, c = 0, d = 1;
+        if (lane < n) {
+            it_lane = sh->qb[3 * lane];
+            c = sh->qb[3 * lane + 1];
+            d = sh->qb[3 * lane + 2];
+        }
+        const float rx = __shfl_sync(kFull, Rf.x, it_lane);
+        const float ry = __shfl_sync(kFull, Rf.y, it_lane);
+        const float rz = __shfl_sync(kFull, Rf.z, it_lane);
+        const float px = __shfl_sync(kFull, rpol.x, it_lane);
+        const float py = __shfl_sync(kFull, rpol.y, it_lane);
+        const float pz = __shfl_sync(kFull, rpol.z, it_lane);
+        bool ok = lane < n;
+        if (ok) {
+            const V3<double> R = v3<double>(rx, ry, rz);
+            const long long base = p.chain_offset[t * kMaxDepth + (d - 1)];
+            const int* groups = p.chain_groups + base + (long long)c * d;
+            const double* planes = p.chain_planes + (base + (long long)c * d) * 4;
+            const double* images = p.chain_images + (base + (long long)c * d) * 3;
+            V3<double> hits[kMaxDepth];
+            back_project(R, planes, images, d, hits);
+            int faces[kMaxDepth];
+            for (int k = 0; k < d; ++k) faces[k] = sh->qbf[kMaxDepth * lane + k];
+            for (int s = 0; s <= d && ok; ++s) {
+                const V3<double> a = s == 0 ? S : hits[s - 1];
+                const V3<double> b = s == d ? R : hits[s];
+                Ignore ig = ignore_none();
+                ig.g0 = s > 0 ? groups[s - 1] : -1;
+                ig.g1 = s < d ? groups[s] : -1;
+                ++rays;
+                if (segment_blocked<T>(sc, cast3<T>(a), cast3<T>(b), ig, stack, err)) ok = false;
+            }
+            if (ok) {
+                const V3<double> img = v3(images[3 * (d - 1)], images[3 * (d - 1) + 1], images[3 * (d - 1) + 2]);
+                const double total = length(R - img);
+                const V3<T> RT = cast3<T>(R);
+                const V3<T> rx_pol = v3<T>(T(px), T(py), T(pz));
+#pragma unroll 1
+                for (int f = 0; f < NF; ++f) {
+                    const double freq = p.freq[f];
+                    const T wl = T(kC0 / freq);
+                    V3<T> prev = ST;
+                    V3<T> incident = safe_normalize(cast3<T>(hits[0]) - prev, v3<T>(T(0), T(0), T(1)));
+                    C3<T> value = c3_from_real(transverse(incident, tx_pol));
+                    V3<T> outgoing = incident;
+                    for (int k = 0; k < d; ++k) {
+                        const V3<T> hit = cast3<T>(hits[k]);
+                        incident = safe_normalize(hit - prev, outgoing);
+                        const float* nf = sc.face_normal + 3 * faces[k];
+                        reflect_bounce(value, outgoing, incident, v3<T>(T(nf[0]), T(nf[1]), T(nf[2])),
+                                       face_slab<T>(p, f, faces[k]), freq, wl);
+                        prev = hit;
+                    }
+                    const V3<T> fdir = safe_normalize(RT - prev, outgoing);
+                    const T amp = T(1) / (T(2) * T(p.k[f]) * T(fmax(total, kUtdEps)));
+                    value = c3_scale(value, phasor_neg_kd<T>(p.k[f], total) * amp);
+                    const Cx<T> pf = project_receiver(value, fdir, rx_pol) * sqrt_p;
+                    sh->contrib[(lane * NF + f) * 3 + 0] = float(value_of(pf.re));
+                    sh->contrib[(lane * NF + f) * 3 + 1] = float(value_of(pf.im));
+                    sh->contrib[(lane * NF + f) * 3 + 2] = float(value_of(cabs2(pf)));
+                }
+                int tt = 0, rr = 0;
+                tile_cell(p, tile, it_lane, &tt, &rr);
+                emit_row(p, t, rr, 1, d, faces, -1, float(total));
+            }
+        }
+        sh->owner[lane] = ok ? it_lane : -1;
+        __syncwarp();
+        for (int i = 0; i < n; ++i) {
+            if (sh->owner[i] == lane) {
+                for (int f = 0; f < NF; ++f) {
+                    acc[f] = acc[f] + cx(T(sh->contrib[(i * NF + f) * 3]), T(sh->contrib[(i * NF + f) * 3 + 1]));
+                    gain[f] = gain[f] + T(sh->contrib[(i * NF + f) * 3 + 2]);
+                }
+            }
+        }
+        __syncwarp();
+    };
+
+    // stage A: FP64 back projection + containment for 32 items
+    auto process_a = [&](int n) {
+        int it_lane = 0, c = 0, d = 1;
+        if (lane < n) {
+            it_lane = sh->qa[3 * lane];
+            c = sh->qa[3 * lane + 1];
+            d = sh->qa[3 * lane + 2];
+        }
+        const float rx = __shfl_sync(kFull, Rf.x, it_lane);
+        const float ry = __shfl_sync(kFull, Rf.y, it_lane);
+        const float rz = __shfl_sync(kFull, Rf.z, it_lane);
+        bool ok = lane < n;
+        int faces[kMaxDepth];
+        if (ok) {
+            const long long base = p.chain_offset[t * kMaxDepth + (d - 1)];
+            const int* groups = p.chain_groups + base + (long long)c * d;
+            const double* planes = p.chain_planes + (base + (long long)c * d) * 4;
+            const double* images = p.chain_images + (base + (long long)c * d) * 3;
+            V3<double> hits[kMaxDepth];
+            ok = back_project(v3<double>(rx, ry, rz), planes, images, d, hits);
+            for (int k = d - 1; k >= 0 && ok; --k) {
+                faces[k] = resolve_in_group(sc, groups[k], hits[k]);
+                ok = faces[k] >= 0;
+            }
+        }
+        // push survivors into queue B (faces stored beside the item)
+        const unsigned mask = __ballot_sync(kFull, ok);
+        if (ok) {
+            const int pos = qb + __popc(mask & lanemask_lt());
+            sh->qb[3 * pos] = it_lane;
+            sh->qb[3 * pos + 1] = c;
+            sh->qb[3 * pos + 2] = d;
+            for (int k = 0; k < d; ++k) sh->qbf[kMaxDepth * pos + k] = faces[k];
+        }
+        __syncwarp();
+        qb += __popc(mask);
+        while (qb >= 32) {
+            process_b(32);
+            // shift queue B (items and faces)
+            const int rem = qb - 32;
+            int a0 = 0, a1 = 0, a2 = 0, fb[kMaxDepth];
+            if (lane < rem) {
+                a0 = sh->qb[3 * (32 + lane)];
+                a1 = sh->qb[3 * (32 + lane) + 1];
+                a2 = sh->qb[3 * (32 + lane) + 2];
+                for (int k = 0; k < kMaxDepth; ++k) fb[k] = sh->qbf[kMaxDepth * (32 + lane) + k];
+            }
+            __syncwarp();
+            if (lane < rem) {
+                sh->qb[3 * lane] = a0;
+                sh->qb[3 * lane + 1] = a1;
+                sh->qb[3 * lane + 2] = a2;
+                for (int k = 0; k < kMaxDepth; ++k) sh->qbf[kMaxDepth * lane + k] = fb[k];
+            }
+            __syncwarp();
+            qb = rem;
+        }
+    };
+
+    if ((p.components & 2) && sc.num_faces > 0) {
+        for (int d = 1; d <= p.max_depth; ++d) {
+            const int cnt = p.chain_count[t * kMaxDepth + (d - 1)];
+            const long long base = p.chain_offset[t * kMaxDepth + (d - 1)];
+            for (int c = 0; c < cnt; ++c) {
+                bool pass = active;
+                if (sizeof(T) == 4 && pass) {
+                    pass = back_project_prefilter(sc, Rf, p.chain_groups + base + (long long)c * d,
+                                                  p.chain_planes + (base + (long long)c * d) * 4,
+                                                  p.chain_images + (base + (long long)c * d) * 3, d);
+                }
+                qa = queue_push(sh->qa, qa, pass, lane, c, d);
+                if (qa >= 32) {
+                    process_a(32);
+                    qa = queue_pop(sh->qa, qa, 32, lane);
+                }
+            }
+        }
+        if (qa > 0) {
+            process_a(qa);
+            qa = 0;
+        }
+        if (qb > 0) {
+            process_b(qb);
+            qb = 0;
+        }
+        if (active) {
+            const long long cell = (long long)t * p.num_rx + r;
+            for (int f = 0; f < NF; ++f) store_slot(p, 1, f, cell, acc[f], gain[f], p.coherent);
+        }
+    }
+    if (p.ray_counter && p.freq_base == 0 && rays) atomicAdd(p.ray_counter, rays);
+}
+
+// ------------------------------------------------------------------ diffraction
+template <int NF>
+struct DiffShared {
+    int qv[3 * kQueueCap];
+    float contrib[32 * NF * 9];
+    int owner[32];
+};
+
+template <typename T, int NF>
+__global__ void __launch_bounds__(kCompBlock) k_diffract(MainParams p, int stack_depth) {
+    extern __shared__ int smem[];
+    int* stack = smem;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    DiffShared<NF>* sh = reinterpret_cast<DiffShared<NF>*>(smem + stack_depth * kCompBlock) + warp;
+    const long long tile = (long long)blockIdx.x * kWarpsPerBlock + warp;
+    int t = 0, r = 0;
+    const bool active = tile_cell(p, tile, lane, &t, &r);
+    const long long per_tx = tiles_per_tx(p);
+    const int tw = int(tile / per_tx);
+    if (tw >= p.num_tx) return;
+    t = tw;
+    const SceneDev& sc = p.sc;
+    int* err = p.status;
+    const V3<double> S = v3<double>(p.tx_pos[3 * t], p.tx_pos[3 * t + 1], p.tx_pos[3 * t + 2]);
+    const V3<T> ST = cast3<T>(S);
+    const V3<T> tx_pol = v3<T>(T(p.tx_pol[3 * t]), T(p.tx_pol[3 * t + 1]), T(p.tx_pol[3 * t + 2]));
+    const V3<float> Rf = active ? rx_point(p, r) : v3(0.f, 0.f, 0.f);
+    const float* rp = p.rx_pol + (long long)(active ? r : 0) * p.rx_pol_stride;
+    const V3<float> rpol = v3(rp[0], rp[1], rp[2]);
+    const T sqrt_p = s_sqrt(s_max(T(p.tx_power[t]), T(0)));
+    Cx<T> acc[NF];
+    T gain[NF];
+    Cx<T> dv[NF][3];
+    for (int f = 0; f < NF; ++f) {
+        acc[f] = cx(T(0), T(0));
+        gain[f] = T(0);
+        for (int k = 0; k < 3; ++k) dv[f][k] = cx(T(0), T(0));
+    }
+    unsigned long long rays = 0;
+    int qv = 0;
+    const int cnt = ((p.components & 4) && p.max_depth >= 1) ? p.edge_count[t] : 0;
+    const int* list = p.edge_list + (long long)t * sc.num_edges;
+
+    // UTD fields for 32 visible items
+    auto process_v = [&](int n) {
+        int it_lane = 0, j = 0;
+        if (lane < n) {
+            it_lane = sh->qv[3 * lane];
+            j = sh->qv[3 * lane + 1];
+        }
+        const float rx = __shfl_sync(kFull, Rf.x, it_lane);
+        const float ry = __shfl_sync(kFull, Rf.y, it_lane);
+        const float rz = __shfl_sync(kFull, Rf.z, it_lane);
+        const float px = __shfl_sync(kFull, rpol.x, it_lane);
+        const float py = __shfl_sync(kFull, rpol.y, it_lane);
+        const float pz = __shfl_sync(kFull, rpol.z, it_lane);
+        bool any = false;
+        if (lane < n) {
+            const EdgeDev& ed = sc.edges[list[j]];
+            const V3<double> R = v3<double>(rx, ry, rz);
+            const V3<T> rx_pol = v3<T>(T(px), T(py), T(pz));
+            double qx = 0, qy = 0, qz = 0, len = 0;
+#pragma unroll 1
+            for (int f = 0; f < NF; ++f) {
+                const DiffractionResult<T> res =
+                    utd_field<T>(ed, S, R, tx_pol, face_slab<T>(p, f, ed.mat_face0), face_slab<T>(p, f, ed.mat_face1), p.freq[f]);
+                qx = res.q[0]; qy = res.q[1]; qz = res.q[2];
+                len = res.length;
+                const C3<T> powered = c3_scale(res.field, cx(sqrt_p, T(0)));
+                float* cb = sh->contrib + (lane * NF + f) * 9;
+                if (res.valid && value_of(c3_power(powered)) >= kUtdGainFloor) {
+                    any = true;
+                    const V3<T> arrival = safe_normalize(cast3<T>(R - v3(qx, qy, qz)), v3<T>(T(0), T(0), T(1)));
+                    const Cx<T> pf = project_receiver(powered, arrival, rx_pol);
+                    cb[0] = float(value_of(pf.re));
+                    cb[1] = float(value_of(pf.im));
+                    cb[2] = float(value_of(cabs2(pf)));
+                    cb[3] = float(value_of(powered.x.re)); cb[4] = float(value_of(powered.x.im));
+                    cb[5] = float(value_of(powered.y.re)); cb[6] = float(value_of(powered.y.im));
+                    cb[7] = float(value_of(powered.z.re)); cb[8] = float(value_of(powered.z.im));
+                } else {
+                    for (int k = 0; k < 9; ++k) cb[k] = 0.f;
+                }
+            }
+            if (any) {
+                int tt = 0, rr = 0;
+                tile_cell(p, tile, it_lane, &tt, &rr);
+                emit_row(p, t, rr, 2, 1, nullptr, ed.edge_id, float(len));
+            }
+        }
+        sh->owner[lane] = any ? it_lane : -1;
+        __syncwarp();
+        for (int i = 0; i < n; ++i) {
+            if (sh->owner[i] == lane) {
+                for (int f = 0; f < NF; ++f) {
+                    const float* cb = sh->contrib + (i * NF + f) * 9;
+                    acc[f] = acc[f] + cx(T(cb[0]), T(cb[1]));
+                    gain[f] = gain[f] + T(cb[2]);
+                    dv[f][0] = dv[f][0] + cx(T(cb[3]), T(cb[4]));
+                    dv[f][1] = dv[f][1] + cx(T(cb[5]), T(cb[6]));
+                    dv[f][2] = dv[f][2] + cx(T(cb[7]), T(cb[8]));
+                }
+            }
+        }
+        __syncwarp();
+    };
+
+    for (int j = 0; j < cnt; ++j) {
+        bool vis = false;
+        if (active) {
+            // visibility of the biased, clamped stationary point
+            const EdgeDev& ed = sc.edges[list[j]];
+            const V3<double> c = v3(ed.pos[0], ed.pos[1], ed.pos[2]);
+            const V3<double> e = v3(ed.dir[0], ed.dir[1], ed.dir[2]);
+            const V3<double> R = cast3<double>(Rf);
+            const V3<double> ds = S - c;
+            const double ts = dot(ds, e);
+            const double rs = length(ds - e * ts);
+            const V3<double> dr = R - c;
+            const double tr = dot(dr, e);
+            const double rr = length(dr - e * tr);
+            const double t_star = (rs + rr) > 0.0 ? ts + (tr - ts) * rs / (rs + rr) : ts;
+            const double tc = fmin(fmax(t_star, -ed.half_length), ed.half_length);
+            const V3<double> qv_pt = c + e * tc + v3(ed.bisector[0], ed.bisector[1], ed.bisector[2]) * kDiffractionRayBias;
+            Ignore ig = ignore_none();
+            ig.f0 = ed.face0;
+            ig.f1 = ed.face1;
+            ++rays;
+            vis = !segment_blocked<T>(sc, ST, cast3<T>(qv_pt), ig, stack, err);
+            if (vis) {
+                ++rays;
+                vis = !segment_blocked<T>(sc, cast3<T>(qv_pt), cast3<T>(R), ig, stack, err);
+            }
+        }
+        qv = queue_push(sh->qv, qv, vis, lane, j, 0);
+        if (qv >= 32) {
+            process_v(32);
+            qv = queue_pop(sh->qv, qv, 32, lane);
+        }
+    }
+    if (qv > 0) {
+        process_v(qv);
+        qv = 0;
+    }
+    if (active && cnt >= 0 && (p.components & 4)) {
+        const long long cell = (long long)t * p.num_rx + r;
+        const long long cells = (long long)p.num_tx * p.num_rx;
+        for (int f = 0; f < NF; ++f) {
+            store_slot(p, 2, f, cell, acc[f], gain[f], p.coherent);
+            T* dvp = static_cast<T*>(p.out_diff_vec_power);
+            if (dvp) dvp[(long long)(p.freq_base + f) * cells + cell] = cabs2(dv[f][0]) + cabs2(dv[f][1]) + cabs2(dv[f][2]);
+        }
+    }
+    if (p.ray_counter && p.freq_base == 0 && rays) atomicAdd(p.ray_counter, rays);
+}
+
+// ------------------------------------------------------------------ totals
+template <typename T>
+__global__ void k_finalize(MainParams p, int nf) {
+    const long long cells = (long long)p.num_tx * p.num_rx;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= cells * nf) return;
+    const int f = int(i / cells);
+    const long long cell = i - (long long)f * cells;
+    const long long fc = (long long)(p.freq_base + f) * cells + cell;
+    const long long stride = (long long)p.num_freq_total * cells;
+    T* cp = static_cast<T*>(p.out_comp_power);
+    T* cf = static_cast<T*>(p.out_comp_field);
+    if (cp == nullptr || cf == nullptr) return;
+    const int used[4] = {p.components & 1, p.components & 2, p.components & 4, p.components & 8};
+    Cx<T> total = cx(T(0), T(0));
+    T gsum = T(0);
+    for (int s = 0; s < 6; ++s) {
+        const long long o = s * stride + fc;
+        if (s < 4 && used[s]) {
+            total = total + cx(cf[2 * o], cf[2 * o + 1]);
+            gsum = gsum + cp[o];
+        } else {
+            cp[o] = T(0);
+            cf[2 * o] = T(0);
+            cf[2 * o + 1] = T(0);
+        }
+    }
+    T* pg = static_cast<T*>(p.out_path_gain);
+    T* fl = static_cast<T*>(p.out_field);
+    if (p.coherent) {
+        if (pg) pg[fc] = cabs2(total);
+        if (fl) { fl[2 * fc] = total.re; fl[2 * fc + 1] = total.im; }
+    } else {
+        if (pg) pg[fc] = gsum;
+        if (fl) { fl[2 * fc] = s_sqrt(s_max(gsum, T(0))); fl[2 * fc + 1] = T(0); }
+    }
+    T* dvp = static_cast<T*>(p.out_diff_vec_power);
+    if (dvp && !(p.components & 4)) dvp[fc] = T(0);
+}
+
+}  // namespace wcb

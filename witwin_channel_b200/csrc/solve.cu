@@ -25,6 +25,7 @@
 #include "paths.cuh"
 #include "solve.h"
 #include "utd.cuh"
+#include "kernels.cuh"
 
 namespace wcb {
 
@@ -234,322 +235,49 @@ __global__ void k_compact_flags(int n, const int* flags, int* list, int* count) 
 }
 
 // ------------------------------------------------------------ main kernel
-template <typename T>
-struct Accum {
-    Cx<T> slot[4];   // los, reflection, diffraction, transmission
-    T gain[4];
-    Cx<T> dv[3];     // diffraction vector sum (powered)
-};
-
-template <typename T>
-WCB_D Slab<T> face_slab(const MainParams& p, int f_index, int face) {
-    const int m = p.sc.face_material[face];
-    const long long o = (long long)f_index * p.num_materials + m;
-    return Slab<T>{T(p.mat_eps_r[o]), T(p.mat_sigma_e[o]), T(p.mat_mu_r[o]), T(p.mat_gain[o]), T(p.mat_thickness[o])};
-}
-
-template <typename T>
-WCB_D LayerTable<T> layer_table_f(const MainParams& p, int f_index);
-
-template <>
-WCB_D LayerTable<float> layer_table_f<float>(const MainParams& p, int f_index) {
-    const long long o = (long long)f_index * p.num_layers;
-    return LayerTable<float>{p.layer_offset, p.layer_count, p.layer_thickness + o, p.layer_eps_r + o,
-                             p.layer_sigma_e + o, p.layer_mu_r + o};
-}
-
-template <>
-WCB_D LayerTable<double> layer_table_f<double>(const MainParams& p, int f_index) {
-    // FP64 precision mode reads the float layer tables through a converting view
-    const long long o = (long long)f_index * p.num_layers;
-    return LayerTable<double>{p.layer_offset, p.layer_count, p.layer_thickness64 + o, p.layer_eps_r64 + o,
-                              p.layer_sigma_e64 + o, p.layer_mu_r64 + o};
-}
-
-WCB_D void emit_row(const MainParams& p, int t, int r, int cid, int depth, const int* seq, int edge, float length) {
-    if (p.rows == nullptr) return;
-    const unsigned long long idx = atomicAdd(p.row_counter, 1ull);
-    if (idx >= (unsigned long long)p.row_capacity) return;
-    RowRec rec;
-    rec.tx = t;
-    rec.rx = r;
-    rec.component = short(cid);
-    rec.depth = short(depth);
-    for (int k = 0; k < kMaxDepth; ++k) rec.seq[k] = k < depth && seq ? seq[k] : -1;
-    rec.edge = edge;
-    rec.length = length;
-    rec.pad = 0;
-    rec.pad2 = 0;
-    p.rows[idx] = rec;
-}
-
-template <typename T>
-WCB_D V3<T> rx_position(const MainParams& p, int r) {
-    if (p.rx_kind == 1) {
-        const int row = r / p.grid_cols;
-        const int col = r - row * p.grid_cols;
-        const float u = __fmul_rn(float(row), p.grid_spacing[0]);
-        const float v = __fmul_rn(float(col), p.grid_spacing[1]);
-        // (origin + x_axis*u) + y_axis*v, rounded per operation (los.cu:391-420)
-        return v3<T>(T(__fadd_rn(__fadd_rn(p.grid_origin[0], __fmul_rn(p.grid_x[0], u)), __fmul_rn(p.grid_y[0], v))),
-                     T(__fadd_rn(__fadd_rn(p.grid_origin[1], __fmul_rn(p.grid_x[1], u)), __fmul_rn(p.grid_y[1], v))),
-                     T(__fadd_rn(__fadd_rn(p.grid_origin[2], __fmul_rn(p.grid_x[2], u)), __fmul_rn(p.grid_y[2], v))));
-    }
-    return v3<T>(T(p.rx_pos[3 * r]), T(p.rx_pos[3 * r + 1]), T(p.rx_pos[3 * r + 2]));
-}
-
-// cell index of lane `i` (warps cover 8x4 receiver-grid patches)
-WCB_D bool cell_of(const MainParams& p, long long i, int* t, int* r) {
-    if (p.rx_kind == 1) {
-        const int tiles_r = (p.grid_rows + 7) / 8;
-        const int tiles_c = (p.grid_cols + 3) / 4;
-        const long long per_tx = (long long)tiles_r * tiles_c * 32;
-        const long long tt = i / per_tx;
-        if (tt >= p.num_tx) return false;
-        const long long rem = i - tt * per_tx;
-        const long long tile = rem / 32;
-        const int lane = int(rem - tile * 32);
-        const int tr = int(tile / tiles_c), tc = int(tile - (long long)tr * tiles_c);
-        const int row = tr * 8 + lane / 4;
-        const int col = tc * 4 + (lane & 3);
-        if (row >= p.grid_rows || col >= p.grid_cols) return false;
-        *t = int(tt);
-        *r = row * p.grid_cols + col;
-        return true;
-    }
-    const long long tt = i / p.num_rx;
-    if (tt >= p.num_tx) return false;
-    *t = int(tt);
-    *r = int(i - tt * p.num_rx);
-    return true;
-}
-
-template <typename T, int NF>
-__global__ void __launch_bounds__(kBlock) k_main(MainParams p) {
-    extern __shared__ int stack[];
-    const long long gi = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    int t, r;
-    if (!cell_of(p, gi, &t, &r)) return;
-    const SceneDev& sc = p.sc;
-    const V3<double> S = v3<double>(p.tx_pos[3 * t], p.tx_pos[3 * t + 1], p.tx_pos[3 * t + 2]);
-    const V3<float> Rf = rx_position<float>(p, r);
-    const V3<double> R = cast3<double>(Rf);
-    const V3<T> ST = cast3<T>(S), RT = cast3<T>(R);
-    const V3<T> tx_pol = v3<T>(T(p.tx_pol[3 * t]), T(p.tx_pol[3 * t + 1]), T(p.tx_pol[3 * t + 2]));
-    const float* rp = p.rx_pol + (long long)r * p.rx_pol_stride;
-    const V3<T> rx_pol = v3<T>(T(rp[0]), T(rp[1]), T(rp[2]));
-    const T sqrt_p = s_sqrt(s_max(T(p.tx_power[t]), T(0)));
-    Accum<T> acc[NF];
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
-        for (int s = 0; s < 4; ++s) { acc[f].slot[s] = cx(T(0), T(0)); acc[f].gain[s] = T(0); }
-        for (int s = 0; s < 3; ++s) acc[f].dv[s] = cx(T(0), T(0));
-    }
-    int* err = p.status;
-    unsigned long long rays = 0;
-    // -------------------------------------------------------------- LoS
-    if (p.components & 1) {
-        const bool blocked = sc.num_faces > 0 && segment_blocked<T>(sc, ST, RT, ignore_none(), stack, err);
-        if (sc.num_faces > 0) ++rays;
-        if (!blocked) {
-            const double dist = length(R - S);
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const PathEval<T> ev = eval_free_space(ST, RT, tx_pol, rx_pol, p.k[f], dist);
-                const Cx<T> pf = ev.coefficient * sqrt_p;
-                acc[f].slot[0] = acc[f].slot[0] + pf;
-                acc[f].gain[0] = acc[f].gain[0] + cabs2(pf);
-            }
-            emit_row(p, t, r, 0, 0, nullptr, -1, float(dist));
-        }
-    }
-    // -------------------------------------------------------------- reflection
-    if ((p.components & 2) && sc.num_faces > 0) {
-        for (int d = 1; d <= p.max_depth; ++d) {
-            const int cnt = p.chain_count[t * kMaxDepth + (d - 1)];
-            const long long base = p.chain_offset[t * kMaxDepth + (d - 1)];
-            const int* cg = p.chain_groups + base * 1;  // offsets are in int units (chain * depth)
-            const double* cpl = p.chain_planes + base * 4;
-            const double* cim = p.chain_images + base * 3;
-            for (int c = 0; c < cnt; ++c) {
-                const int* groups = cg + (long long)c * d;
-                const double* planes = cpl + (long long)c * d * 4;
-                const double* images = cim + (long long)c * d * 3;
-                if (sizeof(T) == 4 && !back_project_prefilter(sc, Rf, groups, planes, images, d)) continue;
-                V3<double> hits[kMaxDepth];
-                if (!back_project(R, planes, images, d, hits)) continue;
-                int faces[kMaxDepth];
-                bool ok = true;
-                for (int k = d - 1; k >= 0 && ok; --k) {
-                    faces[k] = resolve_in_group(sc, groups[k], hits[k]);
-                    ok = faces[k] >= 0;
-                }
-                if (!ok) continue;
-                // visibility of the d+1 segments
-                for (int s = 0; s <= d && ok; ++s) {
-                    const V3<double> a = s == 0 ? S : hits[s - 1];
-                    const V3<double> b = s == d ? R : hits[s];
-                    Ignore ig = ignore_none();
-                    ig.g0 = s > 0 ? groups[s - 1] : -1;
-                    ig.g1 = s < d ? groups[s] : -1;
-                    ++rays;
-                    if (segment_blocked<T>(sc, cast3<T>(a), cast3<T>(b), ig, stack, err)) ok = false;
-                }
-                if (!ok) continue;
-                const V3<double> img = v3(images[3 * (d - 1)], images[3 * (d - 1) + 1], images[3 * (d - 1) + 2]);
-                const double total = length(R - img);
-#pragma unroll
-                for (int f = 0; f < NF; ++f) {
-                    const double freq = p.freq[f];
-                    const T wl = T(kC0 / freq);
-                    const V3<T> ez = v3<T>(T(0), T(0), T(1));
-                    V3<T> prev = ST;
-                    V3<T> incident = safe_normalize(cast3<T>(hits[0]) - prev, ez);
-                    C3<T> value = c3_from_real(transverse(incident, tx_pol));
-                    V3<T> outgoing = incident;
-                    for (int k = 0; k < d; ++k) {
-                        const V3<T> hit = cast3<T>(hits[k]);
-                        incident = safe_normalize(hit - prev, outgoing);
-                        const float* nf = sc.face_normal + 3 * faces[k];
-                        reflect_bounce(value, outgoing, incident, v3<T>(T(nf[0]), T(nf[1]), T(nf[2])),
-                                       face_slab<T>(p, f, faces[k]), freq, wl);
-                        prev = hit;
-                    }
-                    const V3<T> fdir = safe_normalize(RT - prev, outgoing);
-                    const T amp = T(1) / (T(2) * T(p.k[f]) * T(fmax(total, kUtdEps)));
-                    const Cx<T> prop = phasor_neg_kd<T>(p.k[f], total) * amp;
-                    value = c3_scale(value, prop);
-                    const Cx<T> pf = project_receiver(value, fdir, rx_pol) * sqrt_p;
-                    acc[f].slot[1] = acc[f].slot[1] + pf;
-                    acc[f].gain[1] = acc[f].gain[1] + cabs2(pf);
-                }
-                emit_row(p, t, r, 1, d, faces, -1, float(total));
-            }
-        }
-    }
-    // -------------------------------------------------------------- diffraction
-    if ((p.components & 4) && sc.num_edges > 0 && p.max_depth >= 1) {
-        const int cnt = p.edge_count[t];
-        const int* list = p.edge_list + (long long)t * sc.num_edges;
-        for (int j = 0; j < cnt; ++j) {
-            const EdgeDev& ed = sc.edges[list[j]];
-            C3<T> fields[NF];
-            bool any = false;
-            bool valid = false;
-            DiffractionResult<T> res;
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const int m0 = ed.mat_face0, mn = ed.mat_face1;
-                res = utd_field<T>(ed, S, R, tx_pol, face_slab<T>(p, f, m0), face_slab<T>(p, f, mn), p.freq[f]);
-                valid = res.valid;
-                fields[f] = res.field;
-                if (res.valid && value_of(c3_power(res.field)) * value_of(sqrt_p * sqrt_p) >= kUtdGainFloor) any = true;
-            }
-            if (!valid || !any) continue;
-            Ignore ig = ignore_none();
-            ig.f0 = ed.face0;
-            ig.f1 = ed.face1;
-            const V3<double> qv = v3(res.q_vis[0], res.q_vis[1], res.q_vis[2]);
-            ++rays;
-            if (segment_blocked<T>(sc, ST, cast3<T>(qv), ig, stack, err)) continue;
-            ++rays;
-            if (segment_blocked<T>(sc, cast3<T>(qv), RT, ig, stack, err)) continue;
-            const V3<double> q = v3(res.q[0], res.q[1], res.q[2]);
-            const V3<T> arrival = safe_normalize(cast3<T>(R - q), v3<T>(T(0), T(0), T(1)));
-            bool emitted = false;
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const C3<T> powered = c3_scale(fields[f], cx(sqrt_p, T(0)));
-                if (value_of(c3_power(powered)) < kUtdGainFloor) continue;
-                const Cx<T> pf = project_receiver(powered, arrival, rx_pol);
-                acc[f].slot[2] = acc[f].slot[2] + pf;
-                acc[f].gain[2] = acc[f].gain[2] + cabs2(pf);
-                acc[f].dv[0] = acc[f].dv[0] + powered.x;
-                acc[f].dv[1] = acc[f].dv[1] + powered.y;
-                acc[f].dv[2] = acc[f].dv[2] + powered.z;
-                if (!emitted) {
-                    emit_row(p, t, r, 2, 1, nullptr, ed.edge_id, float(res.length));
-                    emitted = true;
-                }
-            }
-        }
-    }
-    // -------------------------------------------------------------- transmission
-    if ((p.components & 8) && sc.num_faces > 0 && p.max_depth >= 1) {
-        HitList hl;
-        ++rays;
-        segment_hits<T>(sc, ST, RT, p.max_depth, &hl, stack, err);
-        if (hl.count > p.max_depth) {
-            if (p.overflow_counter) atomicAdd(p.overflow_counter, 1ull);
-        } else if (hl.count >= 1) {
-            bool ok = true;
-            for (int i = 0; i < hl.count; ++i) {
-                const int m = sc.face_material[hl.face[i]];
-                if (p.mat_volumetric && p.mat_volumetric[m]) ok = false;
-            }
-            if (ok) {
-                const double dist = length(R - S);
-                const V3<T> dir = safe_normalize(RT - ST, v3<T>(T(0), T(0), T(1)));
-#pragma unroll
-                for (int f = 0; f < NF; ++f) {
-                    C3<T> value = c3_from_real(transverse(dir, tx_pol));
-                    T shorten = T(0);
-                    const LayerTable<T> lt = layer_table_f<T>(p, f);
-                    for (int i = 0; i < hl.count; ++i) {
-                        const float* nf = sc.face_normal + 3 * hl.face[i];
-                        transmit_wall(value, shorten, dir, v3<T>(T(nf[0]), T(nf[1]), T(nf[2])),
-                                      sc.face_material[hl.face[i]], lt, p.freq[f]);
-                    }
-                    const T amp = T(1) / (T(2) * T(p.k[f]) * T(fmax(dist, kUtdEps)));
-                    const Cx<T> prop = phasor_neg_kd<T>(p.k[f], dist - double(value_of(shorten))) * amp;
-                    value = c3_scale(value, prop);
-                    const Cx<T> pf = project_receiver(value, dir, rx_pol) * sqrt_p;
-                    acc[f].slot[3] = acc[f].slot[3] + pf;
-                    acc[f].gain[3] = acc[f].gain[3] + cabs2(pf);
-                }
-                emit_row(p, t, r, 5, hl.count, hl.face, -1, float(dist));
-            }
-        }
-    }
-    // -------------------------------------------------------------- outputs
-    if (p.ray_counter && p.freq_base == 0 && rays) atomicAdd(p.ray_counter, rays);
-    const long long cells = (long long)p.num_tx * p.num_rx;
-    const long long cell = (long long)t * p.num_rx + r;
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
-        const long long fc = (long long)(p.freq_base + f) * cells + cell;
-        const long long slot_stride = (long long)p.num_freq_total * cells;
-        Cx<T> total = cx(T(0), T(0));
-        T gsum = T(0);
-        for (int s = 0; s < 4; ++s) {
-            total = total + acc[f].slot[s];
-            gsum = gsum + acc[f].gain[s];
-        }
-        T* pg = static_cast<T*>(p.out_path_gain);
-        T* fl = static_cast<T*>(p.out_field);
-        T* cp = static_cast<T*>(p.out_comp_power);
-        T* cf = static_cast<T*>(p.out_comp_field);
-        T* dvp = static_cast<T*>(p.out_diff_vec_power);
-        if (p.coherent) {
-            if (pg) pg[fc] = cabs2(total);
-            if (fl) { fl[2 * fc] = total.re; fl[2 * fc + 1] = total.im; }
-        } else {
-            if (pg) pg[fc] = gsum;
-            if (fl) { fl[2 * fc] = s_sqrt(s_max(gsum, T(0))); fl[2 * fc + 1] = T(0); }
-        }
-        for (int s = 0; s < 6; ++s) {
-            const long long o = s * slot_stride + fc;
-            const Cx<T> v = s < 4 ? acc[f].slot[s] : cx(T(0), T(0));
-            if (cp) cp[o] = s < 4 ? (p.coherent ? cabs2(v) : acc[f].gain[s]) : T(0);
-            if (cf) { cf[2 * o] = v.re; cf[2 * o + 1] = v.im; }
-        }
-        if (dvp) dvp[fc] = cabs2(acc[f].dv[0]) + cabs2(acc[f].dv[1]) + cabs2(acc[f].dv[2]);
-    }
-}
-
 __global__ void k_to_double(long long n, const float* in, double* out) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < n) out[i] = in[i];
+}
+
+
+template <typename T, int NF>
+void launch_nf(const MainParams& q, unsigned blocks, int sdepth, size_t stack_bytes, cudaStream_t stream) {
+    const int c = q.components;
+    if (c & (1 | 8)) {
+        k_los_trans<T, NF><<<blocks, kCompBlock, stack_bytes, stream>>>(q);
+        note_launch();
+    }
+    if (c & 2) {
+        const size_t bytes = stack_bytes + kWarpsPerBlock * sizeof(ReflShared<NF>);
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_reflect<T, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            attr = true;
+        }
+        k_reflect<T, NF><<<blocks, kCompBlock, bytes, stream>>>(q, sdepth);
+        note_launch();
+    }
+    if (c & 4) {
+        const size_t bytes = stack_bytes + kWarpsPerBlock * sizeof(DiffShared<NF>);
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_diffract<T, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            attr = true;
+        }
+        k_diffract<T, NF><<<blocks, kCompBlock, bytes, stream>>>(q, sdepth);
+        note_launch();
+    }
+}
+
+template <typename T>
+void launch_components(const MainParams& q, int nf, unsigned blocks, int sdepth, size_t stack_bytes, cudaStream_t stream) {
+    switch (nf) {
+        case 1: launch_nf<T, 1>(q, blocks, sdepth, stack_bytes, stream); break;
+        case 2: launch_nf<T, 2>(q, blocks, sdepth, stack_bytes, stream); break;
+        case 3: launch_nf<T, 3>(q, blocks, sdepth, stack_bytes, stream); break;
+        default: launch_nf<T, 4>(q, blocks, sdepth, stack_bytes, stream); break;
+    }
 }
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
@@ -872,14 +600,10 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         p.layer_sigma_e64 = layers64 + 2 * n;
         p.layer_mu_r64 = layers64 + 3 * n;
     }
-    long long threads;
-    if (d->rx_kind == 1) {
-        const long long tiles = (long long)((d->grid_rows + 7) / 8) * ((d->grid_cols + 3) / 4);
-        threads = tiles * 32 * T;
-    } else {
-        threads = (long long)R * T;
-    }
-    const long long blocks = (threads + kBlock - 1) / kBlock;
+    const long long tiles = tiles_per_tx(p) * T;
+    const long long blocks = (tiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int sdepth = std::max(8, std::min(kStackDepth, sc.max_depth + 2));
+    const size_t stack_bytes = size_t(sdepth) * kCompBlock * 4;
     if (prof.enabled) cudaEventRecord(ev_main0, stream);
     for (int fb = 0; fb < d->num_freq; fb += kMaxNF) {
         const int nf = std::min(kMaxNF, d->num_freq - fb);
@@ -908,24 +632,13 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
             q.layer_mu_r64 = p.layer_mu_r64 + lo;
         }
         if (fb > 0) q.rows = nullptr;  // geometry rows are emitted once
-        if (blocks > 0) {
-            if (fp64) {
-                switch (nf) {
-                    case 1: k_main<double, 1><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
-                    case 2: k_main<double, 2><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
-                    case 3: k_main<double, 3><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
-                    default: k_main<double, 4><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
-                }
-            } else {
-                switch (nf) {
-                    case 1: k_main<float, 1><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
-                    case 2: k_main<float, 2><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
-                    case 3: k_main<float, 3><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
-                    default: k_main<float, 4><<<unsigned(blocks), kBlock, smem, stream>>>(q); break;
-                }
-            }
-            note_launch();
-        }
+        if (blocks <= 0) continue;
+        if (fp64) launch_components<double>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream);
+        else launch_components<float>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream);
+        const long long nfin = (long long)T * R * nf;
+        if (fp64) k_finalize<double><<<unsigned((nfin + 255) / 256), 256, 0, stream>>>(q, nf);
+        else k_finalize<float><<<unsigned((nfin + 255) / 256), 256, 0, stream>>>(q, nf);
+        note_launch();
     }
     if (prof.enabled) {
         cudaEventRecord(ev_main1, stream);
@@ -950,10 +663,6 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     return 0;
 }
 
-int solve_set_smem_limits() {
-    const int smem = kStackDepth * kBlock * 4;
-    cudaFuncSetAttribute(k_main<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    return 0;
-}
+
 
 }  // namespace wcb
