@@ -41,7 +41,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "radiomap rays/s (urban canyon, 64 boxes, 256x256 grid, 28 GHz, depth 3 + UTD)"
 UNIT = "rays/s"
 HBM_FALLBACK = 6650.0
-PROFILE_SUMMARY = ROOT / "profiles" / "k_main_urban_canyon.md"
+PROFILE_SUMMARY = ROOT / "profiles" / "urban_canyon_kernels.md"
 
 
 def _peaks() -> dict:
@@ -54,11 +54,14 @@ def _peaks() -> dict:
     return {}
 
 
-def _traffic_per_launch() -> float | None:
+def _traffic_per_launch(kernel: str) -> float | None:
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (a line ``traffic_bytes_per_launch[<kernel>]: <bytes>``)."""
     if not PROFILE_SUMMARY.exists():
         return None
+    key = f"traffic_bytes_per_launch[{kernel}]:"
     for line in PROFILE_SUMMARY.read_text().splitlines():
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+        if line.strip().startswith(key):
             try:
                 return float(line.split(":", 1)[1].strip())
             except ValueError:
@@ -173,6 +176,9 @@ def run_native(args) -> None:
     main_rays = 0
     main_ms = 0.0
     main_launches = 0
+    kernel_ms: dict[str, float] = {}
+    kernel_rays: dict[str, int] = {}
+    last_prof: dict = {}
     sampler = ClockSampler(local)
     t_wall0 = time.perf_counter()
     with sampler:
@@ -187,6 +193,11 @@ def run_native(args) -> None:
             main_rays += prof["rays"]
             main_ms += prof["main_ms"]
             main_launches += prof["main_launches"]
+            for k, v in prof["kernel_ms"].items():
+                kernel_ms[k] = kernel_ms.get(k, 0.0) + v
+            for k, v in prof["kernel_rays"].items():
+                kernel_rays[k] = kernel_rays.get(k, 0) + v
+            last_prof = prof
         torch.cuda.synchronize()
     t_wall = time.perf_counter() - t_wall0
     launches = _native.launch_count() - launches0
@@ -231,11 +242,13 @@ def run_native(args) -> None:
         peaks = _peaks()
         hbm = float(peaks.get("hbm_gbs", HBM_FALLBACK))
         cells_n = ep.num_tx * ep.num_rx
-        bytes_per_launch = (main_rays / args.steps) * _bytes_per_ray(faces) / max(main_launches / args.steps, 1) \
-            + cells_n * B_CELL
-        launch_ms = main_ms / max(main_launches, 1)
-        achieved = bytes_per_launch / (launch_ms / 1000.0) / 1e9
-        traffic = _traffic_per_launch()
+        # dominant per-cell kernel: its rays and the slot bytes it writes per cell
+        dominant = max(("k_reflect", "k_diffract", "k_los_trans"), key=lambda k: kernel_ms.get(k, 0.0))
+        cell_bytes = {"k_reflect": 12, "k_diffract": 16, "k_los_trans": 12}[dominant]
+        bytes_per_launch = kernel_rays.get(dominant, 0) / args.steps * _bytes_per_ray(faces) + cells_n * cell_bytes
+        launch_ms = kernel_ms.get(dominant, 0.0) / args.steps
+        achieved = bytes_per_launch / (launch_ms / 1000.0) / 1e9 if launch_ms > 0 else 0.0
+        traffic = _traffic_per_launch(dominant)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline(scene, freq, cfg, budget_s=args.cpu_budget, cores=1)
@@ -260,7 +273,11 @@ def run_native(args) -> None:
                 "frequency_hz": freq,
                 "max_depth": 3,
                 "rays_per_step": rays / args.steps,
-                "main_kernel_rays_per_step": main_rays / args.steps,
+                "per_cell_kernel_rays_per_step": main_rays / args.steps,
+                "kernel_ms_per_step": {k: v / args.steps for k, v in kernel_ms.items()},
+                "kernel_rays_per_step": {k: v / args.steps for k, v in kernel_rays.items()},
+                "reflection_candidates_per_depth": last_prof.get("chains"),
+                "diffraction_edges_after_prefilter": last_prof.get("edges"),
                 "cells_per_step": cells_n,
                 "l2": "flushed (256 MiB write) before every timed step",
                 "parallelism": f"replicas x{world} (one transmitter per rank)",
@@ -269,7 +286,7 @@ def run_native(args) -> None:
                     "d2h_bytes_per_step": d2h // e2e_steps, "ms_per_step": e2e_ms / e2e_steps},
             "roofline": {
                 "bound": "hbm",
-                "kernel": "k_main (fused LoS/reflection/diffraction per cell)",
+                "kernel": dominant,
                 "achieved": achieved,
                 "peak": hbm,
                 "unit": "GB/s",

@@ -227,7 +227,11 @@ int wcb_field_project_complex3(int64_t n, const float* field_vector, const float
  * (segment visibility / penetration queries) the main kernel traces.
  * wcb_profile_read returns the last solve's figures: values[0] main-kernel ms,
  * values[1] preparation ms, values[2] main-kernel rays, values[3] main-kernel
- * launches, values[4] preparation rays (discovery bounces, edge prefilter). */
+ * launches, values[4] preparation rays (discovery bounces, edge prefilter),
+ * values[5..8] ms of the LoS+transmission, reflection, diffraction and
+ * finalize kernels, values[9..11] rays of the first three, values[12..16]
+ * reflection candidates per depth and values[17] prefiltered diffraction
+ * edges (both for the first transmitter).  `values` holds 18 doubles. */
 int wcb_profile_enable(int32_t enabled);
 int wcb_profile_read(double* values);
 

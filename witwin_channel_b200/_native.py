@@ -229,10 +229,13 @@ def profile_enable(enabled: bool) -> None:
 
 
 def profile_read() -> dict:
-    vals = (ctypes.c_double * 5)()
+    vals = (ctypes.c_double * 18)()
     check(load().wcb_profile_read(vals), "wcb_profile_read")
     return {"main_ms": vals[0], "prep_ms": vals[1], "rays": int(vals[2]), "main_launches": int(vals[3]),
-            "prep_rays": int(vals[4])}
+            "prep_rays": int(vals[4]),
+            "kernel_ms": {"k_los_trans": vals[5], "k_reflect": vals[6], "k_diffract": vals[7], "k_finalize": vals[8]},
+            "kernel_rays": {"k_los_trans": int(vals[9]), "k_reflect": int(vals[10]), "k_diffract": int(vals[11])},
+            "chains": [int(v) for v in vals[12:17]], "edges": int(vals[17])}
 
 
 def build_info() -> str:

@@ -186,6 +186,10 @@ int wcb_profile_read(double* values) {
     values[2] = double(st.rays);
     values[3] = double(st.main_launches);
     values[4] = double(st.prep_rays);
+    for (int i = 0; i < 4; ++i) values[5 + i] = st.kernel_ms[i];
+    for (int i = 0; i < 3; ++i) values[9 + i] = double(st.kernel_rays[i]);
+    for (int i = 0; i < 5; ++i) values[12 + i] = double(st.chains[i]);
+    values[17] = double(st.edges);
     return WCB_OK;
 }
 

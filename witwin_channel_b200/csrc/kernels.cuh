@@ -18,8 +18,10 @@
 
 namespace wcb {
 
-constexpr int kWarpsPerBlock = 4;
+constexpr int kWarpsPerBlock = 4;              // LoS/transmission: one tile per warp
 constexpr int kCompBlock = kWarpsPerBlock * 32;
+constexpr int kSplitWarps = 8;                 // reflection/diffraction: one tile per block,
+constexpr int kSplitBlock = kSplitWarps * 32;  // its candidates interleaved over 8 warps
 constexpr int kQueueCap = 64;
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -256,13 +258,14 @@ struct ReflShared {
 };
 
 template <typename T, int NF>
-__global__ void __launch_bounds__(kCompBlock) k_reflect(MainParams p, int stack_depth) {
+__global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int stack_depth) {
     extern __shared__ int smem[];
     int* stack = smem;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    ReflShared<NF>* sh = reinterpret_cast<ReflShared<NF>*>(smem + stack_depth * kCompBlock) + warp;
-    const long long tile = (long long)blockIdx.x * kWarpsPerBlock + warp;
+    ReflShared<NF>* sh = reinterpret_cast<ReflShared<NF>*>(smem + stack_depth * kSplitBlock) + warp;
+    float* red = reinterpret_cast<float*>(reinterpret_cast<ReflShared<NF>*>(smem + stack_depth * kSplitBlock) + kSplitWarps);
+    const long long tile = blockIdx.x;
     int t = 0, r = 0;
     const bool active = tile_cell(p, tile, lane, &t, &r);
     // the whole warp shares the tile's transmitter
@@ -284,6 +287,7 @@ __global__ void __launch_bounds__(kCompBlock) k_reflect(MainParams p, int stack_
     for (int f = 0; f < NF; ++f) { acc[f] = cx(T(0), T(0)); gain[f] = T(0); }
     unsigned long long rays = 0;
     int qa = 0, qb = 0;
+    int global_c = 0;  // running candidate index across depths (interleaving key)
 
     // stage B: visibility + field for 32 items (FP64 hits recomputed)
     auto process_b = [&](int n) {
@@ -429,12 +433,13 @@ __global__ void __launch_bounds__(kCompBlock) k_reflect(MainParams p, int stack_
         for (int d = 1; d <= p.max_depth; ++d) {
             const int cnt = p.chain_count[t * kMaxDepth + (d - 1)];
             const long long base = p.chain_offset[t * kMaxDepth + (d - 1)];
-            for (int c = 0; c < cnt; ++c) {
+            // this warp takes every kSplitWarps-th candidate of the transmitter
+            const int first = (warp - global_c % kSplitWarps + kSplitWarps) % kSplitWarps;
+            global_c += cnt;
+            for (int c = first; c < cnt; c += kSplitWarps) {
                 bool pass = active;
                 if (sizeof(T) == 4 && pass) {
-                    pass = back_project_prefilter(sc, Rf, p.chain_groups + base + (long long)c * d,
-                                                  p.chain_planes + (base + (long long)c * d) * 4,
-                                                  p.chain_images + (base + (long long)c * d) * 3, d);
+                    pass = back_project_prefilter(sc, Rf, p.chain_pre + (base + c) * 2);
                 }
                 qa = queue_push(sh->qa, qa, pass, lane, c, d);
                 if (qa >= 32) {
@@ -451,9 +456,26 @@ __global__ void __launch_bounds__(kCompBlock) k_reflect(MainParams p, int stack_
             process_b(qb);
             qb = 0;
         }
-        if (active) {
+        // fixed-order reduction of the warps' partial sums, one write per cell
+        for (int f = 0; f < NF; ++f) {
+            float* o = red + ((warp * 32 + lane) * NF + f) * 3;
+            o[0] = float(value_of(acc[f].re));
+            o[1] = float(value_of(acc[f].im));
+            o[2] = float(value_of(gain[f]));
+        }
+        __syncthreads();
+        if (warp == 0 && active) {
             const long long cell = (long long)t * p.num_rx + r;
-            for (int f = 0; f < NF; ++f) store_slot(p, 1, f, cell, acc[f], gain[f], p.coherent);
+            for (int f = 0; f < NF; ++f) {
+                Cx<T> sum = cx(T(0), T(0));
+                T g = T(0);
+                for (int w = 0; w < kSplitWarps; ++w) {
+                    const float* o = red + ((w * 32 + lane) * NF + f) * 3;
+                    sum = sum + cx(T(o[0]), T(o[1]));
+                    g = g + T(o[2]);
+                }
+                store_slot(p, 1, f, cell, sum, g, p.coherent);
+            }
         }
     }
     if (p.ray_counter && p.freq_base == 0 && rays) atomicAdd(p.ray_counter, rays);
@@ -468,13 +490,14 @@ struct DiffShared {
 };
 
 template <typename T, int NF>
-__global__ void __launch_bounds__(kCompBlock) k_diffract(MainParams p, int stack_depth) {
+__global__ void __launch_bounds__(kSplitBlock, 2) k_diffract(MainParams p, int stack_depth) {
     extern __shared__ int smem[];
     int* stack = smem;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    DiffShared<NF>* sh = reinterpret_cast<DiffShared<NF>*>(smem + stack_depth * kCompBlock) + warp;
-    const long long tile = (long long)blockIdx.x * kWarpsPerBlock + warp;
+    DiffShared<NF>* sh = reinterpret_cast<DiffShared<NF>*>(smem + stack_depth * kSplitBlock) + warp;
+    float* red = reinterpret_cast<float*>(reinterpret_cast<DiffShared<NF>*>(smem + stack_depth * kSplitBlock) + kSplitWarps);
+    const long long tile = blockIdx.x;
     int t = 0, r = 0;
     const bool active = tile_cell(p, tile, lane, &t, &r);
     const long long per_tx = tiles_per_tx(p);
@@ -567,7 +590,7 @@ __global__ void __launch_bounds__(kCompBlock) k_diffract(MainParams p, int stack
         __syncwarp();
     };
 
-    for (int j = 0; j < cnt; ++j) {
+    for (int j = warp; j < cnt; j += kSplitWarps) {
         bool vis = false;
         if (active) {
             // visibility of the biased, clamped stationary point
@@ -604,13 +627,34 @@ __global__ void __launch_bounds__(kCompBlock) k_diffract(MainParams p, int stack
         process_v(qv);
         qv = 0;
     }
-    if (active && cnt >= 0 && (p.components & 4)) {
+    // fixed-order reduction of the warps' partial sums, one write per cell
+    for (int f = 0; f < NF; ++f) {
+        float* o = red + ((warp * 32 + lane) * NF + f) * 9;
+        o[0] = float(value_of(acc[f].re));
+        o[1] = float(value_of(acc[f].im));
+        o[2] = float(value_of(gain[f]));
+        for (int k = 0; k < 3; ++k) {
+            o[3 + 2 * k] = float(value_of(dv[f][k].re));
+            o[4 + 2 * k] = float(value_of(dv[f][k].im));
+        }
+    }
+    __syncthreads();
+    if (warp == 0 && active && (p.components & 4)) {
         const long long cell = (long long)t * p.num_rx + r;
         const long long cells = (long long)p.num_tx * p.num_rx;
         for (int f = 0; f < NF; ++f) {
-            store_slot(p, 2, f, cell, acc[f], gain[f], p.coherent);
+            Cx<T> sum = cx(T(0), T(0));
+            T g = T(0);
+            Cx<T> v[3] = {cx(T(0), T(0)), cx(T(0), T(0)), cx(T(0), T(0))};
+            for (int w = 0; w < kSplitWarps; ++w) {
+                const float* o = red + ((w * 32 + lane) * NF + f) * 9;
+                sum = sum + cx(T(o[0]), T(o[1]));
+                g = g + T(o[2]);
+                for (int k = 0; k < 3; ++k) v[k] = v[k] + cx(T(o[3 + 2 * k]), T(o[4 + 2 * k]));
+            }
+            store_slot(p, 2, f, cell, sum, g, p.coherent);
             T* dvp = static_cast<T*>(p.out_diff_vec_power);
-            if (dvp) dvp[(long long)(p.freq_base + f) * cells + cell] = cabs2(dv[f][0]) + cabs2(dv[f][1]) + cabs2(dv[f][2]);
+            if (dvp) dvp[(long long)(p.freq_base + f) * cells + cell] = cabs2(v[0]) + cabs2(v[1]) + cabs2(v[2]);
         }
     }
     if (p.ray_counter && p.freq_base == 0 && rays) atomicAdd(p.ray_counter, rays);

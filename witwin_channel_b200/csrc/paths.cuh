@@ -70,19 +70,19 @@ WCB_D bool back_project(V3<double> R, const double* planes, const double* images
 
 // FP32 pre-test of the last bounce: the back-projected point must fall in the
 // (padded) group box.  Conservative: it only rejects candidates whose FP64
-// solve fails too.
-WCB_D bool back_project_prefilter(const SceneDev& sc, V3<float> R, const int* groups, const double* planes,
-                                  const double* images, int depth) {
-    const int k = depth - 1;
-    const V3<float> n = v3<float>(float(planes[4 * k]), float(planes[4 * k + 1]), float(planes[4 * k + 2]));
-    const float off = float(planes[4 * k + 3]);
-    const V3<float> img = v3<float>(float(images[3 * k]), float(images[3 * k + 1]), float(images[3 * k + 2]));
+// solve fails too.  `pre` holds the chain's last plane and last image.
+WCB_D bool back_project_prefilter(const SceneDev& sc, V3<float> R, const float4* pre) {
+    const float4 pl = __ldg(pre);
+    const float4 im = __ldg(pre + 1);
+    const V3<float> n = v3(pl.x, pl.y, pl.z);
+    const float off = pl.w;
+    const V3<float> img = v3(im.x, im.y, im.z);
     const float denom = dot(img - R, n);
     if (fabsf(denom) < 1e-30f) return true;  // leave the decision to FP64
     const float t = (off - dot(R, n)) / denom;
     if (!(t > -1e-3f && t < 1.0f + 1e-3f)) return false;
     const V3<float> x = R + (img - R) * t;
-    const float* bx = sc.group_box + 6 * groups[k];
+    const float* bx = sc.group_box + 6 * __float_as_int(im.w);
     const float pad = 1e-2f + 1e-5f * (fabsf(x.x) + fabsf(x.y) + fabsf(x.z));
     return !(x.x < bx[0] - pad || x.y < bx[1] - pad || x.z < bx[2] - pad || x.x > bx[3] + pad || x.y > bx[4] + pad ||
              x.z > bx[5] + pad);

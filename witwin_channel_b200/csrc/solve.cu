@@ -162,7 +162,7 @@ __global__ void k_exhaustive_chains(long long total, int depth, int groups_n, in
 
 // FP64 images of the source through each chain's group planes.
 __global__ void k_chain_images(SceneDev sc, const float* tx, int depth, const int* count_ptr, long long count_fixed,
-                               const int* chain_groups, double* planes_out, double* images_out) {
+                               const int* chain_groups, double* planes_out, double* images_out, float4* pre_out) {
     long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const long long count = count_ptr ? *count_ptr : count_fixed;
     if (c >= count) return;
@@ -176,6 +176,11 @@ __global__ void k_chain_images(SceneDev sc, const float* tx, int depth, const in
         po[0] = pl[0]; po[1] = pl[1]; po[2] = pl[2]; po[3] = pl[3];
         double* io = images_out + (c * depth + k) * 3;
         io[0] = p.x; io[1] = p.y; io[2] = p.z;
+        if (k == depth - 1) {
+            // FP32 copy of the last plane and image for the prefilter
+            pre_out[2 * c] = make_float4(float(pl[0]), float(pl[1]), float(pl[2]), float(pl[3]));
+            pre_out[2 * c + 1] = make_float4(float(p.x), float(p.y), float(p.z), __int_as_float(g));
+        }
     }
 }
 
@@ -241,42 +246,59 @@ __global__ void k_to_double(long long n, const float* in, double* out) {
 }
 
 
+struct ComponentEvents {
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
 template <typename T, int NF>
-void launch_nf(const MainParams& q, unsigned blocks, int sdepth, size_t stack_bytes, cudaStream_t stream) {
-    const int c = q.components;
+void launch_nf(const MainParams& q0, unsigned blocks, int sdepth, size_t stack_bytes, cudaStream_t stream,
+               ComponentEvents* evs) {
+    const unsigned tiles = unsigned(tiles_per_tx(q0) * q0.num_tx);
+    const size_t split_stack = size_t(sdepth) * kSplitBlock * 4;
+    const int c = q0.components;
+    MainParams q = q0;
+    unsigned long long* rc = q0.ray_counter;
+    if (evs) cudaEventRecord(evs->ev[0], stream);
     if (c & (1 | 8)) {
+        q.ray_counter = rc ? rc + 0 : nullptr;
         k_los_trans<T, NF><<<blocks, kCompBlock, stack_bytes, stream>>>(q);
         note_launch();
     }
+    if (evs) cudaEventRecord(evs->ev[1], stream);
     if (c & 2) {
-        const size_t bytes = stack_bytes + kWarpsPerBlock * sizeof(ReflShared<NF>);
+        q.ray_counter = rc ? rc + 1 : nullptr;
+        const size_t bytes = split_stack + kSplitWarps * sizeof(ReflShared<NF>) + size_t(kSplitWarps) * 32 * NF * 3 * 4;
         static bool attr = false;
         if (!attr) {
             cudaFuncSetAttribute(k_reflect<T, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             attr = true;
         }
-        k_reflect<T, NF><<<blocks, kCompBlock, bytes, stream>>>(q, sdepth);
+        k_reflect<T, NF><<<tiles, kSplitBlock, bytes, stream>>>(q, sdepth);
         note_launch();
     }
+    if (evs) cudaEventRecord(evs->ev[2], stream);
     if (c & 4) {
-        const size_t bytes = stack_bytes + kWarpsPerBlock * sizeof(DiffShared<NF>);
+        q.ray_counter = rc ? rc + 2 : nullptr;
+        const size_t bytes = split_stack + kSplitWarps * sizeof(DiffShared<NF>) + size_t(kSplitWarps) * 32 * NF * 9 * 4;
         static bool attr = false;
         if (!attr) {
             cudaFuncSetAttribute(k_diffract<T, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             attr = true;
         }
-        k_diffract<T, NF><<<blocks, kCompBlock, bytes, stream>>>(q, sdepth);
+        k_diffract<T, NF><<<tiles, kSplitBlock, bytes, stream>>>(q, sdepth);
         note_launch();
     }
+    if (evs) cudaEventRecord(evs->ev[3], stream);
 }
 
 template <typename T>
-void launch_components(const MainParams& q, int nf, unsigned blocks, int sdepth, size_t stack_bytes, cudaStream_t stream) {
+void launch_components(const MainParams& q, int nf, unsigned blocks, int sdepth, size_t stack_bytes, cudaStream_t stream,
+                       ComponentEvents* evs) {
     switch (nf) {
-        case 1: launch_nf<T, 1>(q, blocks, sdepth, stack_bytes, stream); break;
-        case 2: launch_nf<T, 2>(q, blocks, sdepth, stack_bytes, stream); break;
-        case 3: launch_nf<T, 3>(q, blocks, sdepth, stack_bytes, stream); break;
-        default: launch_nf<T, 4>(q, blocks, sdepth, stack_bytes, stream); break;
+        case 1: launch_nf<T, 1>(q, blocks, sdepth, stack_bytes, stream, evs); break;
+        case 2: launch_nf<T, 2>(q, blocks, sdepth, stack_bytes, stream, evs); break;
+        case 3: launch_nf<T, 3>(q, blocks, sdepth, stack_bytes, stream, evs); break;
+        default: launch_nf<T, 4>(q, blocks, sdepth, stack_bytes, stream, evs); break;
     }
 }
 
@@ -332,7 +354,7 @@ static ChainPlan make_plan(const SceneDev& sc, int max_depth, int rays) {
 }
 
 struct WorkspaceLayout {
-    size_t chain_counts, chain_offsets, chain_groups, chain_planes, chain_images;
+    size_t chain_counts, chain_offsets, chain_groups, chain_planes, chain_images, chain_pre;
     size_t disc_dirs, disc_groups, disc_keys, disc_keys2, disc_vals, disc_vals2, disc_flags, disc_scan, disc_rank,
         disc_temp;
     size_t disc_temp_bytes;
@@ -356,6 +378,7 @@ static WorkspaceLayout layout_for(const SceneDev& sc, const wcb_solve_desc& d, c
     L.chain_groups = take(size_t(T) * ints * 4);
     L.chain_planes = take(size_t(T) * ints * 4 * 8);
     L.chain_images = take(size_t(T) * ints * 3 * 8);
+    L.chain_pre = take(size_t(T) * ints * 2 * 16);
     const bool disc = !(pl.exhaustive_o1 && pl.exhaustive_mb) && (d.components & 2);
     const size_t nr = disc ? size_t(rays) : 0;
     const int md = std::max(d.max_depth, 1);
@@ -381,7 +404,7 @@ static WorkspaceLayout layout_for(const SceneDev& sc, const wcb_solve_desc& d, c
     L.edge_flags = take(size_t(std::max(sc.num_edges, 1)) * 4);
     L.edge_list = take(size_t(T) * std::max(sc.num_edges, 1) * 4);
     L.edge_count = take(size_t(T) * 4);
-    L.overflow = take(32);
+    L.overflow = take(64);
     L.layers64 = 0;
     L.total = o;
     return L;
@@ -412,12 +435,13 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     int* chain_groups = reinterpret_cast<int*>(base + L.chain_groups);
     double* chain_planes = reinterpret_cast<double*>(base + L.chain_planes);
     double* chain_images = reinterpret_cast<double*>(base + L.chain_images);
+    float4* chain_pre = reinterpret_cast<float4*>(base + L.chain_pre);
     int* edge_flags = reinterpret_cast<int*>(base + L.edge_flags);
     int* edge_list = reinterpret_cast<int*>(base + L.edge_list);
     int* edge_count = reinterpret_cast<int*>(base + L.edge_count);
     unsigned long long* overflow = reinterpret_cast<unsigned long long*>(base + L.overflow);
     unsigned long long* ray_counter = overflow + 1;       // preparation rays (discovery, edge prefilter)
-    unsigned long long* main_ray_counter = overflow + 2;  // main-kernel rays
+    unsigned long long* main_ray_counter = overflow + 2;  // per-cell kernel rays: los+trans, reflection, diffraction
     const bool fp64 = d->precision == 1;
     ProfileState& prof = profile_state();
     cudaEvent_t ev_prep = nullptr, ev_main0 = nullptr, ev_main1 = nullptr;
@@ -434,7 +458,7 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     if (T == 0 || R == 0) return 0;
     cudaMemsetAsync(chain_counts, 0, size_t(T) * kMaxDepth * 4, stream);
     cudaMemsetAsync(edge_count, 0, size_t(T) * 4, stream);
-    cudaMemsetAsync(overflow, 0, 32, stream);
+    cudaMemsetAsync(overflow, 0, 64, stream);
     if (out->status) cudaMemsetAsync(out->status, 0, 4, stream);
     if (out->row_count) cudaMemsetAsync(out->row_count, 0, 8, stream);
     // chain offsets (in chain-int units, per tx)
@@ -496,12 +520,13 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                 int* cgrp = chain_groups + offs[t * kMaxDepth + k];
                 double* cpl = chain_planes + offs[t * kMaxDepth + k] * 4;
                 double* cim = chain_images + offs[t * kMaxDepth + k] * 3;
+                float4* cpre = chain_pre + offs[t * kMaxDepth + k] * 2;
                 if (exh) {
                     const long long total = pl.cap[k];
                     fixed_counts[t * kMaxDepth + k] = int(total);
                     if (total > 0) {
                         k_exhaustive_chains<<<int((total + B - 1) / B), B, 0, stream>>>(total, depth, sc.num_groups, cgrp);
-                        k_chain_images<<<int((total + B - 1) / B), B, 0, stream>>>(sc, txp, depth, nullptr, total, cgrp, cpl, cim);
+                        k_chain_images<<<int((total + B - 1) / B), B, 0, stream>>>(sc, txp, depth, nullptr, total, cgrp, cpl, cim, cpre);
                         note_launch(2);
                     }
                     cudaMemcpyAsync(chain_counts + t * kMaxDepth + k, &fixed_counts[t * kMaxDepth + k], 4,
@@ -509,7 +534,7 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                 } else {
                     const long long cap = pl.cap[k];
                     k_chain_images<<<int((cap + B - 1) / B), B, 0, stream>>>(sc, txp, depth, chain_counts + t * kMaxDepth + k,
-                                                                           0, cgrp, cpl, cim);
+                                                                           0, cgrp, cpl, cim, cpre);
                     note_launch();
                 }
             }
@@ -571,6 +596,7 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     p.chain_groups = chain_groups;
     p.chain_planes = chain_planes;
     p.chain_images = chain_images;
+    p.chain_pre = chain_pre;
     p.edge_count = edge_count;
     p.edge_list = edge_list;
     p.out_path_gain = out->path_gain;
@@ -605,6 +631,10 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     const int sdepth = std::max(8, std::min(kStackDepth, sc.max_depth + 2));
     const size_t stack_bytes = size_t(sdepth) * kCompBlock * 4;
     if (prof.enabled) cudaEventRecord(ev_main0, stream);
+    ComponentEvents cev;
+    double comp_ms[4] = {0, 0, 0, 0};
+    if (prof.enabled)
+        for (int i = 0; i < 5; ++i) cudaEventCreate(&cev.ev[i]);
     for (int fb = 0; fb < d->num_freq; fb += kMaxNF) {
         const int nf = std::min(kMaxNF, d->num_freq - fb);
         p.freq_base = fb;
@@ -633,17 +663,31 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         }
         if (fb > 0) q.rows = nullptr;  // geometry rows are emitted once
         if (blocks <= 0) continue;
-        if (fp64) launch_components<double>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream);
-        else launch_components<float>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream);
+        ComponentEvents* evp = prof.enabled ? &cev : nullptr;
+        if (fp64) launch_components<double>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream, evp);
+        else launch_components<float>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream, evp);
         const long long nfin = (long long)T * R * nf;
         if (fp64) k_finalize<double><<<unsigned((nfin + 255) / 256), 256, 0, stream>>>(q, nf);
         else k_finalize<float><<<unsigned((nfin + 255) / 256), 256, 0, stream>>>(q, nf);
         note_launch();
+        if (evp) {
+            cudaEventRecord(cev.ev[4], stream);
+            cudaEventSynchronize(cev.ev[4]);
+            for (int i = 0; i < 4; ++i) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, cev.ev[i], cev.ev[i + 1]);
+                comp_ms[i] += ms;
+            }
+        }
     }
     if (prof.enabled) {
         cudaEventRecord(ev_main1, stream);
-        unsigned long long nr[2] = {0, 0};
-        cudaMemcpyAsync(nr, ray_counter, 16, cudaMemcpyDeviceToHost, stream);
+        unsigned long long nr[4] = {0, 0, 0, 0};
+        cudaMemcpyAsync(nr, ray_counter, 32, cudaMemcpyDeviceToHost, stream);
+        int cc[kMaxDepth] = {0, 0, 0, 0, 0};
+        int ec = 0;
+        cudaMemcpyAsync(cc, chain_counts, sizeof(cc), cudaMemcpyDeviceToHost, stream);
+        cudaMemcpyAsync(&ec, edge_count, 4, cudaMemcpyDeviceToHost, stream);
         cudaEventSynchronize(ev_main1);
         cudaStreamSynchronize(stream);
         float a = 0.f, b = 0.f;
@@ -652,7 +696,12 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         prof.prep_ms = a;
         prof.main_ms = b;
         prof.prep_rays = (long long)nr[0];
-        prof.rays = (long long)nr[1];
+        prof.rays = (long long)(nr[1] + nr[2] + nr[3]);
+        for (int i = 0; i < 3; ++i) prof.kernel_rays[i] = (long long)nr[1 + i];
+        for (int i = 0; i < 4; ++i) prof.kernel_ms[i] = comp_ms[i];
+        for (int i = 0; i < kMaxDepth; ++i) prof.chains[i] = cc[i];
+        prof.edges = ec;
+        for (int i = 0; i < 5; ++i) cudaEventDestroy(cev.ev[i]);
         prof.main_launches = (d->num_freq + kMaxNF - 1) / kMaxNF;
         cudaEventDestroy(ev_prep);
         cudaEventDestroy(ev_main0);

@@ -69,6 +69,7 @@ struct MainParams {
     const int* chain_groups;
     const double* chain_planes;
     const double* chain_images;
+    const float4* chain_pre;         // per chain: last plane (n, offset) and last image (xyz, group) in FP32
     const int* edge_count;           // (T)
     const int* edge_list;            // (T, E)
     // outputs
@@ -89,11 +90,15 @@ struct MainParams {
 // and the ray counter is read back after the solve.
 struct ProfileState {
     bool enabled = false;
-    double main_ms = 0.0;        // summed main-kernel time of the last solve
+    double main_ms = 0.0;        // summed time of the per-cell kernels of the last solve
     double prep_ms = 0.0;        // candidate preparation time of the last solve
-    long long rays = 0;          // rays traced by the main kernel in the last solve
+    long long rays = 0;          // rays traced by the per-cell kernels in the last solve
     long long prep_rays = 0;     // rays traced while preparing candidates (discovery, edge prefilter)
     long long main_launches = 0;
+    double kernel_ms[4] = {0, 0, 0, 0};       // los+transmission, reflection, diffraction, finalize
+    long long kernel_rays[3] = {0, 0, 0};     // los+transmission, reflection, diffraction
+    long long chains[5] = {0, 0, 0, 0, 0};    // reflection candidates per depth (first transmitter)
+    long long edges = 0;                      // diffraction edges kept by the prefilter (first transmitter)
 };
 ProfileState& profile_state();
 

@@ -123,6 +123,15 @@ WCB_HD T fresnel_complement_abs(T x) {
 template <typename T>
 WCB_HD Cx<T> transition(T x) {
     if (value_of(x) <= 0) return cx(T(0), T(0));
+    if (value_of(x) >= (sizeof(T) == 4 ? 30.0 : 400.0)) {
+        // large-argument expansion (Kouyoumjian & Pathak, Proc. IEEE 1974):
+        // F(x) ~ 1 + j/(2x) - 3/(4x^2) - j 15/(8x^3) + 105/(16x^4) + j 945/(32x^5)
+        const T r = T(1) / x;
+        const T r2 = r * r;
+        const T re = T(1) - T(0.75) * r2 + T(6.5625) * r2 * r2;
+        const T im = T(0.5) * r - T(1.875) * r2 * r + T(29.53125) * r2 * r2 * r;
+        return cx(re, im);
+    }
     const T u = s_sqrt(T(2) * x / T(kPi));
     const FresnelPair<T> p = fresnel_pos(u, false);
     if (p.has_h) {
@@ -277,7 +286,8 @@ WCB_HD DiffractionResult<T> utd_field(const EdgeDev& ed, V3<double> S, V3<double
         const T rw = delta / delta_w;
         T w = s_exp(-rw * rw);
         if (value_of(w) <= kWindowCutoff) w = T(0);
-        const Cx<T> mirrored = kp_term(T(2) * b_star - beta, nn, kl, sgn);
+        // the odd part vanishes outside the locality window: skip the mirror
+        const Cx<T> mirrored = value_of(w) > 0 ? kp_term(T(2) * b_star - beta, nn, kl, sgn) : value;
         const Cx<T> odd = (value - mirrored) * (T(0.5) * w);
         const T rb = delta / delta_b;
         const T wb = s_exp(-rb * rb);
