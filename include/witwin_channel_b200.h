@@ -169,6 +169,22 @@ int wcb_rows_select(const void* rows, int64_t num_rows, int32_t width, int64_t m
                     int64_t* selected, int64_t* num_selected, void* workspace, int64_t workspace_bytes, void* stream);
 int wcb_rows_select_workspace_size(int64_t num_rows, int64_t* bytes);
 
+/* wcb_rows_select without a caller workspace and without any allocation (no
+ * counterpart in the reference, whose selection allocates through torch).
+ * For callers that may not allocate device memory at call time: code inside
+ * an out-of-memory handler, real-time loops where a cudaMalloc would
+ * synchronise the device, hosts with pools frozen after start-up.  The
+ * scratch is a fixed WCB_ROWS_SELECT_NOALLOC_SCRATCH_BYTES array in the
+ * library's device image; inputs whose wcb_rows_select_workspace_size exceeds
+ * it (above 597,120 records) return WCB_ERR_CAPACITY before any work.  The first
+ * call on a device looks the array up and may load the library's module:
+ * make it before any stream capture.  All calls on a device share the array
+ * (each call rewrites what it reads), so calls that overlap in time race:
+ * serialise them. */
+#define WCB_ROWS_SELECT_NOALLOC_SCRATCH_BYTES (32ll << 20)
+int wcb_rows_select_noalloc(const void* rows, int64_t num_rows, int32_t width, int64_t max_paths, int32_t scope,
+                            int64_t* selected, int64_t* num_selected, void* stream);
+
 /* Field evaluation of selected path records at one frequency (index freq
  * into the materials tables).  Writes the path-table columns; any output
  * pointer may be NULL. */

@@ -125,6 +125,7 @@ EXPORTED_SYMBOLS = (
     "wcb_solve",
     "wcb_rows_select_workspace_size",
     "wcb_rows_select",
+    "wcb_rows_select_noalloc",
     "wcb_rows_evaluate",
     "wcb_rows_accumulate",
     "wcb_field_free_space",
@@ -169,6 +170,8 @@ def load() -> ctypes.CDLL:
     lib.wcb_rows_select_workspace_size.argtypes = [ctypes.c_int64, _i64p]
     lib.wcb_rows_select.argtypes = [_vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, _vp, _i64p, _vp,
                                     ctypes.c_int64, _vp]
+    lib.wcb_rows_select_noalloc.argtypes = [_vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int64, ctypes.c_int32, _vp,
+                                            _i64p, _vp]
     lib.wcb_rows_evaluate.argtypes = [_vp, ctypes.POINTER(SolveDesc), ctypes.POINTER(Materials), ctypes.c_int32, _vp, _vp,
                                       ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(RowFields), _vp]
     lib.wcb_rows_accumulate.argtypes = [_vp, _vp, ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32,
