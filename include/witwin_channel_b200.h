@@ -214,6 +214,53 @@ int wcb_rows_accumulate(const void* rows, const int64_t* selected, int64_t num_s
                         const float* tx_power, int32_t num_tx, int32_t num_rx, int32_t coherent,
                         const wcb_outputs* outputs, void* stream);
 
+/* Flat accumulation of evaluated paths (replaces the reference op
+ * deterministic_accumulate_flat: kernels/deterministic.py:23-102 over
+ * native/channel/kernels/deterministic.cu:829-970).  Per path: valid flag
+ * (1 byte), tx, rx, component id (0 los, 1 reflection, 2 diffraction,
+ * 3/4/7 coupled, 5 transmission, 6 scattering), gain and field (real, imag)
+ * in `dtype`.  Paths with an out-of-range tx/rx or an unknown component are
+ * dropped.  Outputs: power_total, field_total_real/imag (T,R) and
+ * component_power, component_field_real/imag (6,T,R), all in `dtype`, each
+ * element written once.  Every slot sums its paths in path index order, so
+ * results are bit-reproducible. */
+#define WCB_DTYPE_F32 0
+#define WCB_DTYPE_F64 1
+typedef struct {
+    void* power_total;
+    void* field_total_real;
+    void* field_total_imag;
+    void* component_power;
+    void* component_field_real;
+    void* component_field_imag;
+} wcb_accumulate_outputs;
+int wcb_accumulate_flat_workspace_size(int64_t num_paths, int64_t* bytes);
+int wcb_accumulate_flat(const uint8_t* valid, const int32_t* tx_id, const int32_t* rx_id, const int32_t* component_id,
+                        const void* path_gain, const void* field_real, const void* field_imag, int64_t num_paths,
+                        int32_t num_tx, int32_t num_rx, int32_t coherent, int32_t scattering_coherent, int32_t dtype,
+                        const wcb_accumulate_outputs* outputs, void* workspace, int64_t workspace_bytes,
+                        void* stream);
+/* Pushforward of wcb_accumulate_flat (replaces deterministic_accumulate_flat_jvp,
+ * kernels/deterministic.py:155-185): tangents of gain/field per path (any
+ * NULL = zero) give the tangents of all six outputs in `tangent_out`,
+ * linearised at the forward outputs in `saved`. */
+int wcb_accumulate_flat_jvp_workspace_size(int64_t num_paths, int32_t dtype, int64_t* bytes);
+int wcb_accumulate_flat_jvp(const uint8_t* valid, const int32_t* tx_id, const int32_t* rx_id,
+                            const int32_t* component_id, const void* tangent_path_gain, const void* tangent_field_real,
+                            const void* tangent_field_imag, int64_t num_paths, int32_t num_tx, int32_t num_rx,
+                            int32_t coherent, int32_t scattering_coherent, int32_t dtype,
+                            const wcb_accumulate_outputs* saved, const wcb_accumulate_outputs* tangent_out,
+                            void* workspace, int64_t workspace_bytes, void* stream);
+/* Adjoint of wcb_accumulate_flat (replaces deterministic_accumulate_flat_backward,
+ * kernels/deterministic.py:115-152): `saved` holds the forward outputs, `grads`
+ * their cotangents (any member NULL = zero).  Writes per-path gradients of
+ * gain and field (real, imag); dropped paths get zeros. */
+int wcb_accumulate_flat_backward(const uint8_t* valid, const int32_t* tx_id, const int32_t* rx_id,
+                                 const int32_t* component_id, int64_t num_paths, int32_t num_tx, int32_t num_rx,
+                                 int32_t coherent, int32_t scattering_coherent, int32_t dtype,
+                                 const wcb_accumulate_outputs* saved, const wcb_accumulate_outputs* grads,
+                                 void* grad_path_gain, void* grad_field_real, void* grad_field_imag, void* stream);
+
 /* Standalone field operators (reference kernels/fields.py facades).  All
  * arrays are device f32; complex outputs interleaved.  N rows. */
 int wcb_field_free_space(int64_t n, const float* source, const float* target, const float* tx_power,

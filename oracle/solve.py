@@ -167,9 +167,9 @@ def _exhaustive_chains(g: int, d: int) -> list[tuple[int, ...]]:
     return out
 
 
-def discover(arrays: dict, *, max_depth: int, discovery_rays: int = DISCOVERY_RAYS) -> list | None:
-    """Per-transmitter discovered group chains (``interactions/reflection.py:541-569``),
-    or ``None`` when the exhaustive plan applies at every depth."""
+def discovery_groups(arrays: dict, *, max_depth: int) -> np.ndarray | None:
+    """Face -> coplanar group map when the chain plan needs discovery at some
+    depth (``interactions/reflection.py:186-293``), else ``None``."""
     V, Fc = arrays["vertices"], arrays["faces"]
     if Fc.shape[0] == 0 or max_depth < 1:
         return None
@@ -177,21 +177,37 @@ def discover(arrays: dict, *, max_depth: int, discovery_rays: int = DISCOVERY_RA
     G = groups["group_count"]
     need = G > ORDER1_EXHAUSTIVE_GROUP_LIMIT or (max_depth >= 2 and not all(
         _face_sequence_count(G, d) <= MAX_MULTIBOUNCE_FACE_SEQUENCES for d in range(2, max_depth + 1)))
-    if not need:
+    return groups["face_group_id"] if need else None
+
+
+def discover_directions(arrays: dict, face_group_id: np.ndarray, tx: int, directions: np.ndarray, *,
+                        max_depth: int) -> np.ndarray:
+    """Group chains of the bounce paths launched from transmitter ``tx`` along
+    ``directions`` (``(N, max_depth)``, ``-1`` after a miss)."""
+    V, Fc = arrays["vertices"], arrays["faces"]
+    prims = geom.trace_reflections(geom.Triangles(V, Fc), geom.face_normals(V, Fc), arrays["tx_pos"][tx], directions,
+                                   max(max_depth, 1))
+    return np.where(prims >= 0, face_group_id[np.maximum(prims, 0)], -1)
+
+
+def discover(arrays: dict, *, max_depth: int, discovery_rays: int = DISCOVERY_RAYS) -> list | None:
+    """Per-transmitter discovered group chains (``interactions/reflection.py:541-569``),
+    or ``None`` when the exhaustive plan applies at every depth."""
+    face_group_id = discovery_groups(arrays, max_depth=max_depth)
+    if face_group_id is None:
         return None
-    tris = geom.Triangles(V, Fc)
-    normals = geom.face_normals(V, Fc)
     dirs = geom.fibonacci_directions(discovery_rays)
-    out = []
-    for t in range(arrays["tx_pos"].shape[0]):
-        prims = geom.trace_reflections(tris, normals, arrays["tx_pos"][t], dirs, max(max_depth, 1))
-        out.append(np.where(prims >= 0, groups["face_group_id"][np.maximum(prims, 0)], -1))
-    return out
+    return [discover_directions(arrays, face_group_id, t, dirs, max_depth=max_depth)
+            for t in range(arrays["tx_pos"].shape[0])]
 
 
 def solve(arrays: dict, *, components, max_depth: int, coherent: bool = True, max_paths=None,
           max_paths_scope: str = "global", frequency: float, discovery_rays: int = DISCOVERY_RAYS,
-          edge_policy=None, discovered: list | None = None) -> dict:
+          edge_policy=None, discovered: list | None = None, edge_visible: list | None = None) -> dict:
+    """Full deterministic solve.  ``discovered`` (per transmitter, from
+    ``discover``) and ``edge_visible`` (per transmitter, from
+    ``tx_edge_masks``) let a caller compute the per-transmitter work once and
+    reuse it across receiver subsets."""
     V, Fc = arrays["vertices"], arrays["faces"]
     fm = arrays["face_mats"]
     tx_pos, tx_pow, tx_pol = arrays["tx_pos"], arrays["tx_power"], arrays["tx_pol"]
@@ -294,14 +310,7 @@ def solve(arrays: dict, *, components, max_depth: int, coherent: bool = True, ma
     # ---- diffraction --------------------------------------------------------
     diff_vector = np.zeros((T, R, 3), dtype=np.complex128)
     if "diffraction" in components and max_depth >= 1 and has_struct and R > 0:
-        rec = geom.edge_records(Fc, arrays["face_structure"])
-        pol = edge_policy
-        eg = geom.edge_geometry(
-            V, Fc, normals, rec,
-            boundary_policy=getattr(pol, "boundary_edge_policy", "half_plane") or "half_plane",
-            vertical_only=getattr(pol, "edge_selection_mode", "all_edges") == "vertical_only",
-            vertical_ratio=getattr(pol, "vertical_ratio", 0.7),
-        )
+        eg = edge_table(arrays, edge_policy)
         wavelength = em.SPEED_OF_LIGHT / frequency
         for t in range(T):
             S = tx_pos[t]
@@ -309,7 +318,10 @@ def solve(arrays: dict, *, components, max_depth: int, coherent: bool = True, ma
                 inside, _ = utd.source_exterior(S, eg, e)
                 if not inside:
                     continue
-                if not tx_edge_visible(tris, S, eg, e, wavelength):
+                if edge_visible is not None:
+                    if not edge_visible[t][e]:
+                        continue
+                elif not tx_edge_visible(tris, S, eg, e, wavelength):
                     continue
                 for r in range(R):
                     out = utd.diffraction_field(S, rx_pos[r], tx_pol[t], eg, e, fm, frequency)
@@ -358,6 +370,37 @@ def solve(arrays: dict, *, components, max_depth: int, coherent: bool = True, ma
     acc["transmission_overflow"] = overflow
     acc["rows"] = table
     return acc
+
+
+def edge_table(arrays: dict, edge_policy=None) -> dict:
+    """Selected diffraction edges with their geometry (``diffraction.cu:803-900``,
+    ``scene/resources.py:356-405``)."""
+    V, Fc = arrays["vertices"], arrays["faces"]
+    rec = geom.edge_records(Fc, arrays["face_structure"])
+    pol = edge_policy
+    return geom.edge_geometry(
+        V, Fc, geom.face_normals(V, Fc), rec,
+        boundary_policy=getattr(pol, "boundary_edge_policy", "half_plane") or "half_plane",
+        vertical_only=getattr(pol, "edge_selection_mode", "all_edges") == "vertical_only",
+        vertical_ratio=getattr(pol, "vertical_ratio", 0.7),
+    )
+
+
+def tx_edge_masks(arrays: dict, frequency: float, edge_policy=None) -> list:
+    """Per transmitter, the Tx-visibility prefilter of every edge (False for
+    unselected edges)."""
+    V, Fc = arrays["vertices"], arrays["faces"]
+    tris = geom.Triangles(V, Fc)
+    eg = edge_table(arrays, edge_policy)
+    wavelength = em.SPEED_OF_LIGHT / frequency
+    out = []
+    for t in range(arrays["tx_pos"].shape[0]):
+        mask = np.zeros(len(eg["selected"]), dtype=bool)
+        for e in np.nonzero(eg["selected"])[0]:
+            if utd.source_exterior(arrays["tx_pos"][t], eg, e)[0]:
+                mask[e] = tx_edge_visible(tris, arrays["tx_pos"][t], eg, e, wavelength)
+        out.append(mask)
+    return out
 
 
 def tx_edge_visible(tris, S, eg, e, wavelength) -> bool:

@@ -30,6 +30,9 @@ COMPONENT_TRANSMISSION = 8
 PRECISION_MIXED = 0
 PRECISION_FP64 = 1
 
+DTYPE_F32 = 0
+DTYPE_F64 = 1
+
 _f32p = ctypes.POINTER(ctypes.c_float)
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _i64p = ctypes.POINTER(ctypes.c_int64)
@@ -111,6 +114,17 @@ class RowFields(ctypes.Structure):
     ]
 
 
+class AccumulateOutputs(ctypes.Structure):
+    _fields_ = [
+        ("power_total", _vp),
+        ("field_total_real", _vp),
+        ("field_total_imag", _vp),
+        ("component_power", _vp),
+        ("component_field_real", _vp),
+        ("component_field_imag", _vp),
+    ]
+
+
 ROW_BYTES = 48
 # wcb_row as int32 words: tx, rx, (component | depth << 16), seq[5], edge, length(f32 bits), reserved[2]
 ROW_WORDS = 12
@@ -128,6 +142,11 @@ EXPORTED_SYMBOLS = (
     "wcb_rows_select_noalloc",
     "wcb_rows_evaluate",
     "wcb_rows_accumulate",
+    "wcb_accumulate_flat_workspace_size",
+    "wcb_accumulate_flat",
+    "wcb_accumulate_flat_backward",
+    "wcb_accumulate_flat_jvp_workspace_size",
+    "wcb_accumulate_flat_jvp",
     "wcb_field_free_space",
     "wcb_field_reflection_sequence",
     "wcb_field_transmission_sequence",
@@ -176,6 +195,19 @@ def load() -> ctypes.CDLL:
                                       ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(RowFields), _vp]
     lib.wcb_rows_accumulate.argtypes = [_vp, _vp, ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32,
                                         ctypes.c_int32, ctypes.POINTER(Outputs), _vp]
+    lib.wcb_accumulate_flat_workspace_size.argtypes = [ctypes.c_int64, _i64p]
+    lib.wcb_accumulate_flat.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.POINTER(AccumulateOutputs), _vp, ctypes.c_int64, _vp]
+    lib.wcb_accumulate_flat_backward.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32,
+                                                 ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                 ctypes.POINTER(AccumulateOutputs), ctypes.POINTER(AccumulateOutputs),
+                                                 _vp, _vp, _vp, _vp]
+    lib.wcb_accumulate_flat_jvp_workspace_size.argtypes = [ctypes.c_int64, ctypes.c_int32, _i64p]
+    lib.wcb_accumulate_flat_jvp.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int32,
+                                            ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.POINTER(AccumulateOutputs), ctypes.POINTER(AccumulateOutputs), _vp,
+                                            ctypes.c_int64, _vp]
     lib.wcb_field_free_space.argtypes = [ctypes.c_int64] + [_vp] * 5 + [ctypes.c_double] + [_vp] * 7 + [_vp]
     lib.wcb_field_reflection_sequence.argtypes = [ctypes.c_int64, ctypes.c_int32] + [_vp] * 12 + [ctypes.c_double] + [_vp] * 7 + [_vp]
     lib.wcb_field_transmission_sequence.argtypes = [ctypes.c_int64, ctypes.c_int32] + [_vp] * 8 + [

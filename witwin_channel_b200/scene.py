@@ -229,6 +229,41 @@ class ReceiverGrid:
         return o[None, :] + self.x_axis.float()[None, :] * r[:, None] + self.y_axis.float()[None, :] * c[:, None]
 
 
+_EDGE_SELECTION_MODES = ("all_edges", "vertical_only")
+_BOUNDARY_EDGE_POLICIES = ("exclude", "half_plane")
+
+
+@dataclass
+class EdgePolicy:
+    """Diffraction edge selection read from ``scene.metadata["imported_edge_policy"]``
+    (same fields and checks as the reference's ``scene/resources.py:248-273``):
+    ``vertical_only`` keeps edges with |dz|/length above ``vertical_ratio``;
+    boundary edges (one adjacent face) are kept as half-planes or excluded."""
+
+    vertical_ratio: float = 0.7
+    edge_selection_mode: str = "all_edges"
+    edge_diffraction: bool | None = True
+    boundary_edge_policy: str | None = None
+
+    def __post_init__(self) -> None:
+        mode = str(self.edge_selection_mode)
+        if mode not in _EDGE_SELECTION_MODES:
+            raise ValueError(f"edge_selection_mode must be one of {sorted(_EDGE_SELECTION_MODES)}")
+        wanted = None if self.edge_diffraction is None else bool(self.edge_diffraction)
+        if self.boundary_edge_policy is None:
+            boundary = "exclude" if wanted is False else "half_plane"
+        else:
+            boundary = str(self.boundary_edge_policy)
+        if boundary not in _BOUNDARY_EDGE_POLICIES:
+            raise ValueError(f"boundary_edge_policy must be one of {sorted(_BOUNDARY_EDGE_POLICIES)}")
+        if wanted is not None and wanted != (boundary == "half_plane"):
+            raise ValueError(f"edge_diffraction={wanted!r} conflicts with boundary_edge_policy={boundary!r}")
+        self.vertical_ratio = float(self.vertical_ratio)
+        self.edge_selection_mode = mode
+        self.edge_diffraction = boundary == "half_plane"
+        self.boundary_edge_policy = boundary
+
+
 @dataclass
 class Scene:
     structures: list[Structure] = field(default_factory=list)
