@@ -31,9 +31,14 @@ def _load_mirror(root: Path):
     return mod
 
 
+def _f32(x):
+    """Inputs representable in float32, the CUDA operators' input type."""
+    return np.asarray(x, dtype=np.float32).astype(np.float64)
+
+
 def _unit(rng, n):
     v = rng.normal(size=(n, 3))
-    return v / np.linalg.norm(v, axis=1, keepdims=True)
+    return _f32(v / np.linalg.norm(v, axis=1, keepdims=True))
 
 
 def _t(x):
@@ -51,9 +56,9 @@ def main(root: Path) -> None:
 
     # free space: 64 cases, two carriers
     n = 64
-    src = rng.uniform(-50, 50, size=(n, 3))
-    tgt = src + _unit(rng, n) * rng.uniform(0.5, 400.0, size=(n, 1))
-    pw = rng.uniform(0.1, 4.0, size=n)
+    src = _f32(rng.uniform(-50, 50, size=(n, 3)))
+    tgt = _f32(src + _unit(rng, n) * rng.uniform(0.5, 400.0, size=(n, 1)))
+    pw = _f32(rng.uniform(0.1, 4.0, size=n))
     tpol, rpol = _unit(rng, n), _unit(rng, n)
     freq = np.where(np.arange(n) % 2 == 0, 3.5e9, 28.0e9)
     data.update(fs_source=src, fs_target=tgt, fs_power=pw, fs_tx_pol=tpol, fs_rx_pol=rpol, fs_freq=freq)
@@ -65,17 +70,17 @@ def main(root: Path) -> None:
     # specular chains of depth 1..3 at 28 GHz: random bounce points and normals
     for depth in (1, 2, 3):
         n = 32
-        src = rng.uniform(-30, 30, size=(n, 3))
-        pos = src[:, None, :] + np.cumsum(rng.uniform(-20, 20, size=(n, depth, 3)), axis=1)
-        tgt = pos[:, -1] + rng.uniform(-20, 20, size=(n, 3))
+        src = _f32(rng.uniform(-30, 30, size=(n, 3)))
+        pos = _f32(src[:, None, :] + np.cumsum(rng.uniform(-20, 20, size=(n, depth, 3)), axis=1))
+        tgt = _f32(pos[:, -1] + rng.uniform(-20, 20, size=(n, 3)))
         nrm = rng.normal(size=(n, depth, 3))
-        nrm /= np.linalg.norm(nrm, axis=2, keepdims=True)
-        eps = rng.uniform(1.5, 9.0, size=(n, depth))
-        sig = rng.uniform(0.0, 1.0, size=(n, depth))
+        nrm = _f32(nrm / np.linalg.norm(nrm, axis=2, keepdims=True))
+        eps = _f32(rng.uniform(1.5, 9.0, size=(n, depth)))
+        sig = _f32(rng.uniform(0.0, 1.0, size=(n, depth)))
         mu = np.ones((n, depth))
-        gain = rng.uniform(0.5, 1.0, size=(n, depth))
-        th = rng.uniform(0.05, 0.4, size=(n, depth))
-        pw = rng.uniform(0.1, 4.0, size=n)
+        gain = _f32(rng.uniform(0.5, 1.0, size=(n, depth)))
+        th = _f32(rng.uniform(0.05, 0.4, size=(n, depth)))
+        pw = _f32(rng.uniform(0.1, 4.0, size=n))
         tpol, rpol = _unit(rng, n), _unit(rng, n)
         f = 28.0e9
         out = _np(ref.reflection_sequence_reference(_t(src), _t(tgt), _t(pos), _t(nrm), _t(pw), _t(tpol), _t(rpol),
@@ -91,18 +96,18 @@ def main(root: Path) -> None:
     n, depth = 32, 3
     layer_offset = np.array([0, 1, 3])
     layer_count = np.array([1, 2, 1])
-    layer_th = np.array([0.2, 0.006, 0.006, 0.1])
-    layer_eps = np.array([5.24, 6.27, 6.27, 3.0])
-    layer_sig = np.array([0.626, 0.2287, 0.2287, 0.05])
+    layer_th = _f32([0.2, 0.006, 0.006, 0.1])
+    layer_eps = _f32([5.24, 6.27, 6.27, 3.0])
+    layer_sig = _f32([0.626, 0.2287, 0.2287, 0.05])
     layer_mu = np.ones(4)
-    src = rng.uniform(-30, 30, size=(n, 3))
-    tgt = src + _unit(rng, n) * rng.uniform(2.0, 200.0, size=(n, 1))
+    src = _f32(rng.uniform(-30, 30, size=(n, 3)))
+    tgt = _f32(src + _unit(rng, n) * rng.uniform(2.0, 200.0, size=(n, 1)))
     nrm = rng.normal(size=(n, depth, 3))
-    nrm /= np.linalg.norm(nrm, axis=2, keepdims=True)
+    nrm = _f32(nrm / np.linalg.norm(nrm, axis=2, keepdims=True))
     mids = rng.integers(0, 3, size=(n, depth))
     count = rng.integers(1, depth + 1, size=n)
     valid = np.arange(depth)[None, :] < count[:, None]
-    pw = rng.uniform(0.1, 4.0, size=n)
+    pw = _f32(rng.uniform(0.1, 4.0, size=n))
     tpol, rpol = _unit(rng, n), _unit(rng, n)
     f = 28.0e9
     out = _np(ref.transmission_sequence_reference(

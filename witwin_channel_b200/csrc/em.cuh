@@ -19,8 +19,10 @@ struct Slab {
 };
 
 // Thin-slab Fabry-Perot reflection r_te, r_tm (_reference_fields.py:85-115).
-template <typename T>
-WCB_HD void slab_fresnel(T cos_theta, const Slab<T>& m, double frequency, T wavelength, Cx<T>* r_te, Cx<T>* r_tm) {
+// F is the frequency's type: double in the solve, a dual number in the
+// derivative kernels.
+template <typename T, typename F = double>
+WCB_HD void slab_fresnel(T cos_theta, const Slab<T>& m, F frequency, T wavelength, Cx<T>* r_te, Cx<T>* r_tm) {
     const T omega = T(s_max(kTwoPi * frequency, kUtdSmallEps));
     T ct = s_abs(cos_theta);
     ct = s_min(s_max(ct, T(kUtdSmallEps)), T(1));
@@ -43,9 +45,9 @@ WCB_HD void slab_fresnel(T cos_theta, const Slab<T>& m, double frequency, T wave
 
 // One specular bounce of the transported field (the loop body of
 // _reference_fields.py:143-181).  Updates `value` and `outgoing`.
-template <typename T>
+template <typename T, typename F = double>
 WCB_HD void reflect_bounce(C3<T>& value, V3<T>& outgoing, V3<T> incident, V3<T> normal_in, const Slab<T>& m,
-                           double frequency, T wavelength) {
+                           F frequency, T wavelength) {
     const V3<T> ez = v3<T>(T(0), T(0), T(1));
     V3<T> normal = safe_normalize(normal_in, ez);
     if (value_of(dot(incident, normal)) > 0) normal = -normal;
@@ -94,9 +96,9 @@ WCB_HD PathEval<T> eval_free_space(V3<T> source, V3<T> target, V3<T> tx_pol, V3<
 
 // Rouard stack transmission for one wall (_reference_fields.py:196-273).
 // Layers ordered entry -> exit; returns t.
-template <typename T>
+template <typename T, typename F = double>
 WCB_HD Cx<T> stack_t(T cos_theta, const T* thickness, const T* eps_r, const T* sigma_e, const T* mu_r, int count,
-                     double frequency, int pol_tm) {
+                     F frequency, int pol_tm) {
     if (count <= 0) return cx(T(1), T(0));
     const T omega = T(s_max(kTwoPi * frequency, kUtdSmallEps));
     T ct = s_min(s_max(s_abs(cos_theta), T(kUtdSmallEps)), T(1));

@@ -16,6 +16,7 @@ struct SceneHandle {
     std::vector<void*> owned;
     int* edge_ids = nullptr;     // (E) device, reference edge id of each selected edge
     int* edge_slot = nullptr;    // (edges total) device, selected index of each reference edge or -1
+    int* edge_topo = nullptr;    // (E,4) device: va, vb (edge direction vb - va), fn0, fn1 (-1: half-plane)
     std::vector<int> group_rep_host;
     std::vector<int> face_group_host;
     int num_edges_total = 0;

@@ -343,6 +343,7 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
     std::vector<std::array<double, 3>> epos(NE), edir(NE), n0o(NE), n1o(NE), opp0(NE);
     std::vector<double> elen(NE), ext(NE);
     std::vector<int> face0(NE), face1(NE), mat0(NE), mat1(NE);
+    std::vector<int> fn0(NE), fn1(NE);  // faces whose unit normals are n0 and n1 (-1: n1 = -n0)
     auto fnormal = [&](int f) { return std::array<double, 3>{face_plane[4 * f], face_plane[4 * f + 1], face_plane[4 * f + 2]}; };
     auto opposite = [&](int f, int a, int b) {
         for (int k = 0; k < 3; ++k) {
@@ -396,6 +397,8 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
         face1[e] = r.f1;
         mat0[e] = swapped ? r.f1 : r.f0;
         mat1[e] = swapped ? r.f0 : r.f1;
+        fn0[e] = interior ? (first ? s0 : s1) : s0;
+        fn1[e] = interior ? (first ? s1 : s0) : -1;
     }
     // shared boundary merge: group boundary records by quantized endpoints
     {
@@ -428,6 +431,7 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
                 sel[a] = (merged > M_PI * (1.0 + 1e-6)) && !copl;
                 sel[b] = 0;
                 n1o[a] = n0o[b];
+                fn1[a] = fn0[b];
                 face1[a] = face0[b];
                 mat1[a] = mat0[b];
                 ext[a] = merged;
@@ -438,6 +442,7 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
     }
     std::vector<EdgeDev> edges;
     std::vector<int> edge_ids;
+    std::vector<int> edge_topo;  // per selected edge: va, vb (dir = vb - va), fn0, fn1
     for (int e = 0; e < NE; ++e) {
         if (!boundary_half_plane && boundary[e]) sel[e] = 0;
         if (vertical_only) {
@@ -451,10 +456,15 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
         auto dir = edir[e];
         auto t0 = norm3(cross3(n0o[e], dir));
         std::array<double, 3> to_opp = {opp0[e][0] - epos[e][0], opp0[e][1] - epos[e][1], opp0[e][2] - epos[e][2]};
-        if (dot3(to_opp, t0) < 0.0) {
+        const bool flipped = dot3(to_opp, t0) < 0.0;
+        if (flipped) {
             dir = {-dir[0], -dir[1], -dir[2]};
             t0 = {-t0[0], -t0[1], -t0[2]};
         }
+        edge_topo.push_back(flipped ? recs[e].v1 : recs[e].v0);
+        edge_topo.push_back(flipped ? recs[e].v0 : recs[e].v1);
+        edge_topo.push_back(fn0[e]);
+        edge_topo.push_back(fn1[e]);
         std::array<double, 3> bis = {n0o[e][0] + n1o[e][0], n0o[e][1] + n1o[e][1], n0o[e][2] + n1o[e][2]};
         double bl = std::sqrt(dot3(bis, bis));
         if (bl > 1e-6) bis = {bis[0] / bl, bis[1] / bl, bis[2] / bl};
@@ -497,6 +507,7 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
     sd.group_box = upload(h, group_box, stream);
     sd.edges = upload(h, edges, stream);
     h->edge_ids = upload(h, edge_ids, stream);
+    h->edge_topo = upload(h, edge_topo, stream);
     {
         std::vector<int> slot(std::max(NE, 1), -1);
         for (size_t i = 0; i < edge_ids.size(); ++i) slot[edge_ids[i]] = int(i);

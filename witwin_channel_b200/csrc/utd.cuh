@@ -197,41 +197,65 @@ struct DiffractionResult {
     double length;     // s' + s (FP64)
 };
 
-// Per-frequency face slab lookup callback is provided as two Slab values.
+// Edge frame in geometry type G (double in the solve, a dual number in the
+// derivative kernels).
+template <typename G>
+struct EdgeFrame {
+    V3<G> c, e, t0, n0, bisector;
+    G half_length, n;
+};
+
+WCB_HD EdgeFrame<double> edge_frame(const EdgeDev& ed) {
+    EdgeFrame<double> f;
+    f.c = v3(ed.pos[0], ed.pos[1], ed.pos[2]);
+    f.e = v3(ed.dir[0], ed.dir[1], ed.dir[2]);
+    f.t0 = v3(ed.t0[0], ed.t0[1], ed.t0[2]);
+    f.n0 = v3(ed.n0[0], ed.n0[1], ed.n0[2]);
+    f.bisector = v3(ed.bisector[0], ed.bisector[1], ed.bisector[2]);
+    f.half_length = ed.half_length;
+    f.n = ed.n;
+    return f;
+}
+
+// exp(-j k d) in the amplitude type T from geometry-typed k and d.
 template <typename T>
-WCB_HD DiffractionResult<T> utd_field(const EdgeDev& ed, V3<double> S, V3<double> R, V3<T> tx_pol, const Slab<T>& m0,
-                                      const Slab<T>& mn, double frequency) {
+WCB_HD Cx<T> phasor_kd(double k, double d) { return phasor_neg_kd<T>(k, d); }
+
+// UTD field of one edge: geometry (stationary point, lengths, phase) in G,
+// amplitudes in T.  The face slabs give R_0 and R_n.
+template <typename G, typename T>
+WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> R, V3<T> tx_pol, const Slab<T>& m0,
+                                         const Slab<T>& mn, G frequency, V3<G>* q_out = nullptr) {
     DiffractionResult<T> out;
     out.valid = false;
-    const double k = kTwoPi * frequency / kC0;
-    const V3<double> c = v3(ed.pos[0], ed.pos[1], ed.pos[2]);
-    const V3<double> e = v3(ed.dir[0], ed.dir[1], ed.dir[2]);
-    const V3<double> t0d = v3(ed.t0[0], ed.t0[1], ed.t0[2]);
-    const V3<double> n0d = v3(ed.n0[0], ed.n0[1], ed.n0[2]);
-    const double n = ed.n;
-    // Keller stationary point (unfolding); FP64
-    const V3<double> ds = S - c;
-    const double ts = dot(ds, e);
-    const V3<double> ps = ds - e * ts;
-    const double rs = length(ps);
-    const V3<double> dr = R - c;
-    const double tr = dot(dr, e);
-    const V3<double> pr = dr - e * tr;
-    const double rr = length(pr);
-    const double t_star = (rs + rr) > 0.0 ? ts + (tr - ts) * rs / (rs + rr) : ts;
-    const V3<double> q = c + e * t_star;
-    const double tc = fmin(fmax(t_star, -ed.half_length), ed.half_length);
-    const V3<double> qv = c + e * tc + v3(ed.bisector[0], ed.bisector[1], ed.bisector[2]) * kDiffractionRayBias;
-    out.q[0] = q.x; out.q[1] = q.y; out.q[2] = q.z;
-    out.q_vis[0] = qv.x; out.q_vis[1] = qv.y; out.q_vis[2] = qv.z;
-    const V3<double> sp_vec = q - S;
-    const V3<double> s_vec = R - q;
-    const double s_p = fmax(length(sp_vec), kUtdMinDistance);
-    const double s = fmax(length(s_vec), kUtdMinDistance);
-    out.length = s_p + s;
+    const G k = G(kTwoPi) * frequency / G(kC0);
+    const V3<G> c = ed.c;
+    const V3<G> e = ed.e;
+    const G n = ed.n;
+    // Keller stationary point (unfolding)
+    const V3<G> ds = S - c;
+    const G ts = dot(ds, e);
+    const V3<G> ps = ds - e * ts;
+    const G rs = length(ps);
+    const V3<G> dr = R - c;
+    const G tr = dot(dr, e);
+    const V3<G> pr = dr - e * tr;
+    const G rr = length(pr);
+    const G t_star = value_of(rs + rr) > 0.0 ? ts + (tr - ts) * rs / (rs + rr) : ts;
+    const V3<G> q = c + e * t_star;
+    if (q_out) *q_out = q;
+    const G tc = s_min(s_max(t_star, -ed.half_length), ed.half_length);
+    const V3<G> qv = c + e * tc + ed.bisector * G(kDiffractionRayBias);
+    out.q[0] = value_of(q.x); out.q[1] = value_of(q.y); out.q[2] = value_of(q.z);
+    out.q_vis[0] = value_of(qv.x); out.q_vis[1] = value_of(qv.y); out.q_vis[2] = value_of(qv.z);
+    const V3<G> sp_vec = q - S;
+    const V3<G> s_vec = R - q;
+    const G s_p = s_max(length(sp_vec), G(kUtdMinDistance));
+    const G s = s_max(length(s_vec), G(kUtdMinDistance));
+    out.length = value_of(s_p + s);
     // angles in the edge frame
-    const T phi_p = wedge_angle(cast3<T>(ps), cast3<T>(t0d), cast3<T>(n0d));
-    T phi = wedge_angle(cast3<T>(pr), cast3<T>(t0d), cast3<T>(n0d));
+    const T phi_p = wedge_angle(cast3<T>(ps), cast3<T>(ed.t0), cast3<T>(ed.n0));
+    T phi = wedge_angle(cast3<T>(pr), cast3<T>(ed.t0), cast3<T>(ed.n0));
     const T nn = T(n);
     const T npi = nn * T(kPi);
     if (value_of(phi_p) > value_of(npi)) return out;
@@ -239,8 +263,8 @@ WCB_HD DiffractionResult<T> utd_field(const EdgeDev& ed, V3<double> S, V3<double
         phi = (value_of(phi - npi) < value_of(T(kTwoPi) - phi)) ? npi : T(0);
     }
     out.valid = true;
-    const V3<T> sh_p = cast3<T>(sp_vec * (1.0 / s_p));
-    const V3<T> sh = cast3<T>(s_vec * (1.0 / s));
+    const V3<T> sh_p = cast3<T>(sp_vec * (G(1) / s_p));
+    const V3<T> sh = cast3<T>(s_vec * (G(1) / s));
     const V3<T> ef = cast3<T>(e);
     T cos_b = dot(sh_p, ef);
     cos_b = s_min(s_max(cos_b, T(-1)), T(1));
@@ -267,7 +291,7 @@ WCB_HD DiffractionResult<T> utd_field(const EdgeDev& ed, V3<double> S, V3<double
     const T delta_w = T(4) * unit;
     const T delta_b = T(kCBlend) * unit;
     // face factors
-    const T wavelength = T(kC0 / frequency);
+    const T wavelength = T(G(kC0) / frequency);
     Cx<T> r0_te, r0_tm, rn_te, rn_tm;
     slab_fresnel(s_sin(phi_p), m0, frequency, wavelength, &r0_te, &r0_tm);
     slab_fresnel(s_sin(npi - phi), mn, frequency, wavelength, &rn_te, &rn_tm);
@@ -316,11 +340,18 @@ WCB_HD DiffractionResult<T> utd_field(const EdgeDev& ed, V3<double> S, V3<double
     const T e_beta = dot(tx_axis, beta_hat_p) * inc_amp;
     const T e_phi = dot(tx_axis, phi_hat_p) * inc_amp;
     const T spread = s_sqrt(spT / (sT * (spT + sT)));
-    const Cx<T> ph = phasor_neg_kd<T>(k, s_p + s);
+    const Cx<T> ph = phasor_kd<T>(k, s_p + s);
     const Cx<T> cb = -(d_soft * (e_beta * spread)) * ph;
     const Cx<T> cf = -(d_hard * (e_phi * spread)) * ph;
     out.field = c3_axis(beta_hat, cb) + c3_axis(phi_hat, cf);
     return out;
+}
+
+// The solve's form: FP64 geometry from the precomputed edge record.
+template <typename T>
+WCB_HD DiffractionResult<T> utd_field(const EdgeDev& ed, V3<double> S, V3<double> R, V3<T> tx_pol, const Slab<T>& m0,
+                                      const Slab<T>& mn, double frequency) {
+    return utd_field_gt<double, T>(edge_frame(ed), S, R, tx_pol, m0, mn, frequency);
 }
 
 }  // namespace wcb
