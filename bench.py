@@ -249,6 +249,8 @@ def run_native(args) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t[0])
     e2e_value = rays_all / args.steps * e2e_steps / (e2e_ms / 1000.0)
+    fp64 = _fp64_plain(compiled, ep, mats, freq, bits, cfg, device, step_ms / args.steps)
+    vjp = None if args.no_vjp else _vjp_run(device)
     if rank == 0:
         peaks = _peaks()
         hbm = float(peaks.get("hbm_gbs", HBM_FALLBACK))
@@ -307,6 +309,8 @@ def run_native(args) -> None:
                 "launch_ms": launch_ms,
             },
             "cpu_baseline": cpu,
+            "fp64_plain": fp64,
+            "vjp": vjp,
             "gpu_launches": launches,
             "clocks": sampler.summary(),
             "wall_s": t_wall,
@@ -315,6 +319,76 @@ def run_native(args) -> None:
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _fp64_plain(compiled, ep, mats, freq, bits, cfg, device, mixed_ms: float, steps: int = 3) -> dict:
+    """The same solve with every stage in FP64 (the plain form the mixed path is compared with)."""
+    import torch
+
+    from witwin_channel_b200 import engine
+
+    cells = engine.alloc_cells(1, ep.num_tx, ep.num_rx, device, fp64=True)
+
+    def step():
+        engine.run_solve(compiled, ep, mats, [freq], components=bits, max_depth=cfg.max_depth, coherent=True,
+                         precision=1, cells=cells)
+
+    step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"ms_per_step": ms, "mixed_ms_per_step": mixed_ms, "mixed_speedup": ms / mixed_ms if mixed_ms else None,
+            "steps": steps}
+
+
+def _vjp_run(device, steps: int = 3) -> dict:
+    """The gradient workload: forward + VJP of the log10 path-gain MSE on the
+    urban canyon w.r.t. concrete (eps_r, sigma_e), frequency, Tx position and
+    the vertices of 8 seeded boxes (the target map comes from eps_r x1.10 and
+    the boxes displaced by N(0, 0.5 m))."""
+    import torch
+
+    from witwin_channel_b200 import Config, solve
+    from witwin_channel_b200.workloads import gradient_run, log_mse
+
+    g = gradient_run(seed=1)
+    cfg = Config(components=g["components"], max_depth=g["max_depth"], ad_mode="vjp")
+    leaves = [g["leaves"]["eps_r"], g["leaves"]["sigma_e"], g["leaves"]["tx"], g["frequency"]] + g["leaves"]["vertices"]
+
+    def step():
+        for t in leaves:
+            t.grad = None
+        res = solve(g["scene"], cfg, reference_frequency_hz=g["frequency"])
+        loss = log_mse(res.path_gain, g["target"])
+        loss.backward()
+        return loss, res
+
+    step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        loss, res = step()
+    e1.record()
+    torch.cuda.synchronize()
+    vg = torch.cat([v.grad.reshape(-1) for v in g["leaves"]["vertices"]])
+    return {
+        "workload": "urban canyon 64 boxes, 256x256 grid, 28 GHz, LoS + reflection depth 3 + UTD; loss = MSE of "
+                    "log10 path gain vs a target from eps_r x1.10 and 8 boxes displaced N(0, 0.5 m); gradients for "
+                    "concrete eps_r and sigma_e, frequency, Tx position and the 8 boxes' 64 vertices",
+        "ms_per_step": e0.elapsed_time(e1) / steps,
+        "steps": steps,
+        "paths": int(res.metadata["counts"]["path_count"]),
+        "loss": float(loss),
+        "grad": {"eps_r": float(g["leaves"]["eps_r"].grad), "sigma_e": float(g["leaves"]["sigma_e"].grad),
+                 "frequency": float(g["frequency"].grad), "tx": [float(x) for x in g["leaves"]["tx"].grad],
+                 "vertices_norm": float(vg.norm())},
+    }
 
 
 # --------------------------------------------------------------------------
@@ -535,6 +609,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-vjp", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "native":
         args.warmup = 3

@@ -270,7 +270,8 @@ int wcb_accumulate_flat_backward(const uint8_t* valid, const int32_t* tx_id, con
  * material eps_r (M), material sigma_e (M), layer eps_r (L), layer sigma_e
  * (L), frequency (1), Tx positions (T,3) and point-receiver positions (R,3);
  * layout[8] is the total.  `want` bits: 1 Tx, 2 Rx, 4 frequency, 8 vertices,
- * 16 materials (unrequested parts are written as zeros).  Records are
+ * 16 materials (unrequested parts are written as zeros); vertex_mask (V bytes,
+ * NULL = all) limits the vertex gradient to the vertices marked nonzero.  Records are
  * re-evaluated from raw scene values in FP64 dual numbers (no stored
  * intermediates); the per-parameter sums are deterministic.  row_field
  * (optional, (K,2) FP64) receives each record's re-evaluated path field. */
@@ -280,8 +281,8 @@ int wcb_rows_vjp_workspace_size(int64_t num_selected, int32_t max_depth, int32_t
 int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_materials* materials,
                  int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
                  const double* grad_path_gain, const double* grad_field_real, const double* grad_field_imag,
-                 int32_t want, double* grad_out, int64_t grad_size, double* row_field, void* workspace,
-                 int64_t workspace_bytes, void* stream);
+                 int32_t want, const uint8_t* vertex_mask, double* grad_out, int64_t grad_size, double* row_field,
+                 void* workspace, int64_t workspace_bytes, void* stream);
 
 /* Standalone field operators (reference kernels/fields.py facades).  All
  * arrays are device f32; complex outputs interleaved.  N rows. */

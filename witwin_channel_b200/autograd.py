@@ -48,6 +48,7 @@ class _State:
     saved64: dict       # FP64 accumulation outputs (linearisation point)
     outputs32: dict     # FP32 accumulation outputs (the returned values)
     layer_counts: list
+    vertex_mask: torch.Tensor | None = None
 
 
 def _as_f64(x, device) -> torch.Tensor:
@@ -74,13 +75,17 @@ def _differentiable_inputs(scene, compiled, freq_t: torch.Tensor, device) -> dic
     else:
         rx = torch.stack([r.position.reshape(3).to(device=device, dtype=torch.float64) for r in rxs]) if rxs else \
             torch.zeros((0, 3), dtype=torch.float64, device=device)
-    return {"vertices": V, "eps_r": eps, "sigma_e": sig, "layer_eps_r": leps, "layer_sigma_e": lsig,
+    # differentiate only the vertices of structures whose vertex tensor takes gradients
+    mask = torch.cat([torch.full((st.vertices.reshape(-1, 3).shape[0],), int(bool(st.vertices.requires_grad)),
+                                 dtype=torch.uint8) for st in scene.structures]).to(device) if verts else None
+    return {"vertices": V, "vertex_mask": mask, "eps_r": eps, "sigma_e": sig, "layer_eps_r": leps, "layer_sigma_e": lsig,
             "frequency": freq_t.reshape(()).to(dtype=torch.float64), "tx": tx, "rx": rx,
             "layer_counts": [len(rows) for rows in mv["layers"]]}
 
 
 def rows_vjp(state: _State, g_gain: torch.Tensor | None, g_re: torch.Tensor | None, g_im: torch.Tensor | None,
-             want: int, row_field: torch.Tensor | None = None) -> tuple[torch.Tensor, list[int]]:
+             want: int, row_field: torch.Tensor | None = None,
+             vertex_mask: torch.Tensor | None = None) -> tuple[torch.Tensor, list[int]]:
     """Dense FP64 gradient over the native parameter layout (see ``wcb_rows_vjp``)."""
     lib = _native.load()
     device = state.rows.device
@@ -100,7 +105,8 @@ def rows_vjp(state: _State, g_gain: torch.Tensor | None, g_re: torch.Tensor | No
     _native.check(
         lib.wcb_rows_vjp(state.compiled.native.handle, ctypes.byref(desc), ctypes.byref(ms), 0,
                          _native.ptr(state.rows) if K else None, _native.ptr(state.selected) if K else None, K,
-                         _native.ptr(g_gain), _native.ptr(g_re), _native.ptr(g_im), int(want), _native.ptr(grad),
+                         _native.ptr(g_gain), _native.ptr(g_re), _native.ptr(g_im), int(want),
+                         _native.ptr(vertex_mask), _native.ptr(grad),
                          grad.numel(), _native.ptr(row_field), _native.ptr(ws), ws.numel(),
                          _native.stream_handle(device)),
         "wcb_rows_vjp",
@@ -148,7 +154,7 @@ class _SolveFunction(torch.autograd.Function):
             grad_component_field_real=g64[4], grad_component_field_imag=g64[5], num_tx=T, num_rx=R,
             coherent=state.coherent)
         grad, lay = rows_vjp(state, per_row["grad_path_gain"], per_row["grad_field_real"],
-                             per_row["grad_field_imag"], want)
+                             per_row["grad_field_imag"], want, vertex_mask=state.vertex_mask)
         parts = [grad[lay[i]:lay[i + 1]] for i in range(8)]
         out = [None]
         for i, shape in enumerate(ctx.shapes):
@@ -203,7 +209,8 @@ def solve_vjp(scene: Any, config, reference_frequency_hz):
     inputs = _differentiable_inputs(scene, compiled, freq_t, device)
     state = _State(compiled=compiled, ep=ep, mats=mats, frequency=frequency, components=bits,
                    max_depth=config.max_depth, coherent=config.coherent, rows=rows, selected=selected, flat=flat,
-                   saved64=saved64, outputs32=outputs32, layer_counts=inputs["layer_counts"])
+                   saved64=saved64, outputs32=outputs32, layer_counts=inputs["layer_counts"],
+                   vertex_mask=inputs["vertex_mask"])
     pt, ftr, fti, cp, cfr, cfi = _SolveFunction.apply(
         state, inputs["vertices"], inputs["eps_r"], inputs["sigma_e"], inputs["layer_eps_r"], inputs["layer_sigma_e"],
         inputs["frequency"], inputs["tx"], inputs["rx"])

@@ -136,8 +136,8 @@ int wcb_rows_vjp_workspace_size(int64_t num_selected, int32_t max_depth, int32_t
 int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_materials* materials,
                  int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
                  const double* grad_path_gain, const double* grad_field_real, const double* grad_field_imag,
-                 int32_t want, double* grad_out, int64_t grad_size, double* row_field, void* workspace,
-                 int64_t workspace_bytes, void* stream) {
+                 int32_t want, const uint8_t* vertex_mask, double* grad_out, int64_t grad_size, double* row_field,
+                 void* workspace, int64_t workspace_bytes, void* stream) {
     if (scene == nullptr || desc == nullptr || materials == nullptr || grad_out == nullptr || num_selected < 0)
         return WCB_ERR_INVALID_ARGUMENT;
     if (num_selected > 0 && (rows == nullptr || selected == nullptr)) return WCB_ERR_INVALID_ARGUMENT;
@@ -201,6 +201,7 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
     p.g_re = grad_field_real;
     p.g_im = grad_field_imag;
     p.want = want;
+    p.vertex_mask = vertex_mask;
     p.base_meps = int(layout[1]);
     p.base_msig = int(layout[2]);
     p.base_leps = int(layout[3]);

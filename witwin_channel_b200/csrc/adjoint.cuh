@@ -95,6 +95,7 @@ struct AdjParams {
     const double* g_gain;
     const double* g_re;
     const double* g_im;
+    const unsigned char* vertex_mask;  // per vertex: nonzero = differentiate (NULL: all)
     int want;
     // parameter id layout
     int base_meps, base_msig, base_leps, base_lsig, gid_freq, base_tx, base_rx;
@@ -118,12 +119,17 @@ struct ParamList {
     }
 };
 
+WCB_D bool vertex_wanted(const AdjParams& p, int v) {
+    return (p.want & kWantVertices) && (p.vertex_mask == nullptr || p.vertex_mask[v] != 0);
+}
+
+WCB_D void add_vertex(const AdjParams& p, ParamList& pl, int v) {
+    if (!vertex_wanted(p, v)) return;
+    for (int c = 0; c < 3; ++c) pl.add(gid_vertex(v, c));
+}
+
 WCB_D void add_face_vertices(const AdjParams& p, ParamList& pl, int f) {
-    if (!(p.want & kWantVertices)) return;
-    for (int k = 0; k < 3; ++k) {
-        const int v = p.sc.faces[3 * f + k];
-        for (int c = 0; c < 3; ++c) pl.add(gid_vertex(v, c));
-    }
+    for (int k = 0; k < 3; ++k) add_vertex(p, pl, p.sc.faces[3 * f + k]);
 }
 
 WCB_D void add_material(const AdjParams& p, ParamList& pl, int m) {
@@ -162,10 +168,8 @@ WCB_D void build_params(const AdjParams& p, const RowRec& row, ParamList& pl) {
     } else if (row.component == 2) {
         const int slot = p.edge_slot[row.edge];
         const int* tp = p.edge_topo + 4 * slot;
-        if (p.want & kWantVertices) {
-            for (int c = 0; c < 3; ++c) pl.add(gid_vertex(tp[0], c));
-            for (int c = 0; c < 3; ++c) pl.add(gid_vertex(tp[1], c));
-        }
+        add_vertex(p, pl, tp[0]);
+        add_vertex(p, pl, tp[1]);
         add_face_vertices(p, pl, tp[2]);
         if (tp[3] >= 0) add_face_vertices(p, pl, tp[3]);
         const EdgeDev& ed = p.sc.edges[slot];

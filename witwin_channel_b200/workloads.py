@@ -208,3 +208,62 @@ def large_city_scene(seed: int = 4, grid_side: int = 1024) -> tuple[Scene, float
     grid = make_receiver_grid(origin=origin, x_axis=(1.0, 0.0, 0.0), y_axis=(0.0, 1.0, 0.0),
                               shape=(grid_side, grid_side), spacing=(1.0, 1.0))
     return Scene(structures=structures, endpoints=[make_transmitter(tx), grid]), 28.0e9
+
+
+def gradient_run(seed: int = 1, grid_side: int = 256, moved_boxes: int = 8, displacement_m: float = 0.5,
+                 eps_scale: float = 1.10) -> dict:
+    """The gradient workload on the urban canyon: a differentiable scene
+    (concrete eps_r and sigma_e as leaf tensors, the vertices of `moved_boxes`
+    seeded boxes and the Tx position as leaves, the carrier frequency as a
+    leaf) and a target radiomap solved on a perturbed copy (eps_r x1.10 and
+    the same boxes' vertices displaced by N(0, 0.5 m)).  The loss is the MSE
+    between log10 path-gain maps over the cells where both are positive."""
+    from .deterministic import Config, solve
+
+    freq = 28.0e9
+    layout = city_layout(64, seed)
+    rng = np.random.default_rng(seed + 1000)
+    tx = street_point(layout, rng, 25.0)
+    sigma = 0.0462 * (freq / 1.0e9) ** 0.7822
+    eps = torch.tensor(5.24, dtype=torch.float64, requires_grad=True)
+    sig = torch.tensor(sigma, dtype=torch.float64, requires_grad=True)
+    mat = PhysicalMaterial(eps_r=eps, sigma_e=sig, thickness_m=0.3, name="concrete")
+    structures = city_scene(layout, material=mat)
+    pick = np.random.default_rng(seed + 3000).choice(len(layout.boxes), size=moved_boxes, replace=False)
+    moved = []
+    for b in sorted(int(x) for x in pick):
+        st = structures[b + 1]
+        leaf = st.vertices.detach().clone().requires_grad_(True)
+        st.geometry.vertices = leaf
+        moved.append(b + 1)
+    txa = make_transmitter(tx)
+    txa.position = torch.tensor(tx, dtype=torch.float32, requires_grad=True)
+    spacing = 1.5
+    origin = (-(grid_side - 1) / 2.0 * spacing, -(grid_side - 1) / 2.0 * spacing, 1.5)
+    grid = make_receiver_grid(origin=origin, x_axis=(1.0, 0.0, 0.0), y_axis=(0.0, 1.0, 0.0),
+                              shape=(grid_side, grid_side), spacing=(spacing, spacing))
+    scene = Scene(structures=structures, endpoints=[txa, grid])
+    # the target: a perturbed copy solved without gradients
+    tmat = PhysicalMaterial(eps_r=5.24 * eps_scale, sigma_e=sigma, thickness_m=0.3, name="concrete")
+    tstructs = city_scene(layout, material=tmat)
+    drng = np.random.default_rng(seed + 4000)
+    for idx in moved:
+        v = tstructs[idx].vertices.detach().clone()
+        tstructs[idx].geometry.vertices = v + torch.tensor(drng.normal(0.0, displacement_m, tuple(v.shape)),
+                                                           dtype=torch.float32)
+    tscene = Scene(structures=tstructs, endpoints=[make_transmitter(tx), grid])
+    components = {"los", "reflection", "diffraction"}
+    with torch.no_grad():
+        target = solve(tscene, Config(components=components, max_depth=3), reference_frequency_hz=freq).path_gain
+    freq_t = torch.tensor(freq, dtype=torch.float64, requires_grad=True)
+    return {"scene": scene, "frequency": freq_t, "target": target, "components": components, "max_depth": 3,
+            "leaves": {"eps_r": eps, "sigma_e": sig, "tx": txa.position,
+                       "vertices": [structures[i].vertices for i in moved]},
+            "moved_structures": moved}
+
+
+def log_mse(path_gain, target):
+    """MSE of log10 path gain over cells where both maps are positive."""
+    mask = (path_gain > 0) & (target > 0)
+    d = torch.log10(path_gain[mask].double()) - torch.log10(target[mask].double())
+    return (d * d).mean()
