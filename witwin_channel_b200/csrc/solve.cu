@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "em.cuh"
@@ -188,9 +189,13 @@ __global__ void k_chain_images(SceneDev sc, const float* tx, int depth, const in
 template <typename G>
 __global__ void __launch_bounds__(kBlock) k_edge_flags(SceneDev sc, const float* tx_pos, int t, double wavelength,
                                                        int* flags, int* err, unsigned long long* ray_counter) {
+    // one warp per edge, one lane per sample point (at most 16): the edge is
+    // Tx-visible when any sample is
     extern __shared__ int stack[];
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= sc.num_edges) return;
+    const long long gtid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int j = int(gtid >> 5);
+    const int lane = threadIdx.x & 31;
+    if (j >= sc.num_edges) return;  // whole warps exit together
     const EdgeDev ed = sc.edges[j];
     const V3<double> S = v3<double>(tx_pos[3 * t], tx_pos[3 * t + 1], tx_pos[3 * t + 2]);
     const V3<double> c = v3(ed.pos[0], ed.pos[1], ed.pos[2]);
@@ -198,25 +203,25 @@ __global__ void __launch_bounds__(kBlock) k_edge_flags(SceneDev sc, const float*
     V3<double> ds = S - c;
     ds = ds - e * dot(ds, e);
     const double phi_p = double(wedge_angle(ds, v3(ed.t0[0], ed.t0[1], ed.t0[2]), v3(ed.n0[0], ed.n0[1], ed.n0[2])));
-    int ok = 0;
-    if (phi_p <= ed.n * kPi) {
-        const double L = 2.0 * ed.half_length;
-        int n = int(ceil(L / wavelength));
-        n = n < 4 ? 4 : (n > 16 ? 16 : n);
+    const bool exterior = phi_p <= ed.n * kPi;
+    const double L = 2.0 * ed.half_length;
+    int n = int(ceil(L / wavelength));
+    n = n < 4 ? 4 : (n > 16 ? 16 : n);
+    bool visible = false;
+    if (exterior && lane < n) {
         Ignore ig = ignore_none();
         ig.f0 = ed.face0;
         ig.f1 = ed.face1;
         const V3<double> bis = v3(ed.bisector[0], ed.bisector[1], ed.bisector[2]);
-        unsigned long long traced = 0;
-        for (int i = 0; i < n && !ok; ++i) {
-            const double tt = -0.5 * L + (i + 0.5) / n * L;
-            const V3<double> p = c + e * tt + bis * kDiffractionRayBias;
-            ++traced;
-            if (!segment_blocked<G>(sc, cast3<G>(S), cast3<G>(p), ig, stack, err)) ok = 1;
-        }
-        if (ray_counter) atomicAdd(ray_counter, traced);
+        const double tt = -0.5 * L + (lane + 0.5) / n * L;
+        const V3<double> p = c + e * tt + bis * kDiffractionRayBias;
+        visible = !segment_blocked<G>(sc, cast3<G>(S), cast3<G>(p), ig, stack, err);
     }
-    flags[j] = ok;
+    const unsigned any = __ballot_sync(0xffffffffu, visible);
+    if (lane == 0) {
+        flags[j] = any != 0u;
+        if (ray_counter && exterior) atomicAdd(ray_counter, (unsigned long long)n);
+    }
 }
 
 // ordered compaction of edge flags (one block per call)
@@ -246,26 +251,26 @@ __global__ void k_to_double(long long n, const float* in, double* out) {
 }
 
 
+// Start/end events of the four per-cell kernels (LoS+transmission,
+// reflection, diffraction, finalize), each recorded on the kernel's stream.
 struct ComponentEvents {
-    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t start[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t end[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
+// LoS+transmission and diffraction go on `stream`, reflection on `side` (its
+// candidate tables were built there); the caller joins the streams before
+// the finalize kernel.
 template <typename T, int NF>
 void launch_nf(const MainParams& q0, unsigned blocks, int sdepth, size_t stack_bytes, cudaStream_t stream,
-               ComponentEvents* evs) {
+               cudaStream_t side, ComponentEvents* evs) {
     const unsigned tiles = unsigned(tiles_per_tx(q0) * q0.num_tx);
     const size_t split_stack = size_t(sdepth) * kSplitBlock * 4;
     const int c = q0.components;
     MainParams q = q0;
     unsigned long long* rc = q0.ray_counter;
-    if (evs) cudaEventRecord(evs->ev[0], stream);
-    if (c & (1 | 8)) {
-        q.ray_counter = rc ? rc + 0 : nullptr;
-        k_los_trans<T, NF><<<blocks, kCompBlock, stack_bytes, stream>>>(q);
-        note_launch();
-    }
-    if (evs) cudaEventRecord(evs->ev[1], stream);
     if (c & 2) {
+        if (evs) cudaEventRecord(evs->start[1], side);
         q.ray_counter = rc ? rc + 1 : nullptr;
         const size_t bytes = split_stack + kSplitWarps * sizeof(ReflShared<NF>) + size_t(kSplitWarps) * 32 * NF * 3 * 4;
         static bool attr = false;
@@ -273,10 +278,18 @@ void launch_nf(const MainParams& q0, unsigned blocks, int sdepth, size_t stack_b
             cudaFuncSetAttribute(k_reflect<T, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             attr = true;
         }
-        k_reflect<T, NF><<<tiles, kSplitBlock, bytes, stream>>>(q, sdepth);
+        k_reflect<T, NF><<<tiles, kSplitBlock, bytes, side>>>(q, sdepth);
+        note_launch();
+        if (evs) cudaEventRecord(evs->end[1], side);
+    }
+    if (evs) cudaEventRecord(evs->start[0], stream);
+    if (c & (1 | 8)) {
+        q.ray_counter = rc ? rc + 0 : nullptr;
+        k_los_trans<T, NF><<<blocks, kCompBlock, stack_bytes, stream>>>(q);
         note_launch();
     }
-    if (evs) cudaEventRecord(evs->ev[2], stream);
+    if (evs) cudaEventRecord(evs->end[0], stream);
+    if (evs) cudaEventRecord(evs->start[2], stream);
     if (c & 4) {
         q.ray_counter = rc ? rc + 2 : nullptr;
         const size_t bytes = split_stack + kSplitWarps * sizeof(DiffShared<NF>) + size_t(kSplitWarps) * 32 * NF * 9 * 4;
@@ -288,18 +301,29 @@ void launch_nf(const MainParams& q0, unsigned blocks, int sdepth, size_t stack_b
         k_diffract<T, NF><<<tiles, kSplitBlock, bytes, stream>>>(q, sdepth);
         note_launch();
     }
-    if (evs) cudaEventRecord(evs->ev[3], stream);
+    if (evs) cudaEventRecord(evs->end[2], stream);
 }
 
 template <typename T>
 void launch_components(const MainParams& q, int nf, unsigned blocks, int sdepth, size_t stack_bytes, cudaStream_t stream,
-                       ComponentEvents* evs) {
+                       cudaStream_t side, ComponentEvents* evs) {
     switch (nf) {
-        case 1: launch_nf<T, 1>(q, blocks, sdepth, stack_bytes, stream, evs); break;
-        case 2: launch_nf<T, 2>(q, blocks, sdepth, stack_bytes, stream, evs); break;
-        case 3: launch_nf<T, 3>(q, blocks, sdepth, stack_bytes, stream, evs); break;
-        default: launch_nf<T, 4>(q, blocks, sdepth, stack_bytes, stream, evs); break;
+        case 1: launch_nf<T, 1>(q, blocks, sdepth, stack_bytes, stream, side, evs); break;
+        case 2: launch_nf<T, 2>(q, blocks, sdepth, stack_bytes, stream, side, evs); break;
+        case 3: launch_nf<T, 3>(q, blocks, sdepth, stack_bytes, stream, side, evs); break;
+        default: launch_nf<T, 4>(q, blocks, sdepth, stack_bytes, stream, side, evs); break;
     }
+}
+
+// One non-blocking side stream per device, created on first use.
+cudaStream_t side_stream() {
+    static std::mutex mu;
+    static cudaStream_t streams[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (streams[dev] == nullptr) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+    return streams[dev];
 }
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
@@ -470,12 +494,25 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     const int B = 256;
     const size_t smem = size_t(kStackDepth) * kBlock * 4;
     int* err = out->status;
+    // The reflection candidates (discovery, chain tables) and the reflection
+    // kernel run on a side stream, overlapping the edge prefilter, the LoS and
+    // the diffraction kernels on the caller's stream; the streams join before
+    // the finalize kernel.
+    cudaStream_t side = side_stream();
+    if (side == nullptr) side = stream;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    if (side != stream) {
+        cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&join, cudaEventDisableTiming);
+        cudaEventRecord(fork, stream);
+        cudaStreamWaitEvent(side, fork, 0);
+    }
     // ---------------- reflection candidates
     if ((d->components & 2) && sc.num_faces > 0 && d->max_depth >= 1) {
         const bool need_disc = !(pl.exhaustive_o1 && (d->max_depth < 2 || pl.exhaustive_mb));
         float* dirs = reinterpret_cast<float*>(base + L.disc_dirs);
         if (need_disc) {
-            k_fibonacci<<<(rays + B - 1) / B, B, 0, stream>>>(rays, dirs);
+            k_fibonacci<<<(rays + B - 1) / B, B, 0, side>>>(rays, dirs);
             note_launch();
         }
         // exhaustive tables are identical for every tx: generate per tx
@@ -485,9 +522,9 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                 int* dg = reinterpret_cast<int*>(base + L.disc_groups);
                 const int md = d->max_depth;
                 if (fp64)
-                    k_discovery_trace<double><<<(rays + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, rays, md, dirs, txp, dg, err, prof.enabled ? ray_counter : nullptr);
+                    k_discovery_trace<double><<<(rays + kBlock - 1) / kBlock, kBlock, smem, side>>>(sc, rays, md, dirs, txp, dg, err, prof.enabled ? ray_counter : nullptr);
                 else
-                    k_discovery_trace<float><<<(rays + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, rays, md, dirs, txp, dg, err, prof.enabled ? ray_counter : nullptr);
+                    k_discovery_trace<float><<<(rays + kBlock - 1) / kBlock, kBlock, smem, side>>>(sc, rays, md, dirs, txp, dg, err, prof.enabled ? ray_counter : nullptr);
                 note_launch();
                 unsigned long long* keys = reinterpret_cast<unsigned long long*>(base + L.disc_keys);
                 unsigned long long* keys2 = reinterpret_cast<unsigned long long*>(base + L.disc_keys2);
@@ -501,15 +538,15 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                     const int depth = k + 1;
                     const bool use_disc = depth == 1 ? !pl.exhaustive_o1 : !pl.exhaustive_mb;
                     // ranks are needed for the next depth even when this depth is exhaustive
-                    k_chain_keys<<<(rays + B - 1) / B, B, 0, stream>>>(rays, md, k, dg, rank, keys, vals);
+                    k_chain_keys<<<(rays + B - 1) / B, B, 0, side>>>(rays, md, k, dg, rank, keys, vals);
                     size_t tb = L.disc_temp_bytes;
-                    cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys2, vals, vals2, rays, 0, 64, stream);
-                    k_chain_flags<<<(rays + B - 1) / B, B, 0, stream>>>(rays, keys2, flags);
+                    cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys2, vals, vals2, rays, 0, 64, side);
+                    k_chain_flags<<<(rays + B - 1) / B, B, 0, side>>>(rays, keys2, flags);
                     tb = L.disc_temp_bytes;
-                    cub::DeviceScan::InclusiveSum(temp, tb, flags, scan, rays, stream);
+                    cub::DeviceScan::InclusiveSum(temp, tb, flags, scan, rays, side);
                     int* cgrp = use_disc ? chain_groups + offs[t * kMaxDepth + k] : nullptr;
                     int* ccount = use_disc ? chain_counts + t * kMaxDepth + k : nullptr;
-                    k_chain_emit<<<(rays + B - 1) / B, B, 0, stream>>>(rays, md, k, keys2, vals2, flags, scan, dg, rank,
+                    k_chain_emit<<<(rays + B - 1) / B, B, 0, side>>>(rays, md, k, keys2, vals2, flags, scan, dg, rank,
                                                                        cgrp, use_disc ? int(pl.cap[k]) : 0, ccount);
                     note_launch(3);
                 }
@@ -525,15 +562,15 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                     const long long total = pl.cap[k];
                     fixed_counts[t * kMaxDepth + k] = int(total);
                     if (total > 0) {
-                        k_exhaustive_chains<<<int((total + B - 1) / B), B, 0, stream>>>(total, depth, sc.num_groups, cgrp);
-                        k_chain_images<<<int((total + B - 1) / B), B, 0, stream>>>(sc, txp, depth, nullptr, total, cgrp, cpl, cim, cpre);
+                        k_exhaustive_chains<<<int((total + B - 1) / B), B, 0, side>>>(total, depth, sc.num_groups, cgrp);
+                        k_chain_images<<<int((total + B - 1) / B), B, 0, side>>>(sc, txp, depth, nullptr, total, cgrp, cpl, cim, cpre);
                         note_launch(2);
                     }
                     cudaMemcpyAsync(chain_counts + t * kMaxDepth + k, &fixed_counts[t * kMaxDepth + k], 4,
-                                    cudaMemcpyHostToDevice, stream);
+                                    cudaMemcpyHostToDevice, side);
                 } else {
                     const long long cap = pl.cap[k];
-                    k_chain_images<<<int((cap + B - 1) / B), B, 0, stream>>>(sc, txp, depth, chain_counts + t * kMaxDepth + k,
+                    k_chain_images<<<int((cap + B - 1) / B), B, 0, side>>>(sc, txp, depth, chain_counts + t * kMaxDepth + k,
                                                                            0, cgrp, cpl, cim, cpre);
                     note_launch();
                 }
@@ -544,10 +581,12 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     if ((d->components & 4) && sc.num_edges > 0 && d->max_depth >= 1) {
         const double wavelength = kC0 / d->frequency_hz[0];
         for (int t = 0; t < T; ++t) {
+            const long long threads = (long long)sc.num_edges * 32;
+            const unsigned eblocks = unsigned((threads + kBlock - 1) / kBlock);
             if (fp64)
-                k_edge_flags<double><<<(sc.num_edges + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, d->tx_pos, t, wavelength, edge_flags, err, prof.enabled ? ray_counter : nullptr);
+                k_edge_flags<double><<<eblocks, kBlock, smem, stream>>>(sc, d->tx_pos, t, wavelength, edge_flags, err, prof.enabled ? ray_counter : nullptr);
             else
-                k_edge_flags<float><<<(sc.num_edges + kBlock - 1) / kBlock, kBlock, smem, stream>>>(sc, d->tx_pos, t, wavelength, edge_flags, err, prof.enabled ? ray_counter : nullptr);
+                k_edge_flags<float><<<eblocks, kBlock, smem, stream>>>(sc, d->tx_pos, t, wavelength, edge_flags, err, prof.enabled ? ray_counter : nullptr);
             k_compact_flags<<<1, 256, 0, stream>>>(sc.num_edges, edge_flags, edge_list + size_t(t) * sc.num_edges, edge_count + t);
             note_launch(2);
         }
@@ -615,7 +654,15 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     double* layers64 = nullptr;
     if (fp64 && m->num_layers > 0) {
         const long long n = (long long)m->num_layers * d->num_freq;
-        if (cudaMallocAsync(&layers64, size_t(n) * 4 * 8, stream) != cudaSuccess) return 2;
+        if (cudaMallocAsync(&layers64, size_t(n) * 4 * 8, stream) != cudaSuccess) {
+            if (side != stream) {
+                cudaEventRecord(join, side);
+                cudaStreamWaitEvent(stream, join, 0);
+                cudaEventDestroy(fork);
+                cudaEventDestroy(join);
+            }
+            return 2;
+        }
         const float* src[4] = {m->layer_thickness, m->layer_eps_r, m->layer_sigma_e, m->layer_mu_r};
         for (int q = 0; q < 4; ++q) {
             k_to_double<<<int((n + B - 1) / B), B, 0, stream>>>(n, src[q], layers64 + q * n);
@@ -634,7 +681,10 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     ComponentEvents cev;
     double comp_ms[4] = {0, 0, 0, 0};
     if (prof.enabled)
-        for (int i = 0; i < 5; ++i) cudaEventCreate(&cev.ev[i]);
+        for (int i = 0; i < 4; ++i) {
+            cudaEventCreate(&cev.start[i]);
+            cudaEventCreate(&cev.end[i]);
+        }
     for (int fb = 0; fb < d->num_freq; fb += kMaxNF) {
         const int nf = std::min(kMaxNF, d->num_freq - fb);
         p.freq_base = fb;
@@ -664,18 +714,24 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         if (fb > 0) q.rows = nullptr;  // geometry rows are emitted once
         if (blocks <= 0) continue;
         ComponentEvents* evp = prof.enabled ? &cev : nullptr;
-        if (fp64) launch_components<double>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream, evp);
-        else launch_components<float>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream, evp);
+        if (fp64) launch_components<double>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream, side, evp);
+        else launch_components<float>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream, side, evp);
+        if (side != stream) {
+            cudaEventRecord(join, side);
+            cudaStreamWaitEvent(stream, join, 0);
+        }
         const long long nfin = (long long)T * R * nf;
+        if (evp) cudaEventRecord(cev.start[3], stream);
         if (fp64) k_finalize<double><<<unsigned((nfin + 255) / 256), 256, 0, stream>>>(q, nf);
         else k_finalize<float><<<unsigned((nfin + 255) / 256), 256, 0, stream>>>(q, nf);
         note_launch();
         if (evp) {
-            cudaEventRecord(cev.ev[4], stream);
-            cudaEventSynchronize(cev.ev[4]);
+            cudaEventRecord(cev.end[3], stream);
+            cudaEventSynchronize(cev.end[3]);
             for (int i = 0; i < 4; ++i) {
+                if (i == 1 && !(q.components & 2)) continue;
                 float ms = 0.f;
-                cudaEventElapsedTime(&ms, cev.ev[i], cev.ev[i + 1]);
+                cudaEventElapsedTime(&ms, cev.start[i], cev.end[i]);
                 comp_ms[i] += ms;
             }
         }
@@ -701,11 +757,22 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         for (int i = 0; i < 4; ++i) prof.kernel_ms[i] = comp_ms[i];
         for (int i = 0; i < kMaxDepth; ++i) prof.chains[i] = cc[i];
         prof.edges = ec;
-        for (int i = 0; i < 5; ++i) cudaEventDestroy(cev.ev[i]);
+        for (int i = 0; i < 4; ++i) {
+            cudaEventDestroy(cev.start[i]);
+            cudaEventDestroy(cev.end[i]);
+        }
         prof.main_launches = (d->num_freq + kMaxNF - 1) / kMaxNF;
         cudaEventDestroy(ev_prep);
         cudaEventDestroy(ev_main0);
         cudaEventDestroy(ev_main1);
+    }
+    if (side != stream) {
+        // leave the side stream joined to the caller's stream (also when no
+        // per-cell kernel ran)
+        cudaEventRecord(join, side);
+        cudaStreamWaitEvent(stream, join, 0);
+        cudaEventDestroy(fork);
+        cudaEventDestroy(join);
     }
     if (layers64) cudaFreeAsync(layers64, stream);
     if (cudaGetLastError() != cudaSuccess) return 2;
