@@ -23,8 +23,10 @@
  *                         max_paths) + deterministic.py:461-514 (path table)
  *   wcb_field_*        <- kernels/fields.py facades over fields.cu:36-204 and
  *                         RayD's field_transmission_sequence
- *   wcb_rows_vjp       <- kernels/deterministic.py:186-367 and the field AD
- *                         Functions in kernels/fields.py:1087-2140
+ *   wcb_accumulate_flat* <- kernels/deterministic.py:23-367 over
+ *                         deterministic.cu:829-1262 (forward, adjoint, JVP)
+ *   wcb_rows_vjp       <- the field AD Functions in kernels/fields.py:1087-2140 and
+ *                         the frozen-winner re-solve of propagation/geometry.py:214-286
  */
 #ifndef WITWIN_CHANNEL_B200_H
 #define WITWIN_CHANNEL_B200_H
