@@ -30,28 +30,42 @@
 namespace wcb {
 namespace adj {
 
-__global__ void k_vjp_count(AdjParams p) {
+// per record: its parameter count, its (component, depth) grouping key and
+// the per-component record counts
+__global__ void k_vjp_count(AdjParams p, int* keys, int* idx) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= p.count) return;
+    const RowRec row = p.rows[p.selected[i]];
     ParamList pl;
-    build_params(p, p.rows[p.selected[i]], pl);
+    build_params(p, row, pl);
     p.counts[i] = pl.n;
+    const int rank = component_rank(row.component);
+    keys[i] = rank * 8 + min(max(int(row.depth), 0), 7);
+    idx[i] = int(i);
+    atomicAdd(p.comp_counts + rank, 1);
 }
 
-// one thread per parameter: its contributions are a contiguous run of the
-// id-sorted pairs, summed in record order
-__global__ void k_vjp_reduce(long long params, long long n, const unsigned* ids, const double* vals, double* grad) {
-    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (g >= params) return;
-    long long lo = 0, hi = n;
-    while (lo < hi) {
-        const long long mid = (lo + hi) >> 1;
-        if ((long long)ids[mid] < g) lo = mid + 1;
-        else hi = mid;
+// One block per run of equal ids in the id-sorted pairs (a parameter's
+// contributions): each thread sums a fixed strided subset in record order,
+// then a fixed-shape block tree; the result does not depend on timing, so
+// the gradient is deterministic.  Parameters without a run stay zero.
+constexpr int kReduceBlock = 256;
+
+__global__ void __launch_bounds__(kReduceBlock) k_vjp_reduce_runs(const unsigned* run_ids, const int* run_counts,
+                                                                   const long long* run_offsets, const int* num_runs,
+                                                                   const double* vals, double* grad) {
+    typedef cub::BlockReduce<double, kReduceBlock> Reduce;
+    __shared__ typename Reduce::TempStorage tmp;
+    const int runs = *num_runs;
+    for (int r = blockIdx.x; r < runs; r += gridDim.x) {
+        const long long beg = run_offsets[r];
+        const int n = run_counts[r];
+        double s = 0.0;
+        for (int q = threadIdx.x; q < n; q += kReduceBlock) s += vals[beg + q];
+        const double total = Reduce(tmp).Sum(s);
+        if (threadIdx.x == 0) grad[run_ids[r]] = total;
+        __syncthreads();
     }
-    double s = 0.0;
-    for (long long q = lo; q < n && (long long)ids[q] == g; ++q) s += vals[q];
-    grad[g] = s;
 }
 
 size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -60,7 +74,8 @@ size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
 // record count) come first; the (id, contribution) pairs and the sort scratch
 // (sized by the pair count) follow.
 struct VjpLayout {
-    size_t counts, offsets, scan_tmp, scan_bytes, ids, ids2, vals, vals2, sort_tmp, sort_bytes, total;
+    size_t counts, offsets, comp_counts, keys, keys2, order, order2, scan_tmp, scan_bytes, ids, ids2, vals, vals2,
+        run_ids, run_counts, run_offsets, num_runs, sort_tmp, sort_bytes, total;
 };
 
 VjpLayout vjp_layout(long long K, long long pairs) {
@@ -71,16 +86,33 @@ VjpLayout vjp_layout(long long K, long long pairs) {
     auto take = [&](size_t b) { const size_t a = o; o = a256(o + b); return a; };
     L.counts = take(k * 4);
     L.offsets = take(k * 8);
-    L.scan_bytes = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, L.scan_bytes, (int*)nullptr, (long long*)nullptr, int(k));
+    L.comp_counts = take(16);
+    L.keys = take(k * 4);
+    L.keys2 = take(k * 4);
+    L.order = take(k * 4);
+    L.order2 = take(k * 4);
+    size_t scan_b = 0, group_b = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_b, (int*)nullptr, (long long*)nullptr, int(k));
+    cub::DeviceRadixSort::SortPairs(nullptr, group_b, (int*)nullptr, (int*)nullptr, (int*)nullptr, (int*)nullptr,
+                                    int(k), 0, 5);
+    L.scan_bytes = std::max(scan_b, group_b);
     L.scan_tmp = take(L.scan_bytes);
     L.ids = take(m * 4);
     L.ids2 = take(m * 4);
     L.vals = take(m * 8);
     L.vals2 = take(m * 8);
-    L.sort_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, L.sort_bytes, (unsigned*)nullptr, (unsigned*)nullptr, (double*)nullptr,
-                                    (double*)nullptr, int(std::min<size_t>(m, INT_MAX)), 0, 32);
+    L.run_ids = take(m * 4);
+    L.run_counts = take(m * 4);
+    L.run_offsets = take(m * 8);
+    L.num_runs = take(16);
+    size_t sort_b = 0, rle_b = 0, roff_b = 0;
+    const int mi = int(std::min<size_t>(m, INT_MAX));
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_b, (unsigned*)nullptr, (unsigned*)nullptr, (double*)nullptr,
+                                    (double*)nullptr, mi, 0, 32);
+    cub::DeviceRunLengthEncode::Encode(nullptr, rle_b, (const unsigned*)nullptr, (unsigned*)nullptr, (int*)nullptr,
+                                       (int*)nullptr, mi);
+    cub::DeviceScan::ExclusiveSum(nullptr, roff_b, (int*)nullptr, (long long*)nullptr, mi);
+    L.sort_bytes = std::max(sort_b, std::max(rle_b, roff_b));
     L.sort_tmp = take(L.sort_bytes);
     L.total = o;
     return L;
@@ -213,28 +245,56 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
     long long* offsets = reinterpret_cast<long long*>(b + L.offsets);
     p.offsets = offsets;
     p.row_field = row_field;
+    p.comp_counts = reinterpret_cast<int*>(b + L.comp_counts);
+    int* keys = reinterpret_cast<int*>(b + L.keys);
+    int* keys2 = reinterpret_cast<int*>(b + L.keys2);
+    int* order = reinterpret_cast<int*>(b + L.order);
+    int* order2 = reinterpret_cast<int*>(b + L.order2);
     const int grid = int((K + wcb::adj::kBlock - 1) / wcb::adj::kBlock);
-    wcb::adj::k_vjp_count<<<grid, wcb::adj::kBlock, 0, s>>>(p);
+    cudaMemsetAsync(p.comp_counts, 0, 16, s);
+    wcb::adj::k_vjp_count<<<grid, wcb::adj::kBlock, 0, s>>>(p, keys, order);
     size_t tb = L.scan_bytes;
     if (cub::DeviceScan::ExclusiveSum(b + L.scan_tmp, tb, p.counts, offsets, int(K), s) != cudaSuccess)
         return WCB_ERR_CUDA;
-    wcb::note_launch(2);
+    // records grouped by (component, depth), record order kept within a group
+    tb = L.scan_bytes;
+    if (cub::DeviceRadixSort::SortPairs(b + L.scan_tmp, tb, keys, keys2, order, order2, int(K), 0, 5, s) !=
+        cudaSuccess)
+        return WCB_ERR_CUDA;
+    wcb::note_launch(3);
     long long last_off = 0;
     int last_cnt = 0;
+    int comp_counts[4] = {0, 0, 0, 0};
     cudaMemcpyAsync(&last_off, offsets + K - 1, 8, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&last_cnt, p.counts + K - 1, 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(comp_counts, p.comp_counts, 16, cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return WCB_ERR_CUDA;
+    p.order = order2;
     const long long pairs = last_off + last_cnt;
     if (pairs >= INT_MAX) return WCB_ERR_NOT_SUPPORTED;
     L = wcb::adj::vjp_layout(K, pairs);
     if (workspace_bytes < (long long)L.total) return WCB_ERR_CAPACITY;
     p.out_ids = reinterpret_cast<unsigned*>(b + L.ids);
     p.out_vals = reinterpret_cast<double*>(b + L.vals);
-    wcb::adj::k_vjp_rows<wcb::adj::kLanes, 0><<<grid, wcb::adj::kBlock, 0, s>>>(p);
-    wcb::adj::k_vjp_rows<wcb::adj::kLanes, 1><<<grid, wcb::adj::kBlock, 0, s>>>(p);
-    wcb::adj::k_vjp_rows<wcb::adj::kLanes, 5><<<grid, wcb::adj::kBlock, 0, s>>>(p);
-    wcb::adj::launch_vjp_diffraction(p, grid, s);
-    wcb::note_launch(4);
+    {
+        // one launch per component over its dense range of the grouped order
+        const int cids[4] = {0, 1, 5, 2};
+        long long begin = 0;
+        for (int r = 0; r < 4; ++r) {
+            p.order_begin = begin;
+            p.order_count = comp_counts[r];
+            begin += comp_counts[r];
+            if (p.order_count <= 0) continue;
+            const unsigned g = unsigned((p.order_count + wcb::adj::kBlock - 1) / wcb::adj::kBlock);
+            switch (cids[r]) {
+                case 0: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 0><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
+                case 1: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 1><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
+                case 5: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 5><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
+                default: wcb::adj::launch_vjp_diffraction(p, s); break;
+            }
+            wcb::note_launch();
+        }
+    }
     unsigned* ids2 = reinterpret_cast<unsigned*>(b + L.ids2);
     double* vals2 = reinterpret_cast<double*>(b + L.vals2);
     int end_bit = 1;
@@ -246,8 +306,25 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
             return WCB_ERR_CUDA;
         wcb::note_launch();
     }
-    wcb::adj::k_vjp_reduce<<<int((P + 255) / 256), 256, 0, s>>>(P, pairs, ids2, vals2, grad_out);
-    wcb::note_launch();
+    cudaMemsetAsync(grad_out, 0, size_t(P) * 8, s);
+    if (pairs > 0) {
+        unsigned* run_ids = reinterpret_cast<unsigned*>(b + L.run_ids);
+        int* run_counts = reinterpret_cast<int*>(b + L.run_counts);
+        long long* run_offsets = reinterpret_cast<long long*>(b + L.run_offsets);
+        int* num_runs = reinterpret_cast<int*>(b + L.num_runs);
+        tb = L.sort_bytes;
+        if (cub::DeviceRunLengthEncode::Encode(b + L.sort_tmp, tb, ids2, run_ids, run_counts, num_runs, int(pairs), s) !=
+            cudaSuccess)
+            return WCB_ERR_CUDA;
+        tb = L.sort_bytes;
+        if (cub::DeviceScan::ExclusiveSum(b + L.sort_tmp, tb, run_counts, run_offsets, int(std::min<long long>(pairs, P)),
+                                          s) != cudaSuccess)
+            return WCB_ERR_CUDA;
+        const int blocks = int(std::min<long long>(P, 4096));
+        wcb::adj::k_vjp_reduce_runs<<<blocks, wcb::adj::kReduceBlock, 0, s>>>(run_ids, run_counts, run_offsets, num_runs,
+                                                                             vals2, grad_out);
+        wcb::note_launch(3);
+    }
     rc = cudaGetLastError() == cudaSuccess ? WCB_OK : WCB_ERR_CUDA;
     return rc;
 }

@@ -100,6 +100,9 @@ struct AdjParams {
     // parameter id layout
     int base_meps, base_msig, base_leps, base_lsig, gid_freq, base_tx, base_rx;
     int* counts;
+    int* comp_counts;          // (4) records per component: LoS, reflection, transmission, diffraction
+    const int* order;          // record indices grouped by (component, depth)
+    long long order_begin, order_count;
     const long long* offsets;
     unsigned* out_ids;
     double* out_vals;
@@ -375,10 +378,14 @@ WCB_D Cx<Dual<N>> eval_record(const AdjParams& p, const RowRec& row, const Windo
 // Per-record VJP of one component: evaluate the record's path field with the
 // record's parameters as dual lanes, N at a time, and write one (id,
 // contribution) pair per parameter.  Records of other components are skipped.
+// rank of a component in the (component, depth) grouping
+WCB_HD int component_rank(int c) { return c == 0 ? 0 : c == 1 ? 1 : c == 5 ? 2 : 3; }
+
 template <int N, int COMP>
 __global__ void __launch_bounds__(kBlock) k_vjp_rows(AdjParams p) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= p.count) return;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= p.order_count) return;
+    const long long i = p.order[p.order_begin + j];
     const RowRec row = p.rows[p.selected[i]];
     if (row.component != COMP) return;
     ParamList pl;
@@ -409,7 +416,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp_rows(AdjParams p) {
     }
 }
 
-void launch_vjp_diffraction(const AdjParams& p, int grid, cudaStream_t s);
+void launch_vjp_diffraction(const AdjParams& p, cudaStream_t s);
 
 }  // namespace adj
 }  // namespace wcb

@@ -5,8 +5,9 @@
 namespace wcb {
 namespace adj {
 
-void launch_vjp_diffraction(const AdjParams& p, int grid, cudaStream_t s) {
-    k_vjp_rows<kLanes, 2><<<grid, kBlock, 0, s>>>(p);
+void launch_vjp_diffraction(const AdjParams& p, cudaStream_t s) {
+    if (p.order_count <= 0) return;
+    k_vjp_rows<kLanes, 2><<<unsigned((p.order_count + kBlock - 1) / kBlock), kBlock, 0, s>>>(p);
 }
 
 }  // namespace adj

@@ -318,16 +318,25 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
         const T blend = wb + (T(1) - wb) * t_mono;
         return (value - odd) * t_mono + odd * (gamma * blend);
     };
-    const Cx<T> t1 = mended(bm, +1, true);
-    const Cx<T> t2 = mended(bm, -1, true);
-    const Cx<T> t3 = mended(bp, +1, false);
-    const Cx<T> t4 = mended(bp, -1, false);
+    // the four KP terms: (beta-, +), (beta-, -) incident; (beta+, +) weighted by
+    // R_n, (beta+, -) weighted by R_0.  One loop body (not four inlined
+    // copies) keeps the kernel's instruction footprint small.
+    Cx<T> sum_soft = cx(T(0), T(0)), sum_hard = cx(T(0), T(0));
+#pragma unroll 1
+    for (int q = 0; q < 4; ++q) {
+        const bool incident = q < 2;
+        const Cx<T> term = mended(incident ? bm : bp, (q & 1) ? -1 : +1, incident);
+        const Cx<T> one = cx(T(1), T(0));
+        const Cx<T> w_soft = incident ? one : (q == 2 ? rn_te : r0_te);
+        const Cx<T> w_hard = incident ? one : (q == 2 ? rn_tm : r0_tm);
+        sum_soft = sum_soft + w_soft * term;
+        sum_hard = sum_hard + w_hard * term;
+    }
     // pre = -exp(-j pi/4) / (2 n sqrt(2 pi k) sin_b)
     const T pre_mag = T(1) / (T(2) * nn * s_sqrt(T(kTwoPi) * kT) * sin_b);
     const Cx<T> pre = cx(-inv_sqrt2 * pre_mag, inv_sqrt2 * pre_mag);
-    const Cx<T> inc = t1 + t2;
-    const Cx<T> d_soft = pre * (inc + rn_te * t3 + r0_te * t4);
-    const Cx<T> d_hard = pre * (inc + rn_tm * t3 + r0_tm * t4);
+    const Cx<T> d_soft = pre * sum_soft;
+    const Cx<T> d_hard = pre * sum_hard;
     // ray-fixed bases
     V3<T> phi_hat_p = cross(ef, sh_p);
     phi_hat_p = phi_hat_p * (T(1) / s_max(length(phi_hat_p), T(1e-12)));
