@@ -251,6 +251,7 @@ def run_native(args) -> None:
     e2e_value = rays_all / args.steps * e2e_steps / (e2e_ms / 1000.0)
     fp64 = _fp64_plain(compiled, ep, mats, freq, bits, cfg, device, step_ms / args.steps)
     vjp = None if args.no_vjp else _vjp_run(device)
+    batched = None if args.no_batched else _batched_run(device)
     if rank == 0:
         peaks = _peaks()
         hbm = float(peaks.get("hbm_gbs", HBM_FALLBACK))
@@ -311,6 +312,7 @@ def run_native(args) -> None:
             "cpu_baseline": cpu,
             "fp64_plain": fp64,
             "vjp": vjp,
+            "batched": batched,
             "gpu_launches": launches,
             "clocks": sampler.summary(),
             "wall_s": t_wall,
@@ -388,6 +390,98 @@ def _vjp_run(device, steps: int = 3) -> dict:
         "grad": {"eps_r": float(g["leaves"]["eps_r"].grad), "sigma_e": float(g["leaves"]["sigma_e"].grad),
                  "frequency": float(g["frequency"].grad), "tx": [float(x) for x in g["leaves"]["tx"].grad],
                  "vertices_norm": float(vg.norm())},
+    }
+
+
+def _batched_run(device) -> dict:
+    """The batched uneven workload: 8 scenes (16..256 boxes, grids 64^2..512^2),
+    4 Tx x {3.5, 6, 28, 39} GHz each, LoS + reflection depth 3 + UTD.  Mixed
+    precision batched (one launch sequence per scene for its 4 Tx and 4
+    frequencies, scenes on 4 streams) against the plain FP64 form (one solve
+    per scene, Tx and frequency), forward and forward + VJP."""
+    import torch
+
+    from witwin_channel_b200 import Config, solve
+    from witwin_channel_b200.autograd import vjp_forward
+    from witwin_channel_b200.batch import single_transmitter_scene, solve_batch
+    from witwin_channel_b200.scene import PhysicalMaterial
+    from witwin_channel_b200.workloads import BATCH_FREQS, batched_scenes
+
+    scenes = batched_scenes()
+    # differentiable values: one concrete material per scene (eps_r, sigma_e leaves) and the Tx positions
+    leaves = []
+    for sc in scenes:
+        eps = torch.tensor(5.24, dtype=torch.float64, requires_grad=True)
+        sig = torch.tensor(0.5, dtype=torch.float64, requires_grad=True)
+        mat = PhysicalMaterial(eps_r=eps, sigma_e=sig, thickness_m=0.3, name="concrete")
+        for st in sc.structures[1:]:
+            st.material = mat
+        for t in sc.transmitters:
+            t.position = t.position.detach().clone().requires_grad_(True)
+            leaves.append(t.position)
+        leaves += [eps, sig]
+    comps = {"los", "reflection", "diffraction"}
+    cfg = Config(components=comps, max_depth=3)
+    cfg_ad = Config(components=comps, max_depth=3, ad_mode="vjp")
+    subs = [[single_transmitter_scene(sc, t) for t in range(4)] for sc in scenes]  # compiled once, reused
+    cells = sum(int(sc.receivers[0].shape[0]) * int(sc.receivers[0].shape[1]) for sc in scenes)
+    jobs = cells * 4 * len(BATCH_FREQS)
+
+    def timed(fn, reps=1):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def fwd_batched():
+        solve_batch(scenes, cfg, BATCH_FREQS)
+
+    def fwd_plain():
+        for per_scene in subs:
+            for sub in per_scene:
+                for f in BATCH_FREQS:
+                    solve(sub, cfg, reference_frequency_hz=f, precision="fp64")
+
+    def vjp_batched():
+        for t in leaves:
+            t.grad = None
+        for sc in scenes:
+            v = vjp_forward(sc, cfg_ad, BATCH_FREQS)
+            (v["power_total"].double().sum() * 1e6).backward()
+
+    def vjp_plain():
+        for t in leaves:
+            t.grad = None
+        for per_scene in subs:
+            for sub in per_scene:
+                for f in BATCH_FREQS:
+                    solve(sub, cfg, reference_frequency_hz=f, precision="fp64")
+                    v = vjp_forward(sub, cfg_ad, [f])
+                    (v["power_total"].double().sum() * 1e6).backward()
+
+    fb = timed(fwd_batched, 3)
+    fp = timed(fwd_plain)
+    vb = timed(vjp_batched)
+    vp = timed(vjp_plain)
+    return {
+        "workload": "8 scenes (16..256 boxes, seeds 3..10), grids 64^2..512^2, 4 Tx x {3.5, 6, 28, 39} GHz each, "
+                    "LoS + reflection depth 3 + UTD; gradients for each scene's concrete eps_r, sigma_e and Tx positions",
+        "cell_jobs": jobs,
+        "forward_mixed_batched_ms": fb,
+        "forward_fp64_plain_ms": fp,
+        "forward_speedup": fp / fb,
+        "forward_cell_jobs_per_s": jobs / (fb / 1000.0),
+        "forward_vjp_mixed_batched_ms": fb + vb,
+        "forward_vjp_plain_ms": fp + vp,
+        "forward_vjp_speedup": (fp + vp) / (fb + vb),
+        "plain_form": "one FP64 cell-mode solve plus one single-frequency VJP per (scene, Tx, frequency)",
+        "batched_form": "one mixed-precision launch sequence per scene for its 4 Tx and 4 frequencies (scenes on 4 "
+                        "streams) plus one frozen-topology VJP per scene over the 4 frequencies",
     }
 
 
@@ -610,6 +704,7 @@ def main() -> None:
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-vjp", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "native":
         args.warmup = 3

@@ -38,15 +38,15 @@ class _State:
     compiled: Any
     ep: engine.Endpoints
     mats: Any
-    frequency: float
+    frequencies: list       # solve frequencies (Hz)
     components: int
     max_depth: int
     coherent: bool
     rows: torch.Tensor
     selected: torch.Tensor
-    flat: dict          # valid, tx, rx, cid (int32), per-row gain/field f64
-    saved64: dict       # FP64 accumulation outputs (linearisation point)
-    outputs32: dict     # FP32 accumulation outputs (the returned values)
+    flat: dict              # valid, tx, rx, cid (int32) of the selected records
+    saved64: list           # per frequency: FP64 accumulation outputs (linearisation point)
+    outputs32: list         # per frequency: FP32 accumulation outputs (the returned values)
     layer_counts: list
     vertex_mask: torch.Tensor | None = None
 
@@ -57,15 +57,26 @@ def _as_f64(x, device) -> torch.Tensor:
     return torch.tensor(float(x), dtype=torch.float64, device=device)
 
 
-def _differentiable_inputs(scene, compiled, freq_t: torch.Tensor, device) -> dict:
+def _stack0(values: list, device) -> torch.Tensor:
+    return torch.stack(values) if values else torch.zeros(0, dtype=torch.float64, device=device)
+
+
+def _differentiable_inputs(scene, compiled, freqs_t: torch.Tensor, device) -> dict:
+    """The scene values the solve is differentiated in: vertices (V,3), per
+    frequency material and layer eps_r / sigma_e (NF,M) and (NF,L), the
+    frequencies (NF,), Tx positions (T,3) and point-receiver positions (R,3)."""
     verts = [st.vertices.reshape(-1, 3).to(device=device, dtype=torch.float64) for st in scene.structures]
     V = torch.cat(verts) if verts else torch.zeros((0, 3), dtype=torch.float64, device=device)
-    mv = compiled.material_values(freq_t, keep_graph=True)
-    eps = torch.stack([_as_f64(x, device) for x in mv["eps_r"]]) if mv["eps_r"] else torch.zeros(0, dtype=torch.float64, device=device)
-    sig = torch.stack([_as_f64(x, device) for x in mv["sigma_e"]]) if mv["sigma_e"] else torch.zeros(0, dtype=torch.float64, device=device)
-    flat = [row for rows in mv["layers"] for row in rows]
-    leps = torch.stack([_as_f64(r[1], device) for r in flat]) if flat else torch.zeros(0, dtype=torch.float64, device=device)
-    lsig = torch.stack([_as_f64(r[2], device) for r in flat]) if flat else torch.zeros(0, dtype=torch.float64, device=device)
+    eps, sig, leps, lsig = [], [], [], []
+    layer_counts = []
+    for f in range(freqs_t.shape[0]):
+        mv = compiled.material_values(freqs_t[f], keep_graph=True)
+        eps.append(_stack0([_as_f64(x, device) for x in mv["eps_r"]], device))
+        sig.append(_stack0([_as_f64(x, device) for x in mv["sigma_e"]], device))
+        flat = [row for rows in mv["layers"] for row in rows]
+        leps.append(_stack0([_as_f64(r[1], device) for r in flat], device))
+        lsig.append(_stack0([_as_f64(r[2], device) for r in flat], device))
+        layer_counts = [len(rows) for rows in mv["layers"]]
     txs = scene.transmitters
     tx = torch.stack([t.position.reshape(3).to(device=device, dtype=torch.float64) for t in txs]) if txs else \
         torch.zeros((0, 3), dtype=torch.float64, device=device)
@@ -78,18 +89,19 @@ def _differentiable_inputs(scene, compiled, freq_t: torch.Tensor, device) -> dic
     # differentiate only the vertices of structures whose vertex tensor takes gradients
     mask = torch.cat([torch.full((st.vertices.reshape(-1, 3).shape[0],), int(bool(st.vertices.requires_grad)),
                                  dtype=torch.uint8) for st in scene.structures]).to(device) if verts else None
-    return {"vertices": V, "vertex_mask": mask, "eps_r": eps, "sigma_e": sig, "layer_eps_r": leps, "layer_sigma_e": lsig,
-            "frequency": freq_t.reshape(()).to(dtype=torch.float64), "tx": tx, "rx": rx,
-            "layer_counts": [len(rows) for rows in mv["layers"]]}
+    return {"vertices": V, "vertex_mask": mask, "eps_r": torch.stack(eps), "sigma_e": torch.stack(sig),
+            "layer_eps_r": torch.stack(leps), "layer_sigma_e": torch.stack(lsig),
+            "frequency": freqs_t.to(dtype=torch.float64), "tx": tx, "rx": rx, "layer_counts": layer_counts}
 
 
-def rows_vjp(state: _State, g_gain: torch.Tensor | None, g_re: torch.Tensor | None, g_im: torch.Tensor | None,
-             want: int, row_field: torch.Tensor | None = None,
+def rows_vjp(state: _State, freq_index: int, g_gain: torch.Tensor | None, g_re: torch.Tensor | None,
+             g_im: torch.Tensor | None, want: int, row_field: torch.Tensor | None = None,
              vertex_mask: torch.Tensor | None = None) -> tuple[torch.Tensor, list[int]]:
-    """Dense FP64 gradient over the native parameter layout (see ``wcb_rows_vjp``)."""
+    """Dense FP64 gradient over the native parameter layout (see ``wcb_rows_vjp``)
+    for the records' fields at frequency ``freq_index``."""
     lib = _native.load()
     device = state.rows.device
-    desc, keep = engine.make_desc(state.ep, [state.frequency], state.components, state.max_depth, state.coherent)
+    desc, keep = engine.make_desc(state.ep, state.frequencies, state.components, state.max_depth, state.coherent)
     ms = state.mats.as_struct()
     layout = (ctypes.c_int64 * 9)()
     _native.check(lib.wcb_rows_vjp_layout(state.compiled.native.handle, ctypes.byref(desc), ctypes.byref(ms), layout),
@@ -100,10 +112,10 @@ def rows_vjp(state: _State, g_gain: torch.Tensor | None, g_re: torch.Tensor | No
     max_layers = max(state.layer_counts) if state.layer_counts else 1
     _native.check(lib.wcb_rows_vjp_workspace_size(K, int(state.max_depth), int(max_layers), ctypes.byref(nbytes)),
                   "wcb_rows_vjp_workspace_size")
-    ws = torch.empty(max(nbytes.value, 256), dtype=torch.uint8, device=device)
+    ws = _VJP_WORKSPACE.get(nbytes.value, device)
     grad = torch.zeros(max(total, 1), dtype=torch.float64, device=device)
     _native.check(
-        lib.wcb_rows_vjp(state.compiled.native.handle, ctypes.byref(desc), ctypes.byref(ms), 0,
+        lib.wcb_rows_vjp(state.compiled.native.handle, ctypes.byref(desc), ctypes.byref(ms), int(freq_index),
                          _native.ptr(state.rows) if K else None, _native.ptr(state.selected) if K else None, K,
                          _native.ptr(g_gain), _native.ptr(g_re), _native.ptr(g_im), int(want),
                          _native.ptr(vertex_mask), _native.ptr(grad),
@@ -115,15 +127,18 @@ def rows_vjp(state: _State, g_gain: torch.Tensor | None, g_re: torch.Tensor | No
     return grad[:total], [int(layout[i]) for i in range(9)]
 
 
+_VJP_WORKSPACE = engine.Workspace()
+
+
 class _SolveFunction(torch.autograd.Function):
-    """Cell outputs of the frozen-topology solve as a function of the scene values."""
+    """Cell outputs (NF,T,R) / (NF,6,T,R) of the frozen-topology solve as a
+    function of the scene values."""
 
     @staticmethod
     def forward(ctx, state: _State, vertices, eps_r, sigma_e, layer_eps_r, layer_sigma_e, frequency, tx, rx):
         ctx.state = state
         ctx.shapes = [tuple(t.shape) for t in (vertices, eps_r, sigma_e, layer_eps_r, layer_sigma_e, frequency, tx, rx)]
-        o = state.outputs32
-        return tuple(o[k].clone() for k in ACCUM_FIELDS)
+        return tuple(torch.stack([o[k] for o in state.outputs32]) for k in ACCUM_FIELDS)
 
     @staticmethod
     def backward(ctx, *grads):
@@ -144,22 +159,81 @@ class _SolveFunction(torch.autograd.Function):
         if want == 0 or all(g is None for g in grads):
             return none
         T, R = state.ep.num_tx, state.ep.num_rx
-        g64 = [None if g is None else g.to(torch.float64).contiguous() for g in grads]
-        s = state.saved64
-        f = state.flat
-        per_row = deterministic_accumulate_flat_backward(
-            f["valid"], f["tx"], f["rx"], f["cid"], s["component_field_real"], s["component_field_imag"],
-            s["field_total_real"], s["field_total_imag"], s["power_total"], grad_power_total=g64[0],
-            grad_field_total_real=g64[1], grad_field_total_imag=g64[2], grad_component_power=g64[3],
-            grad_component_field_real=g64[4], grad_component_field_imag=g64[5], num_tx=T, num_rx=R,
-            coherent=state.coherent)
-        grad, lay = rows_vjp(state, per_row["grad_path_gain"], per_row["grad_field_real"],
-                             per_row["grad_field_imag"], want, vertex_mask=state.vertex_mask)
-        parts = [grad[lay[i]:lay[i + 1]] for i in range(8)]
-        out = [None]
-        for i, shape in enumerate(ctx.shapes):
-            out.append(parts[i].reshape(shape) if needs[i + 1] else None)
-        return tuple(out)
+        dev = state.rows.device
+        acc = [torch.zeros(shape, dtype=torch.float64, device=dev) for shape in ctx.shapes]
+        f_ = state.flat
+        for fi in range(len(state.frequencies)):
+            gf = [None if g is None else g[fi].to(torch.float64).contiguous() for g in grads]
+            if all(g is None for g in gf):
+                continue
+            s = state.saved64[fi]
+            per_row = deterministic_accumulate_flat_backward(
+                f_["valid"], f_["tx"], f_["rx"], f_["cid"], s["component_field_real"], s["component_field_imag"],
+                s["field_total_real"], s["field_total_imag"], s["power_total"], grad_power_total=gf[0],
+                grad_field_total_real=gf[1], grad_field_total_imag=gf[2], grad_component_power=gf[3],
+                grad_component_field_real=gf[4], grad_component_field_imag=gf[5], num_tx=T, num_rx=R,
+                coherent=state.coherent)
+            grad, lay = rows_vjp(state, fi, per_row["grad_path_gain"], per_row["grad_field_real"],
+                                 per_row["grad_field_imag"], want, vertex_mask=state.vertex_mask)
+            parts = [grad[lay[i]:lay[i + 1]] for i in range(8)]
+            acc[0] += parts[0].reshape(ctx.shapes[0])
+            for i in (1, 2, 3, 4):
+                acc[i][fi] += parts[i]
+            acc[5][fi] += parts[5][0] if parts[5].numel() else 0.0
+            acc[6] += parts[6].reshape(ctx.shapes[6])
+            acc[7] += parts[7].reshape(ctx.shapes[7])
+        return (None,) + tuple(a if needs[i + 1] else None for i, a in enumerate(acc))
+
+
+def vjp_forward(scene: Any, config, frequencies_hz) -> dict:
+    """Row-mode forward at every frequency (geometry and records frozen once)
+    with autograd-connected cell outputs: ``path_gain``/``field_total_*`` (NF,T,R),
+    ``component_*`` (NF,6,T,R) in the flat (tx, rx) order, plus the records."""
+    if not config.coherent and "diffraction" in config.components:
+        raise NotImplementedError("ad_mode='vjp' with incoherent accumulation and diffraction is not provided")
+    device = torch.device("cuda", torch.cuda.current_device())
+    if isinstance(frequencies_hz, torch.Tensor):
+        freqs_t = frequencies_hz.to(device=device).reshape(-1)
+    else:
+        freqs_t = torch.tensor([float(f) for f in frequencies_hz], dtype=torch.float64, device=device)
+    frequencies = [float(f) for f in freqs_t.detach().cpu()]
+    compiled = compile_scene(scene, device)
+    from .deterministic import _endpoints
+
+    ep = _endpoints(scene, device)
+    mats = compiled.material_tables(frequencies, device)
+    bits = engine.component_bits(config.components)
+    T, R = ep.num_tx, ep.num_rx
+    res = engine.run_solve(compiled, ep, mats, frequencies, components=bits, max_depth=config.max_depth,
+                           coherent=config.coherent, want_rows=True)
+    rows = res["rows"]
+    width = max(int(config.max_depth), 0)
+    selected = engine.select_rows(rows, width, config.max_paths, config.max_paths_scope)
+    dec = engine.decode_rows(rows, selected)
+    K = int(selected.shape[0])
+    flat = {"valid": torch.ones(K, dtype=torch.bool, device=device), "tx": dec["tx_id"], "rx": dec["rx_id"],
+            "cid": dec["component_id"].contiguous()}
+    outputs32, saved64, evs = [], [], []
+    for fi in range(len(frequencies)):
+        ev = engine.evaluate_rows(compiled, ep, mats, frequencies, fi, rows, selected, width, components=bits,
+                                  max_depth=config.max_depth, coherent=config.coherent)
+        pf = ev["path_field"]
+        g32, r32, i32 = ev["path_gain"].contiguous(), pf.real.contiguous(), pf.imag.contiguous()
+        outputs32.append(_forward(flat["valid"], flat["tx"], flat["rx"], flat["cid"], g32, r32, i32, T, R,
+                                  config.coherent, 0))
+        saved64.append(_forward(flat["valid"], flat["tx"], flat["rx"], flat["cid"], g32.double(), r32.double(),
+                                i32.double(), T, R, config.coherent, 0))
+        evs.append(ev)
+    inputs = _differentiable_inputs(scene, compiled, freqs_t, device)
+    state = _State(compiled=compiled, ep=ep, mats=mats, frequencies=frequencies, components=bits,
+                   max_depth=config.max_depth, coherent=config.coherent, rows=rows, selected=selected, flat=flat,
+                   saved64=saved64, outputs32=outputs32, layer_counts=inputs["layer_counts"],
+                   vertex_mask=inputs["vertex_mask"])
+    out = _SolveFunction.apply(state, inputs["vertices"], inputs["eps_r"], inputs["sigma_e"], inputs["layer_eps_r"],
+                               inputs["layer_sigma_e"], inputs["frequency"], inputs["tx"], inputs["rx"])
+    result = dict(zip(ACCUM_FIELDS, out))
+    result.update(compiled=compiled, ep=ep, dec=dec, evaluations=evs, count=K, width=width)
+    return result
 
 
 def solve_vjp(scene: Any, config, reference_frequency_hz):
@@ -170,59 +244,29 @@ def solve_vjp(scene: Any, config, reference_frequency_hz):
         _OPTIONAL_COMPONENTS,
         _SLOTS,
         Result,
-        _endpoints,
         _layout,
         _metadata,
         _path_table,
     )
 
-    if not config.coherent and "diffraction" in config.components:
-        raise NotImplementedError("ad_mode='vjp' with incoherent accumulation and diffraction is not provided")
-    device = torch.device("cuda", torch.cuda.current_device())
-    if isinstance(reference_frequency_hz, torch.Tensor):
-        freq_t = reference_frequency_hz.to(device=device)
-    else:
-        freq_t = torch.tensor(float(reference_frequency_hz), dtype=torch.float64, device=device)
-    frequency = float(freq_t.detach())
-    compiled = compile_scene(scene, device)
-    ep = _endpoints(scene, device)
-    mats = compiled.material_tables([frequency], device)
-    bits = engine.component_bits(config.components)
-    T, R = ep.num_tx, ep.num_rx
     launches0 = _native.launch_count()
-    res = engine.run_solve(compiled, ep, mats, [frequency], components=bits, max_depth=config.max_depth,
-                           coherent=config.coherent, want_rows=True)
-    rows = res["rows"]
-    width = max(int(config.max_depth), 0)
-    selected = engine.select_rows(rows, width, config.max_paths, config.max_paths_scope)
-    ev = engine.evaluate_rows(compiled, ep, mats, [frequency], 0, rows, selected, width, components=bits,
-                              max_depth=config.max_depth, coherent=config.coherent)
-    dec = engine.decode_rows(rows, selected)
-    K = int(selected.shape[0])
-    flat = {"valid": torch.ones(K, dtype=torch.bool, device=device), "tx": dec["tx_id"], "rx": dec["rx_id"],
-            "cid": dec["component_id"].contiguous()}
-    pf = ev["path_field"]
-    g32, r32, i32 = ev["path_gain"].contiguous(), pf.real.contiguous(), pf.imag.contiguous()
-    outputs32 = _forward(flat["valid"], flat["tx"], flat["rx"], flat["cid"], g32, r32, i32, T, R, config.coherent, 0)
-    saved64 = _forward(flat["valid"], flat["tx"], flat["rx"], flat["cid"], g32.double(), r32.double(), i32.double(),
-                       T, R, config.coherent, 0)
-    inputs = _differentiable_inputs(scene, compiled, freq_t, device)
-    state = _State(compiled=compiled, ep=ep, mats=mats, frequency=frequency, components=bits,
-                   max_depth=config.max_depth, coherent=config.coherent, rows=rows, selected=selected, flat=flat,
-                   saved64=saved64, outputs32=outputs32, layer_counts=inputs["layer_counts"],
-                   vertex_mask=inputs["vertex_mask"])
-    pt, ftr, fti, cp, cfr, cfi = _SolveFunction.apply(
-        state, inputs["vertices"], inputs["eps_r"], inputs["sigma_e"], inputs["layer_eps_r"], inputs["layer_sigma_e"],
-        inputs["frequency"], inputs["tx"], inputs["rx"])
-    rx = ep.rx
+    freq = reference_frequency_hz.reshape(1) if isinstance(reference_frequency_hz, torch.Tensor) else \
+        [float(reference_frequency_hz)]
+    v = vjp_forward(scene, config, freq)
+    device = v["power_total"].device
+    pt, ftr, fti = v["power_total"][0], v["field_total_real"][0], v["field_total_imag"][0]
+    cp, cfr, cfi = v["component_power"][0], v["component_field_real"][0], v["component_field_imag"][0]
+    rx = v["ep"].rx
     names = _BASE_COMPONENTS + tuple(n for n in _OPTIONAL_COMPONENTS if n in config.components)
     comp_power = {n: _layout(cp[_SLOTS[n]], rx) for n in names}
     comp_fields = {n: _layout(torch.complex(cfr[_SLOTS[n]], cfi[_SLOTS[n]]), rx) for n in names} \
         if config.return_field else {n: torch.empty((0,), dtype=torch.complex64, device=device) for n in names}
+    dec = v["dec"]
     counts = {name: int((dec["component_id"] == c).sum().item())
               for name, c in (("los", 0), ("reflection", 1), ("diffraction", 2), ("transmission", 5))}
-    paths = _path_table(dec, ev, width, compiled, config.return_field) if config.export_paths else None
-    meta = _metadata(config, counts, K, _native.launch_count() - launches0, {"ad": "fixed-topology vjp"})
+    paths = _path_table(dec, v["evaluations"][0], v["width"], v["compiled"], config.return_field) \
+        if config.export_paths else None
+    meta = _metadata(config, counts, v["count"], _native.launch_count() - launches0, {"ad": "fixed-topology vjp"})
     return Result(
         path_gain=_layout(pt, rx),
         field=_layout(torch.complex(ftr, fti), rx) if config.return_field

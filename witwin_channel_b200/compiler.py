@@ -129,6 +129,7 @@ class CompiledScene:
     face_material: torch.Tensor
     num_vertices: int
     structure_vertex_offsets: list = field(default_factory=list)
+    row_count_hint: int = 0  # path records of the last row-mode solve (sizes the next record buffer)
 
     # ---- material tables ------------------------------------------------
     def material_values(self, frequency: float, *, keep_graph: bool = False) -> dict[str, list]:

@@ -78,6 +78,13 @@ def make_desc(ep: Endpoints, frequencies: list[float], components: int, max_dept
     return d, freqs
 
 
+def check_device_status(status: torch.Tensor) -> None:
+    """Raise if a solve's device status word has a failure bit set (reads it: a sync)."""
+    st = int(status.item())
+    if st != 0:
+        raise RuntimeError(f"native solve reported device status bits {st:#x} (traversal stack overflow)")
+
+
 def component_bits(components) -> int:
     bits = 0
     if "los" in components:
@@ -132,17 +139,20 @@ def alloc_cells(nf: int, T: int, R: int, device: torch.device, fp64: bool = Fals
 def run_solve(compiled: CompiledScene, ep: Endpoints, mats: MaterialTables, frequencies: list[float], *,
               components: int, max_depth: int, coherent: bool, precision: int = _native.PRECISION_MIXED,
               cells: CellOutputs | None = None, want_rows: bool = False, row_capacity: int | None = None,
-              discovery_rays: int = 0) -> dict:
+              discovery_rays: int = 0, check_status: bool = True, workspace: Workspace | None = None) -> dict:
     lib = _native.load()
     device = ep.tx_pos.device
     desc, keep = make_desc(ep, frequencies, components, max_depth, coherent, precision, discovery_rays)
     nbytes = ctypes.c_int64()
     _native.check(lib.wcb_solve_workspace_size(compiled.native.handle, ctypes.byref(desc), ctypes.byref(nbytes)),
                   "wcb_solve_workspace_size")
-    ws = _WORKSPACE.get(nbytes.value, device)
+    ws = (workspace or _WORKSPACE).get(nbytes.value, device)
     status = torch.zeros(1, dtype=torch.int32, device=device)
     row_count = torch.zeros(1, dtype=torch.int64, device=device)
-    capacity = row_capacity if row_capacity is not None else max(1024, ep.num_tx * ep.num_rx * 4)
+    # row capacity: the caller's, else the last count seen on this scene (with
+    # headroom), else 8 records per cell; a short buffer makes the solve run again
+    hint = compiled.row_count_hint
+    capacity = row_capacity if row_capacity is not None else max(1024, ep.num_tx * ep.num_rx * 8, int(hint * 1.25))
     while True:
         rows = torch.empty((capacity, _native.ROW_WORDS), dtype=torch.int32, device=device) if want_rows else None
         out = _native.Outputs()
@@ -160,17 +170,17 @@ def run_solve(compiled: CompiledScene, ep: Endpoints, mats: MaterialTables, freq
                            ctypes.byref(out), _native.ptr(ws), ws.numel(), _native.stream_handle(device))
         del mats_struct
         if rc == _native.WCB_ERR_CAPACITY and want_rows:
-            capacity = int(row_count.item()) + 1024
+            capacity = int(int(row_count.item()) * 1.25) + 1024
             continue
         _native.check(rc, "wcb_solve")
         break
-    st = int(status.item())
-    if st != 0:
-        raise RuntimeError(f"native solve reported device status bits {st:#x} (traversal stack overflow)")
-    result = {"desc": desc, "keep": keep}
+    if check_status:
+        check_device_status(status)
+    result = {"desc": desc, "keep": keep, "status": status, "workspace": ws}
     if want_rows:
         n = int(row_count.item())
         result["rows"] = rows[:n]
+        compiled.row_count_hint = max(n, compiled.row_count_hint)
     return result
 
 
