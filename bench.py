@@ -252,6 +252,7 @@ def run_native(args) -> None:
     fp64 = _fp64_plain(compiled, ep, mats, freq, bits, cfg, device, step_ms / args.steps)
     vjp = None if args.no_vjp else _vjp_run(device)
     batched = None if args.no_batched else _batched_run(device)
+    large = None if args.no_large else _large_run(device)
     if rank == 0:
         peaks = _peaks()
         hbm = float(peaks.get("hbm_gbs", HBM_FALLBACK))
@@ -313,6 +314,7 @@ def run_native(args) -> None:
             "fp64_plain": fp64,
             "vjp": vjp,
             "batched": batched,
+            "large": large,
             "gpu_launches": launches,
             "clocks": sampler.summary(),
             "wall_s": t_wall,
@@ -391,6 +393,61 @@ def _vjp_run(device, steps: int = 3) -> dict:
                  "frequency": float(g["frequency"].grad), "tx": [float(x) for x in g["leaves"]["tx"].grad],
                  "vertices_norm": float(vg.norm())},
     }
+
+
+def _large_run(device, steps: int = 2) -> dict:
+    """The large-city workload: 2048 boxes with subdivided roofs (~112k
+    triangles), 25% with an interior two-layer glass sheet, 1 Tx, 1024^2 grid,
+    28 GHz, LoS + reflection depth 5 + UTD + transmission, paths exported and
+    converted to a CFR over 1024 subcarriers spanning 400 MHz."""
+    import numpy as np
+    import torch
+
+    from witwin_channel_b200 import Config, _native, solve
+    from witwin_channel_b200.channel import cfr
+    from witwin_channel_b200.workloads import large_city_scene
+
+    scene, freq = large_city_scene()
+    cfg = Config(components={"los", "reflection", "diffraction", "transmission"}, max_depth=5, export_paths=True,
+                 return_field=False)
+    freqs = (np.arange(1024) - 512) * 390.625e3
+    R = int(scene.receivers[0].shape[0]) * int(scene.receivers[0].shape[1])
+    _native.profile_enable(True)
+    res = solve(scene, cfg, reference_frequency_hz=freq)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record()
+    for _ in range(steps):
+        res = solve(scene, cfg, reference_frequency_hz=freq)
+    e[1].record()
+    prof = _native.profile_read()
+    h = cfr(res.paths, freqs, num_tx=1, num_rx=R)
+    torch.cuda.synchronize()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record()
+    for _ in range(steps):
+        h = cfr(res.paths, freqs, num_tx=1, num_rx=R)
+    c1.record()
+    torch.cuda.synchronize()
+    rays = prof["rays"] + prof["prep_rays"]
+    cfr_ms = c0.elapsed_time(c1) / steps
+    out = {
+        "workload": "2048 boxes (46x46 lots, roofs split 4x4, ~112k triangles, 25% with a 2-layer glass sheet), "
+                    "1 Tx, 1024x1024 grid at 1 m, 28 GHz, LoS + reflection depth 5 + UTD + transmission; CFR "
+                    "over 1024 subcarriers (390.625 kHz spacing)",
+        "triangles": int(sum(int(st.faces.shape[0]) for st in scene.structures)),
+        "solve_ms": e[0].elapsed_time(e[1]) / steps,
+        "kernel_ms": prof["kernel_ms"],
+        "rays": rays,
+        "rays_per_s_kernels": rays / ((prof["main_ms"] + prof["prep_ms"]) / 1000.0),
+        "paths": int(res.metadata["counts"]["path_count"]),
+        "cfr_ms": cfr_ms,
+        "cfr_bytes": int(h.numel() * 8),
+        "cfr_write_gbs": h.numel() * 8 / (cfr_ms / 1000.0) / 1e9,
+    }
+    del h, res
+    torch.cuda.empty_cache()
+    return out
 
 
 def _batched_run(device) -> dict:
@@ -705,6 +762,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-vjp", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-large", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "native":
         args.warmup = 3

@@ -286,6 +286,18 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
                  int32_t want, const uint8_t* vertex_mask, double* grad_out, int64_t grad_size, double* row_field,
                  void* workspace, int64_t workspace_bytes, void* stream);
 
+/* Channel frequency response of path records (replaces PathResult.cfr,
+ * path.py:646-656): per (tx, rx) cell and subcarrier k,
+ * H_k = sum_p a_p exp(-j 2 pi (tau_p - tau_min) f_k), tau_min the cell's
+ * smallest delay when normalize_delays (else 0).  Records (tx, rx, delay,
+ * complex coefficient a) must be grouped by cell in (rx, tx) order (the
+ * canonical order).  Subcarriers: f0 + k df for df != 0, else the device
+ * array `frequencies` (num_freq, FP64); num_freq <= 2048.  out: (T,R,num_freq)
+ * complex64, every element written once. */
+int wcb_cfr(const int32_t* tx_id, const int32_t* rx_id, const float* delay_s, const float* path_field,
+            int64_t num_paths, int32_t num_tx, int32_t num_rx, int32_t num_freq, double f0, double df,
+            const double* frequencies, int32_t normalize_delays, float* out, void* stream);
+
 /* Standalone field operators (reference kernels/fields.py facades).  All
  * arrays are device f32; complex outputs interleaved.  N rows. */
 int wcb_field_free_space(int64_t n, const float* source, const float* target, const float* tx_power,
