@@ -292,11 +292,13 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
  * smallest delay when normalize_delays (else 0).  Records (tx, rx, delay,
  * complex coefficient a) must be grouped by cell in (rx, tx) order (the
  * canonical order).  Subcarriers: f0 + k df for df != 0, else the device
- * array `frequencies` (num_freq, FP64); num_freq <= 2048.  out: (T,R,num_freq)
- * complex64, every element written once. */
+ * array `frequencies` (num_freq, FP64).  out: (T,R,num_freq) complex64, every
+ * element written once.  Workspace: wcb_cfr_workspace_size bytes. */
+int wcb_cfr_workspace_size(int32_t num_tx, int32_t num_rx, int64_t* bytes);
 int wcb_cfr(const int32_t* tx_id, const int32_t* rx_id, const float* delay_s, const float* path_field,
             int64_t num_paths, int32_t num_tx, int32_t num_rx, int32_t num_freq, double f0, double df,
-            const double* frequencies, int32_t normalize_delays, float* out, void* stream);
+            const double* frequencies, int32_t normalize_delays, float* out, void* workspace,
+            int64_t workspace_bytes, void* stream);
 
 /* Standalone field operators (reference kernels/fields.py facades).  All
  * arrays are device f32; complex outputs interleaved.  N rows. */

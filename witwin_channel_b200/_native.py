@@ -150,6 +150,7 @@ EXPORTED_SYMBOLS = (
     "wcb_rows_vjp_layout",
     "wcb_rows_vjp_workspace_size",
     "wcb_rows_vjp",
+    "wcb_cfr_workspace_size",
     "wcb_cfr",
     "wcb_field_free_space",
     "wcb_field_reflection_sequence",
@@ -217,8 +218,9 @@ def load() -> ctypes.CDLL:
     lib.wcb_rows_vjp.argtypes = [_vp, ctypes.POINTER(SolveDesc), ctypes.POINTER(Materials), ctypes.c_int32, _vp, _vp,
                                  ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int32, _vp, _vp, ctypes.c_int64, _vp, _vp,
                                  ctypes.c_int64, _vp]
+    lib.wcb_cfr_workspace_size.argtypes = [ctypes.c_int32, ctypes.c_int32, _i64p]
     lib.wcb_cfr.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
-                            ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int32, _vp, _vp]
+                            ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int32, _vp, _vp, ctypes.c_int64, _vp]
     lib.wcb_field_free_space.argtypes = [ctypes.c_int64] + [_vp] * 5 + [ctypes.c_double] + [_vp] * 7 + [_vp]
     lib.wcb_field_reflection_sequence.argtypes = [ctypes.c_int64, ctypes.c_int32] + [_vp] * 12 + [ctypes.c_double] + [_vp] * 7 + [_vp]
     lib.wcb_field_transmission_sequence.argtypes = [ctypes.c_int64, ctypes.c_int32] + [_vp] * 8 + [

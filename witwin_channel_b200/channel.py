@@ -11,9 +11,13 @@ written once.
 
 from __future__ import annotations
 
+import ctypes
+
 import torch
 
-from . import _native
+from . import _native, engine
+
+_CFR_WORKSPACE = engine.Workspace()
 
 
 def _coefficients(paths) -> torch.Tensor:
@@ -22,7 +26,7 @@ def _coefficients(paths) -> torch.Tensor:
 
 def cfr(paths, frequencies, *, num_tx: int, num_rx: int, normalize_delays: bool = True) -> torch.Tensor:
     """(num_tx, num_rx, K) complex64 frequency response at ``frequencies`` (Hz,
-    shape (K,); K <= 2048).  An evenly spaced grid takes the rotation fast path."""
+    shape (K,)).  An evenly spaced grid takes the rotation fast path."""
     if not isinstance(frequencies, torch.Tensor):
         frequencies = torch.as_tensor(frequencies, dtype=torch.float64)
     if frequencies.ndim != 1:
@@ -41,16 +45,23 @@ def cfr(paths, frequencies, *, num_tx: int, num_rx: int, normalize_delays: bool 
     elif K == 1:
         df = 1.0  # a single subcarrier: any step works
     n = int(paths.tx_id.shape[0])
+    if n > 1:
+        key = paths.rx_id.long() * max(int(num_tx), 1) + paths.tx_id.long()
+        if bool((key[1:] < key[:-1]).any()):
+            raise ValueError("paths must be in the canonical (rx, tx) order of an exported path table")
     out = torch.empty((num_tx, num_rx, K), dtype=torch.complex64, device=device)
     a = _coefficients(paths).contiguous()
     lib = _native.load()
+    nbytes = ctypes.c_int64()
+    _native.check(lib.wcb_cfr_workspace_size(int(num_tx), int(num_rx), ctypes.byref(nbytes)), "wcb_cfr_workspace_size")
+    ws = _CFR_WORKSPACE.get(nbytes.value, device)
     _native.check(
         lib.wcb_cfr(_native.ptr(paths.tx_id.contiguous()) if n else None,
                     _native.ptr(paths.rx_id.contiguous()) if n else None,
                     _native.ptr(paths.delay_s.float().contiguous()) if n else None,
                     _native.ptr(torch.view_as_real(a)) if n else None, n, int(num_tx), int(num_rx), K,
                     float(f_host[0]), df, _native.ptr(freqs), int(bool(normalize_delays)), _native.ptr(out),
-                    _native.stream_handle(device)),
+                    _native.ptr(ws), ws.numel(), _native.stream_handle(device)),
         "wcb_cfr",
     )
     return out
