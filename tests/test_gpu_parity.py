@@ -202,3 +202,17 @@ def test_solve_is_deterministic():
     a = solve(scene, cfg, reference_frequency_hz=freq).path_gain
     b = solve(scene, cfg, reference_frequency_hz=freq).path_gain
     assert torch.equal(a, b)
+
+
+def test_compiled_scene_is_cached_and_invalidated():
+    import torch as _t
+
+    from witwin_channel_b200.compiler import compile_scene
+
+    scene = scenes.two_wall_scene()
+    dev = _t.device("cuda")
+    a = compile_scene(scene, dev)
+    assert compile_scene(scene, dev) is a
+    with _t.no_grad():
+        scene.structures[0].vertices.add_(0.0)  # bumps the tensor version: geometry may have changed
+    assert compile_scene(scene, dev) is not a

@@ -195,7 +195,9 @@ class CompiledScene:
         )
 
 
-_CACHE: "weakref.WeakKeyDictionary[Any, tuple[tuple, CompiledScene]]" = weakref.WeakKeyDictionary()
+# compiled scenes keyed by the scene object's identity (scene types need not be
+# hashable); an entry dies with its scene through the weak reference's callback
+_CACHE: dict[int, tuple[Any, tuple, "CompiledScene"]] = {}
 
 
 def _geometry_token(scene: Any) -> tuple:
@@ -211,14 +213,14 @@ def _geometry_token(scene: Any) -> tuple:
 def compile_scene(scene: Any, device: torch.device | None = None) -> CompiledScene:
     """Compile (or fetch from the per-scene cache) the device scene."""
 
-    device = device or torch.device("cuda")
+    if device is None or (device.type == "cuda" and device.index is None):
+        device = torch.device("cuda", torch.cuda.current_device())
     token = _geometry_token(scene)
-    try:
-        cached = _CACHE.get(scene)
-    except TypeError:
-        cached = None
-    if cached is not None and cached[0] == token:
-        return cached[1]
+    scene_key = id(scene)
+    cached = _CACHE.get(scene_key)
+    if cached is not None and cached[0] is not None and cached[0]() is scene and cached[1] == token \
+            and cached[2].face_material.device == device:
+        return cached[2]
     verts, faces, fsurf, fstruct, fmat = [], [], [], [], []
     materials: list = []
     mat_index: dict[int, int] = {}
@@ -256,9 +258,11 @@ def compile_scene(scene: Any, device: torch.device | None = None) -> CompiledSce
     compiled = CompiledScene(scene=scene, native=native, materials=materials, face_material=fm,
                              num_vertices=int(V.shape[0]), structure_vertex_offsets=offsets)
     try:
-        _CACHE[scene] = (token, compiled)
-    except TypeError:
-        pass
+        ref = weakref.ref(scene, lambda _r, k=scene_key: _CACHE.pop(k, None))
+    except TypeError:  # not weak-referenceable: compile on every call
+        ref = None
+    if ref is not None:
+        _CACHE[scene_key] = (ref, token, compiled)
     return compiled
 
 
