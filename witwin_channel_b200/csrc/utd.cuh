@@ -106,9 +106,20 @@ WCB_HD FresnelPair<T> fresnel(T x) {
     return out;
 }
 
-// |(1+j)/2 - (C(x) + jS(x))| for any real x.
+// |(1+j)/2 - (C(x) + jS(x))| for any real x.  The squared modulus equals
+// f(x)^2 + g(x)^2 with the auxiliary functions f, g of Abramowitz & Stegun
+// 7.3.5-7.3.6; for x >= 6 in FP32 their asymptotic series (A&S 7.3.27-7.3.28:
+// pi x f ~ 1 - 3u^2 + 105u^4, pi x g ~ u - 15u^3 + 945u^5, u = 1/(pi x^2))
+// is accurate to ~5e-9 relative and replaces the continued fraction.
 template <typename T>
 WCB_HD T fresnel_complement_abs(T x) {
+    if (sizeof(T) == 4 && value_of(x) >= 6.0) {
+        const T u = T(1) / (T(kPi) * x * x);
+        const T u2 = u * u;
+        const T pf = T(1) - T(3) * u2 + T(105) * u2 * u2;
+        const T pg = u * (T(1) - T(15) * u2 + T(945) * u2 * u2);
+        return s_sqrt(pf * pf + pg * pg) / (T(kPi) * x);
+    }
     if (value_of(x) >= 0) {
         const FresnelPair<T> p = fresnel_pos(x, false);
         return p.has_h ? x * cabs(p.h) : cabs(p.complement);
