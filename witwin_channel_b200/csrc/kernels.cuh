@@ -287,10 +287,9 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
     for (int f = 0; f < NF; ++f) { acc[f] = cx(T(0), T(0)); gain[f] = T(0); }
     unsigned long long rays = 0;
     int qa = 0, qb = 0;
-    int global_c = 0;  // running candidate index across depths (interleaving key)
 
     // stage B: visibility + field for 32 items (FP64 hits recomputed)
-    auto process_b = [&](int n) {
+    auto process_b = [&](int n) __attribute__((always_inline)) {
         int it_lane = 0, c = 0, d = 1;
         if (lane < n) {
             it_lane = sh->qb[3 * lane];
@@ -371,7 +370,7 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
     };
 
     // stage A: FP64 back projection + containment for 32 items
-    auto process_a = [&](int n) {
+    auto process_a = [&](int n) __attribute__((always_inline)) {
         int it_lane = 0, c = 0, d = 1;
         if (lane < n) {
             it_lane = sh->qa[3 * lane];
@@ -406,55 +405,75 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
         }
         __syncwarp();
         qb += __popc(mask);
-        while (qb >= 32) {
-            process_b(32);
-            // shift queue B (items and faces)
-            const int rem = qb - 32;
-            int a0 = 0, a1 = 0, a2 = 0, fb[kMaxDepth];
-            if (lane < rem) {
-                a0 = sh->qb[3 * (32 + lane)];
-                a1 = sh->qb[3 * (32 + lane) + 1];
-                a2 = sh->qb[3 * (32 + lane) + 2];
-                for (int k = 0; k < kMaxDepth; ++k) fb[k] = sh->qbf[kMaxDepth * (32 + lane) + k];
-            }
-            __syncwarp();
-            if (lane < rem) {
-                sh->qb[3 * lane] = a0;
-                sh->qb[3 * lane + 1] = a1;
-                sh->qb[3 * lane + 2] = a2;
-                for (int k = 0; k < kMaxDepth; ++k) sh->qbf[kMaxDepth * lane + k] = fb[k];
-            }
-            __syncwarp();
-            qb = rem;
+    };
+
+    // drop the first n items of queue B (items and their faces)
+    auto pop_b = [&](int n) __attribute__((always_inline)) {
+        const int rem = qb - n;
+        int a0 = 0, a1 = 0, a2 = 0, fb[kMaxDepth];
+        if (lane < rem) {
+            a0 = sh->qb[3 * (n + lane)];
+            a1 = sh->qb[3 * (n + lane) + 1];
+            a2 = sh->qb[3 * (n + lane) + 2];
+#pragma unroll
+            for (int k = 0; k < kMaxDepth; ++k) fb[k] = sh->qbf[kMaxDepth * (n + lane) + k];
         }
+        __syncwarp();
+        if (lane < rem) {
+            sh->qb[3 * lane] = a0;
+            sh->qb[3 * lane + 1] = a1;
+            sh->qb[3 * lane + 2] = a2;
+#pragma unroll
+            for (int k = 0; k < kMaxDepth; ++k) sh->qbf[kMaxDepth * lane + k] = fb[k];
+        }
+        __syncwarp();
+        qb = rem;
     };
 
     if ((p.components & 2) && sc.num_faces > 0) {
-        for (int d = 1; d <= p.max_depth; ++d) {
-            const int cnt = p.chain_count[t * kMaxDepth + (d - 1)];
-            const long long base = p.chain_offset[t * kMaxDepth + (d - 1)];
-            // this warp takes every kSplitWarps-th candidate of the transmitter
-            const int first = (warp - global_c % kSplitWarps + kSplitWarps) % kSplitWarps;
-            global_c += cnt;
-            for (int c = first; c < cnt; c += kSplitWarps) {
+        // One loop drives the three stages so each is inlined once: push
+        // prefiltered candidates into queue A, run stage A on a full (or the
+        // last) batch, then stage B on a full (or the last) batch.  Both
+        // queues hold fewer than 32 items at the top of the loop, so neither
+        // exceeds 63.  This warp takes every kSplitWarps-th candidate of the
+        // transmitter, counted across depths.
+        int d = 1, c = 0, cnt = 0, global_c = 0;
+        long long base = 0;
+        auto enter_depth = [&]() __attribute__((always_inline)) {
+            while (d <= p.max_depth) {
+                cnt = p.chain_count[t * kMaxDepth + (d - 1)];
+                base = p.chain_offset[t * kMaxDepth + (d - 1)];
+                c = (warp - global_c % kSplitWarps + kSplitWarps) % kSplitWarps;
+                global_c += cnt;
+                if (c < cnt) return;
+                ++d;
+            }
+        };
+        enter_depth();
+        while (true) {
+            if (d <= p.max_depth) {
                 bool pass = active;
-                if (sizeof(T) == 4 && pass) {
-                    pass = back_project_prefilter(sc, Rf, p.chain_pre + (base + c) * 2);
-                }
+                if (sizeof(T) == 4 && pass) pass = back_project_prefilter(sc, Rf, p.chain_pre + (base + c) * 2);
                 qa = queue_push(sh->qa, qa, pass, lane, c, d);
-                if (qa >= 32) {
-                    process_a(32);
-                    qa = queue_pop(sh->qa, qa, 32, lane);
+                c += kSplitWarps;
+                if (c >= cnt) {
+                    ++d;
+                    enter_depth();
                 }
             }
-        }
-        if (qa > 0) {
-            process_a(qa);
-            qa = 0;
-        }
-        if (qb > 0) {
-            process_b(qb);
-            qb = 0;
+            const bool a_drained = d > p.max_depth;
+            if (qa >= 32 || (a_drained && qa > 0)) {
+                const int n = qa < 32 ? qa : 32;
+                process_a(n);
+                qa = queue_pop(sh->qa, qa, n, lane);
+            }
+            const bool b_drained = a_drained && qa == 0;
+            if (qb >= 32 || (b_drained && qb > 0)) {
+                const int n = qb < 32 ? qb : 32;
+                process_b(n);
+                pop_b(n);
+            }
+            if (b_drained && qb == 0) break;
         }
         // fixed-order reduction of the warps' partial sums, one write per cell
         for (int f = 0; f < NF; ++f) {
@@ -527,7 +546,7 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_diffract(MainParams p, int s
     const int* list = p.edge_list + (long long)t * sc.num_edges;
 
     // UTD fields for 32 visible items
-    auto process_v = [&](int n) {
+    auto process_v = [&](int n) __attribute__((always_inline)) {
         int it_lane = 0, j = 0;
         if (lane < n) {
             it_lane = sh->qv[3 * lane];
@@ -590,7 +609,10 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_diffract(MainParams p, int s
         __syncwarp();
     };
 
-    for (int j = warp; j < cnt; j += kSplitWarps) {
+    // one loop drives visibility and the UTD stage so each is inlined once
+    int j = warp;
+    while (true) {
+      if (j < cnt) {
         bool vis = false;
         if (active) {
             // visibility of the biased, clamped stationary point
@@ -618,14 +640,15 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_diffract(MainParams p, int s
             }
         }
         qv = queue_push(sh->qv, qv, vis, lane, j, 0);
-        if (qv >= 32) {
-            process_v(32);
-            qv = queue_pop(sh->qv, qv, 32, lane);
-        }
-    }
-    if (qv > 0) {
-        process_v(qv);
-        qv = 0;
+        j += kSplitWarps;
+      }
+      const bool drained = j >= cnt;
+      if (qv >= 32 || (drained && qv > 0)) {
+          const int n = qv < 32 ? qv : 32;
+          process_v(n);
+          qv = queue_pop(sh->qv, qv, n, lane);
+      }
+      if (drained && qv == 0) break;
     }
     // fixed-order reduction of the warps' partial sums, one write per cell
     for (int f = 0; f < NF; ++f) {

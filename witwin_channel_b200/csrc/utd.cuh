@@ -308,7 +308,7 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
     slab_fresnel(s_sin(npi - phi), mn, frequency, wavelength, &rn_te, &rn_tm);
     const T bm = phi - phi_p;
     const T bp = phi + phi_p;
-    auto mended = [&](T beta, int sgn, bool incident_group) -> Cx<T> {
+    auto mended = [&](T beta, int sgn, bool incident_group) __attribute__((always_inline)) -> Cx<T> {
         const Cx<T> value = kp_term(beta, nn, kl, sgn);
         T b_star;
         if (incident_group) {
