@@ -257,10 +257,17 @@ def run_native(args) -> None:
         peaks = _peaks()
         hbm = float(peaks.get("hbm_gbs", HBM_FALLBACK))
         cells_n = ep.num_tx * ep.num_rx
-        # dominant per-cell kernel: its rays and the slot bytes it writes per cell
-        dominant = max(("k_reflect", "k_diffract", "k_los_trans"), key=lambda k: kernel_ms.get(k, 0.0))
-        cell_bytes = {"k_reflect": 12, "k_diffract": 16, "k_los_trans": 12}[dominant]
-        bytes_per_launch = kernel_rays.get(dominant, 0) / args.steps * _bytes_per_ray(faces) + cells_n * cell_bytes
+        # dominant per-cell kernel: its rays and the bytes it writes per cell (slot
+        # values; for diffraction one visibility bit per kept edge, written by the
+        # visibility kernel and read by the UTD kernel)
+        edges_kept = float(last_prof.get("edges") or 0)
+        kinds = ("k_reflect", "k_diffract_vis", "k_diffract_utd", "k_los_trans")
+        dominant = max(kinds, key=lambda k: kernel_ms.get(k, 0.0))
+        cell_bytes = {"k_reflect": 12, "k_diffract_vis": edges_kept / 8, "k_diffract_utd": 16 + edges_kept / 8,
+                      "k_los_trans": 12}[dominant]
+        rays_of = {"k_reflect": "k_reflect", "k_diffract_vis": "k_diffract", "k_los_trans": "k_los_trans"}
+        dom_rays = kernel_rays.get(rays_of.get(dominant, ""), 0)
+        bytes_per_launch = dom_rays / args.steps * _bytes_per_ray(faces) + cells_n * cell_bytes
         launch_ms = kernel_ms.get(dominant, 0.0) / args.steps
         achieved = bytes_per_launch / (launch_ms / 1000.0) / 1e9 if launch_ms > 0 else 0.0
         traffic = _traffic_per_launch(dominant)

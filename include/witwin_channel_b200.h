@@ -332,8 +332,10 @@ int wcb_field_project_complex3(int64_t n, const float* field_vector, const float
  * launches, values[4] preparation rays (discovery bounces, edge prefilter),
  * values[5..8] ms of the LoS+transmission, reflection, diffraction and
  * finalize kernels, values[9..11] rays of the first three, values[12..16]
- * reflection candidates per depth and values[17] prefiltered diffraction
- * edges (both for the first transmitter).  `values` holds 18 doubles. */
+ * reflection candidates per depth, values[17] prefiltered diffraction
+ * edges (both for the first transmitter) and values[18] the ms of the
+ * diffraction visibility kernel (part of values[7]).  `values` holds 19
+ * doubles. */
 int wcb_profile_enable(int32_t enabled);
 int wcb_profile_read(double* values);
 

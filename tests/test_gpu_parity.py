@@ -216,3 +216,49 @@ def test_compiled_scene_is_cached_and_invalidated():
     with _t.no_grad():
         scene.structures[0].vertices.add_(0.0)  # bumps the tensor version: geometry may have changed
     assert compile_scene(scene, dev) is not a
+
+
+def _cell_maps(scene, freqs, comps):
+    from witwin_channel_b200 import engine
+    from witwin_channel_b200.compiler import compile_scene
+    from witwin_channel_b200.deterministic import _endpoints
+
+    device = torch.device("cuda", torch.cuda.current_device())
+    compiled = compile_scene(scene, device)
+    ep = _endpoints(scene, device)
+    mats = compiled.material_tables(list(freqs), device)
+    cells = engine.alloc_cells(len(freqs), ep.num_tx, ep.num_rx, device)
+    engine.run_solve(compiled, ep, mats, list(freqs), components=engine.component_bits(comps), max_depth=1,
+                     coherent=True, cells=cells)
+    return cells
+
+
+def test_diffraction_edge_chunks_match_one_chunk(monkeypatch):
+    """The diffraction kernels split a long edge list into chunks whose
+    visibility words fit a fixed budget; a tiny budget (32-edge chunks, with
+    running sums carried between chunks) gives the same rows and, up to FP32
+    summation order, the same maps as one chunk, also over two frequency
+    blocks (5 frequencies)."""
+    scene, freq = scenes.small_city(n_boxes=8, seed=11, grid=(12, 10))
+    comps = {"los", "diffraction"}
+    cfg = Config(components=comps, max_depth=1, export_paths=True, coherent=True)
+    freqs = (3.5e9, 6.0e9, 12.0e9, 20.0e9, 28.0e9)
+    one = solve(scene, cfg, reference_frequency_hz=freq)
+    one_c = _cell_maps(scene, freqs, comps)
+    monkeypatch.setenv("WCB_DIFFRACTION_CHUNK_WORDS", "1")
+    many = solve(scene, cfg, reference_frequency_hz=freq)
+    many_c = _cell_maps(scene, freqs, comps)
+    assert int((one.paths.component_id == 2).sum()) > 32
+    ka = _rows_key(one.paths.tx_id.cpu(), one.paths.rx_id.cpu(), one.paths.component_id.cpu(), one.paths.depth.cpu(),
+                   one.paths.primitive_sequence.cpu(), one.paths.edge_id.cpu())
+    kb = _rows_key(many.paths.tx_id.cpu(), many.paths.rx_id.cpu(), many.paths.component_id.cpu(),
+                   many.paths.depth.cpu(), many.paths.primitive_sequence.cpu(), many.paths.edge_id.cpu())
+    assert ka == kb
+    pairs = ((one.component_power["diffraction"], many.component_power["diffraction"]),
+             (one.path_gain, many.path_gain), (one_c.comp_power[2], many_c.comp_power[2]),
+             (one_c.diff_vec_power, many_c.diff_vec_power), (one_c.path_gain, many_c.path_gain))
+    for a, b in pairs:
+        a = a.double().cpu()
+        b = b.double().cpu()
+        assert float(a.abs().max()) > 0
+        assert torch.all((a - b).abs() <= 1e-5 * a.abs() + 1e-6 * float(a.abs().max()))

@@ -277,11 +277,12 @@ def profile_enable(enabled: bool) -> None:
 
 
 def profile_read() -> dict:
-    vals = (ctypes.c_double * 18)()
+    vals = (ctypes.c_double * 19)()
     check(load().wcb_profile_read(vals), "wcb_profile_read")
     return {"main_ms": vals[0], "prep_ms": vals[1], "rays": int(vals[2]), "main_launches": int(vals[3]),
             "prep_rays": int(vals[4]),
-            "kernel_ms": {"k_los_trans": vals[5], "k_reflect": vals[6], "k_diffract": vals[7], "k_finalize": vals[8]},
+            "kernel_ms": {"k_los_trans": vals[5], "k_reflect": vals[6], "k_diffract": vals[7], "k_finalize": vals[8],
+                          "k_diffract_vis": vals[18], "k_diffract_utd": vals[7] - vals[18]},
             "kernel_rays": {"k_los_trans": int(vals[9]), "k_reflect": int(vals[10]), "k_diffract": int(vals[11])},
             "chains": [int(v) for v in vals[12:17]], "edges": int(vals[17])}
 

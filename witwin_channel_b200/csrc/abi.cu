@@ -190,6 +190,7 @@ int wcb_profile_read(double* values) {
     for (int i = 0; i < 3; ++i) values[9 + i] = double(st.kernel_rays[i]);
     for (int i = 0; i < 5; ++i) values[12 + i] = double(st.chains[i]);
     values[17] = double(st.edges);
+    values[18] = st.diffract_vis_ms;
     return WCB_OK;
 }
 

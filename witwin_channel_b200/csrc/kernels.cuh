@@ -508,14 +508,24 @@ struct DiffShared {
     int owner[32];
 };
 
-template <typename T, int NF>
-__global__ void __launch_bounds__(kSplitBlock, 2) k_diffract(MainParams p, int stack_depth) {
+// Diffraction runs as two kernels per chunk of the transmitter's edge list:
+// k_diffract_vis traces the two biased segments of every (cell, edge) pair and
+// stores one 32-bit visibility word per (tile, edge); k_diffract_utd
+// evaluates the UTD field of the visible pairs.  Apart, the traversal kernel
+// runs at twice the occupancy of the field kernel and neither competes with
+// the other for instruction cache.
+
+// Visibility words of edges [j0, j0 + chunk) of each tile's transmitter: bit
+// `lane` of word (tile, j - j0) is set when both Tx -> Q and Q -> Rx are clear
+// for that lane's cell, Q the clamped stationary point on the edge moved by
+// kDiffractionRayBias along its exterior bisector.
+template <typename T>
+__global__ void __launch_bounds__(kSplitBlock, 4) k_diffract_vis(MainParams p, int stack_depth, int j0, int chunk,
+                                                                 unsigned* vis_words) {
     extern __shared__ int smem[];
     int* stack = smem;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    DiffShared<NF>* sh = reinterpret_cast<DiffShared<NF>*>(smem + stack_depth * kSplitBlock) + warp;
-    float* red = reinterpret_cast<float*>(reinterpret_cast<DiffShared<NF>*>(smem + stack_depth * kSplitBlock) + kSplitWarps);
     const long long tile = blockIdx.x;
     int t = 0, r = 0;
     const bool active = tile_cell(p, tile, lane, &t, &r);
@@ -525,8 +535,75 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_diffract(MainParams p, int s
     t = tw;
     const SceneDev& sc = p.sc;
     int* err = p.status;
+    const int cnt = ((p.components & 4) && p.max_depth >= 1) ? p.edge_count[t] : 0;
+    const int jend = cnt < j0 + chunk ? cnt : j0 + chunk;
+    if (j0 >= jend) return;
+    const int* list = p.edge_list + (long long)t * sc.num_edges;
     const V3<double> S = v3<double>(p.tx_pos[3 * t], p.tx_pos[3 * t + 1], p.tx_pos[3 * t + 2]);
     const V3<T> ST = cast3<T>(S);
+    const V3<float> Rf = active ? rx_point(p, r) : v3(0.f, 0.f, 0.f);
+    const V3<double> R = cast3<double>(Rf);
+    unsigned long long rays = 0;
+    for (int j = j0 + warp; j < jend; j += kSplitWarps) {
+        bool vis = false;
+        if (active) {
+            const EdgeDev& ed = sc.edges[list[j]];
+            const V3<double> c = v3(ed.pos[0], ed.pos[1], ed.pos[2]);
+            const V3<double> e = v3(ed.dir[0], ed.dir[1], ed.dir[2]);
+            const V3<double> ds = S - c;
+            const double ts = dot(ds, e);
+            const double rs = length(ds - e * ts);
+            const V3<double> dr = R - c;
+            const double tr = dot(dr, e);
+            const double rr = length(dr - e * tr);
+            const double t_star = (rs + rr) > 0.0 ? ts + (tr - ts) * rs / (rs + rr) : ts;
+            const double tc = fmin(fmax(t_star, -ed.half_length), ed.half_length);
+            const V3<double> qv_pt = c + e * tc + v3(ed.bisector[0], ed.bisector[1], ed.bisector[2]) * kDiffractionRayBias;
+            Ignore ig = ignore_none();
+            ig.f0 = ed.face0;
+            ig.f1 = ed.face1;
+            ++rays;
+            vis = !segment_blocked<T>(sc, ST, cast3<T>(qv_pt), ig, stack, err);
+            if (vis) {
+                ++rays;
+                vis = !segment_blocked<T>(sc, cast3<T>(qv_pt), cast3<T>(R), ig, stack, err);
+            }
+        }
+        const unsigned word = __ballot_sync(kFull, vis);
+        if (lane == 0) vis_words[tile * chunk + (j - j0)] = word;
+    }
+    if (p.ray_counter && p.freq_base == 0 && rays) atomicAdd(p.ray_counter, rays);
+}
+
+// UTD fields of the visible pairs of edges [j0, j0 + chunk).  Each warp takes
+// every kSplitWarps-th edge, queues its visible cells and evaluates full
+// batches of 32; per-cell sums are reduced over the warps in a fixed order.
+// With more than one chunk the running sums (9 values per cell and
+// frequency) pass between chunks through `carry`; the chunk that reaches the
+// end of the transmitter's edge list writes the outputs.  Chunk 0 always
+// runs, so a transmitter without visible edges still gets its zeros.
+template <typename T, int NF>
+__global__ void __launch_bounds__(kSplitBlock, 2) k_diffract_utd(MainParams p, int j0, int chunk,
+                                                                 const unsigned* vis_words, T* carry) {
+    extern __shared__ int smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    DiffShared<NF>* sh = reinterpret_cast<DiffShared<NF>*>(smem) + warp;
+    float* red = reinterpret_cast<float*>(reinterpret_cast<DiffShared<NF>*>(smem) + kSplitWarps);
+    const long long tile = blockIdx.x;
+    int t = 0, r = 0;
+    const bool active = tile_cell(p, tile, lane, &t, &r);
+    const long long per_tx = tiles_per_tx(p);
+    const int tw = int(tile / per_tx);
+    if (tw >= p.num_tx) return;
+    t = tw;
+    const SceneDev& sc = p.sc;
+    const int cnt = ((p.components & 4) && p.max_depth >= 1) ? p.edge_count[t] : 0;
+    if (j0 > 0 && j0 >= cnt) return;
+    const int jend = cnt < j0 + chunk ? cnt : j0 + chunk;
+    const bool first = j0 == 0;
+    const bool last = j0 + chunk >= cnt;
+    const V3<double> S = v3<double>(p.tx_pos[3 * t], p.tx_pos[3 * t + 1], p.tx_pos[3 * t + 2]);
     const V3<T> tx_pol = v3<T>(T(p.tx_pol[3 * t]), T(p.tx_pol[3 * t + 1]), T(p.tx_pol[3 * t + 2]));
     const V3<float> Rf = active ? rx_point(p, r) : v3(0.f, 0.f, 0.f);
     const float* rp = p.rx_pol + (long long)(active ? r : 0) * p.rx_pol_stride;
@@ -540,12 +617,10 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_diffract(MainParams p, int s
         gain[f] = T(0);
         for (int k = 0; k < 3; ++k) dv[f][k] = cx(T(0), T(0));
     }
-    unsigned long long rays = 0;
     int qv = 0;
-    const int cnt = ((p.components & 4) && p.max_depth >= 1) ? p.edge_count[t] : 0;
     const int* list = p.edge_list + (long long)t * sc.num_edges;
 
-    // UTD fields for 32 visible items
+    // UTD fields for up to 32 visible items
     auto process_v = [&](int n) __attribute__((always_inline)) {
         int it_lane = 0, j = 0;
         if (lane < n) {
@@ -609,46 +684,21 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_diffract(MainParams p, int s
         __syncwarp();
     };
 
-    // one loop drives visibility and the UTD stage so each is inlined once
-    int j = warp;
+    // one loop drives the queue so the UTD stage is inlined once
+    int j = j0 + warp;
     while (true) {
-      if (j < cnt) {
-        bool vis = false;
-        if (active) {
-            // visibility of the biased, clamped stationary point
-            const EdgeDev& ed = sc.edges[list[j]];
-            const V3<double> c = v3(ed.pos[0], ed.pos[1], ed.pos[2]);
-            const V3<double> e = v3(ed.dir[0], ed.dir[1], ed.dir[2]);
-            const V3<double> R = cast3<double>(Rf);
-            const V3<double> ds = S - c;
-            const double ts = dot(ds, e);
-            const double rs = length(ds - e * ts);
-            const V3<double> dr = R - c;
-            const double tr = dot(dr, e);
-            const double rr = length(dr - e * tr);
-            const double t_star = (rs + rr) > 0.0 ? ts + (tr - ts) * rs / (rs + rr) : ts;
-            const double tc = fmin(fmax(t_star, -ed.half_length), ed.half_length);
-            const V3<double> qv_pt = c + e * tc + v3(ed.bisector[0], ed.bisector[1], ed.bisector[2]) * kDiffractionRayBias;
-            Ignore ig = ignore_none();
-            ig.f0 = ed.face0;
-            ig.f1 = ed.face1;
-            ++rays;
-            vis = !segment_blocked<T>(sc, ST, cast3<T>(qv_pt), ig, stack, err);
-            if (vis) {
-                ++rays;
-                vis = !segment_blocked<T>(sc, cast3<T>(qv_pt), cast3<T>(R), ig, stack, err);
-            }
+        if (j < jend) {
+            const unsigned word = vis_words[tile * chunk + (j - j0)];
+            qv = queue_push(sh->qv, qv, (word >> lane) & 1u, lane, j, 0);
+            j += kSplitWarps;
         }
-        qv = queue_push(sh->qv, qv, vis, lane, j, 0);
-        j += kSplitWarps;
-      }
-      const bool drained = j >= cnt;
-      if (qv >= 32 || (drained && qv > 0)) {
-          const int n = qv < 32 ? qv : 32;
-          process_v(n);
-          qv = queue_pop(sh->qv, qv, n, lane);
-      }
-      if (drained && qv == 0) break;
+        const bool drained = j >= jend;
+        if (qv >= 32 || (drained && qv > 0)) {
+            const int n = qv < 32 ? qv : 32;
+            process_v(n);
+            qv = queue_pop(sh->qv, qv, n, lane);
+        }
+        if (drained && qv == 0) break;
     }
     // fixed-order reduction of the warps' partial sums, one write per cell
     for (int f = 0; f < NF; ++f) {
@@ -669,18 +719,33 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_diffract(MainParams p, int s
             Cx<T> sum = cx(T(0), T(0));
             T g = T(0);
             Cx<T> v[3] = {cx(T(0), T(0)), cx(T(0), T(0)), cx(T(0), T(0))};
+            T* cr = carry ? carry + ((long long)f * cells + cell) * 9 : nullptr;
+            if (!first && cr) {
+                sum = cx(cr[0], cr[1]);
+                g = cr[2];
+                for (int k = 0; k < 3; ++k) v[k] = cx(cr[3 + 2 * k], cr[4 + 2 * k]);
+            }
             for (int w = 0; w < kSplitWarps; ++w) {
                 const float* o = red + ((w * 32 + lane) * NF + f) * 9;
                 sum = sum + cx(T(o[0]), T(o[1]));
                 g = g + T(o[2]);
                 for (int k = 0; k < 3; ++k) v[k] = v[k] + cx(T(o[3 + 2 * k]), T(o[4 + 2 * k]));
             }
-            store_slot(p, 2, f, cell, sum, g, p.coherent);
-            T* dvp = static_cast<T*>(p.out_diff_vec_power);
-            if (dvp) dvp[(long long)(p.freq_base + f) * cells + cell] = cabs2(v[0]) + cabs2(v[1]) + cabs2(v[2]);
+            if (last) {
+                store_slot(p, 2, f, cell, sum, g, p.coherent);
+                T* dvp = static_cast<T*>(p.out_diff_vec_power);
+                if (dvp) dvp[(long long)(p.freq_base + f) * cells + cell] = cabs2(v[0]) + cabs2(v[1]) + cabs2(v[2]);
+            } else if (cr) {
+                cr[0] = sum.re;
+                cr[1] = sum.im;
+                cr[2] = g;
+                for (int k = 0; k < 3; ++k) {
+                    cr[3 + 2 * k] = v[k].re;
+                    cr[4 + 2 * k] = v[k].im;
+                }
+            }
         }
     }
-    if (p.ray_counter && p.freq_base == 0 && rays) atomicAdd(p.ray_counter, rays);
 }
 
 // ------------------------------------------------------------------ totals

@@ -17,8 +17,10 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "em.cuh"
@@ -256,14 +258,54 @@ __global__ void k_to_double(long long n, const float* in, double* out) {
 struct ComponentEvents {
     cudaEvent_t start[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t end[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> vis;  // around each diffraction visibility launch
 };
+
+// Diffraction edge chunking: the visibility words of one chunk take at most
+// kVisWordBudget 32-bit words (64 MiB), one word per (tile, edge).  The
+// environment variable WCB_DIFFRACTION_CHUNK_WORDS lowers the budget (tests
+// use it to run the multi-chunk path on small scenes).
+constexpr long long kVisWordBudget = 16ll << 20;
+
+static long long vis_word_budget() {
+    const char* v = std::getenv("WCB_DIFFRACTION_CHUNK_WORDS");
+    if (v != nullptr) {
+        const long long n = std::atoll(v);
+        if (n > 0 && n < kVisWordBudget) return n;
+    }
+    return kVisWordBudget;
+}
+
+struct DiffractionPlan {
+    int chunk = 0;           // edges per chunk
+    int chunks = 0;          // chunks covering the scene's edge count
+    unsigned* words = nullptr;
+    void* carry = nullptr;   // running per-cell sums between chunks (chunks > 1)
+    bool run_vis = true;     // false when this frequency block reuses the words
+};
+
+static long long host_tiles_per_tx(const wcb_solve_desc& d) {
+    if (d.rx_kind == 1) return (long long)((d.grid_rows + 7) / 8) * ((d.grid_cols + 3) / 4);
+    return (d.num_rx + 31) / 32;
+}
+
+static DiffractionPlan diffraction_plan(const SceneDev& sc, const wcb_solve_desc& d) {
+    DiffractionPlan dp;
+    const long long tiles = host_tiles_per_tx(d) * d.num_tx;
+    if (!(d.components & 4) || sc.num_edges <= 0 || tiles <= 0 || d.max_depth < 1) return dp;
+    long long chunk = std::max(32ll, vis_word_budget() / tiles);
+    chunk = std::min<long long>(chunk, sc.num_edges);
+    dp.chunk = int(chunk);
+    dp.chunks = int((sc.num_edges + chunk - 1) / chunk);
+    return dp;
+}
 
 // LoS+transmission and diffraction go on `stream`, reflection on `side` (its
 // candidate tables were built there); the caller joins the streams before
 // the finalize kernel.
 template <typename T, int NF>
 void launch_nf(const MainParams& q0, unsigned blocks, int sdepth, size_t stack_bytes, cudaStream_t stream,
-               cudaStream_t side, ComponentEvents* evs) {
+               cudaStream_t side, ComponentEvents* evs, const DiffractionPlan& dp) {
     const unsigned tiles = unsigned(tiles_per_tx(q0) * q0.num_tx);
     const size_t split_stack = size_t(sdepth) * kSplitBlock * 4;
     const int c = q0.components;
@@ -290,28 +332,47 @@ void launch_nf(const MainParams& q0, unsigned blocks, int sdepth, size_t stack_b
     }
     if (evs) cudaEventRecord(evs->end[0], stream);
     if (evs) cudaEventRecord(evs->start[2], stream);
-    if (c & 4) {
+    if ((c & 4) && dp.chunks > 0) {
         q.ray_counter = rc ? rc + 2 : nullptr;
-        const size_t bytes = split_stack + kSplitWarps * sizeof(DiffShared<NF>) + size_t(kSplitWarps) * 32 * NF * 9 * 4;
+        const size_t bytes = kSplitWarps * sizeof(DiffShared<NF>) + size_t(kSplitWarps) * 32 * NF * 9 * 4;
         static bool attr = false;
         if (!attr) {
-            cudaFuncSetAttribute(k_diffract<T, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaFuncSetAttribute(k_diffract_vis<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaFuncSetAttribute(k_diffract_utd<T, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             attr = true;
         }
-        k_diffract<T, NF><<<tiles, kSplitBlock, bytes, stream>>>(q, sdepth);
-        note_launch();
+        for (int k = 0; k < dp.chunks; ++k) {
+            const int j0 = k * dp.chunk;
+            if (dp.run_vis) {
+                std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+                if (evs) {
+                    cudaEventCreate(&ev.first);
+                    cudaEventCreate(&ev.second);
+                    cudaEventRecord(ev.first, stream);
+                }
+                k_diffract_vis<T><<<tiles, kSplitBlock, split_stack, stream>>>(q, sdepth, j0, dp.chunk, dp.words);
+                note_launch();
+                if (evs) {
+                    cudaEventRecord(ev.second, stream);
+                    evs->vis.push_back(ev);
+                }
+            }
+            k_diffract_utd<T, NF><<<tiles, kSplitBlock, bytes, stream>>>(q, j0, dp.chunk, dp.words,
+                                                                        static_cast<T*>(dp.carry));
+            note_launch();
+        }
     }
     if (evs) cudaEventRecord(evs->end[2], stream);
 }
 
 template <typename T>
 void launch_components(const MainParams& q, int nf, unsigned blocks, int sdepth, size_t stack_bytes, cudaStream_t stream,
-                       cudaStream_t side, ComponentEvents* evs) {
+                       cudaStream_t side, ComponentEvents* evs, const DiffractionPlan& dp) {
     switch (nf) {
-        case 1: launch_nf<T, 1>(q, blocks, sdepth, stack_bytes, stream, side, evs); break;
-        case 2: launch_nf<T, 2>(q, blocks, sdepth, stack_bytes, stream, side, evs); break;
-        case 3: launch_nf<T, 3>(q, blocks, sdepth, stack_bytes, stream, side, evs); break;
-        default: launch_nf<T, 4>(q, blocks, sdepth, stack_bytes, stream, side, evs); break;
+        case 1: launch_nf<T, 1>(q, blocks, sdepth, stack_bytes, stream, side, evs, dp); break;
+        case 2: launch_nf<T, 2>(q, blocks, sdepth, stack_bytes, stream, side, evs, dp); break;
+        case 3: launch_nf<T, 3>(q, blocks, sdepth, stack_bytes, stream, side, evs, dp); break;
+        default: launch_nf<T, 4>(q, blocks, sdepth, stack_bytes, stream, side, evs, dp); break;
     }
 }
 
@@ -383,6 +444,7 @@ struct WorkspaceLayout {
         disc_temp;
     size_t disc_temp_bytes;
     size_t edge_flags, edge_list, edge_count;
+    size_t diff_words, diff_carry;
     size_t overflow;
     size_t layers64;
     size_t total;
@@ -428,6 +490,11 @@ static WorkspaceLayout layout_for(const SceneDev& sc, const wcb_solve_desc& d, c
     L.edge_flags = take(size_t(std::max(sc.num_edges, 1)) * 4);
     L.edge_list = take(size_t(T) * std::max(sc.num_edges, 1) * 4);
     L.edge_count = take(size_t(T) * 4);
+    const DiffractionPlan dp = diffraction_plan(sc, d);
+    const long long tiles = host_tiles_per_tx(d) * T;
+    L.diff_words = take(dp.chunks > 0 ? size_t(tiles) * dp.chunk * 4 : 0);
+    const long long cells = (long long)T * (d.rx_kind == 1 ? (long long)d.grid_rows * d.grid_cols : d.num_rx);
+    L.diff_carry = take(dp.chunks > 1 ? size_t(cells) * kMaxNF * 9 * 8 : 0);
     L.overflow = take(64);
     L.layers64 = 0;
     L.total = o;
@@ -680,6 +747,10 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     if (prof.enabled) cudaEventRecord(ev_main0, stream);
     ComponentEvents cev;
     double comp_ms[4] = {0, 0, 0, 0};
+    double vis_ms = 0.0;
+    DiffractionPlan dplan = diffraction_plan(sc, *d);
+    dplan.words = reinterpret_cast<unsigned*>(base + L.diff_words);
+    dplan.carry = dplan.chunks > 1 ? static_cast<void*>(base + L.diff_carry) : nullptr;
     if (prof.enabled)
         for (int i = 0; i < 4; ++i) {
             cudaEventCreate(&cev.start[i]);
@@ -714,8 +785,10 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         if (fb > 0) q.rows = nullptr;  // geometry rows are emitted once
         if (blocks <= 0) continue;
         ComponentEvents* evp = prof.enabled ? &cev : nullptr;
-        if (fp64) launch_components<double>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream, side, evp);
-        else launch_components<float>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream, side, evp);
+        // a single edge chunk keeps its visibility words for every frequency block
+        dplan.run_vis = fb == 0 || dplan.chunks > 1;
+        if (fp64) launch_components<double>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream, side, evp, dplan);
+        else launch_components<float>(q, nf, unsigned(blocks), sdepth, stack_bytes, stream, side, evp, dplan);
         if (side != stream) {
             cudaEventRecord(join, side);
             cudaStreamWaitEvent(stream, join, 0);
@@ -734,6 +807,14 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                 cudaEventElapsedTime(&ms, cev.start[i], cev.end[i]);
                 comp_ms[i] += ms;
             }
+            for (auto& ev : cev.vis) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev.first, ev.second);
+                vis_ms += ms;
+                cudaEventDestroy(ev.first);
+                cudaEventDestroy(ev.second);
+            }
+            cev.vis.clear();
         }
     }
     if (prof.enabled) {
@@ -755,6 +836,7 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         prof.rays = (long long)(nr[1] + nr[2] + nr[3]);
         for (int i = 0; i < 3; ++i) prof.kernel_rays[i] = (long long)nr[1 + i];
         for (int i = 0; i < 4; ++i) prof.kernel_ms[i] = comp_ms[i];
+        prof.diffract_vis_ms = vis_ms;
         for (int i = 0; i < kMaxDepth; ++i) prof.chains[i] = cc[i];
         prof.edges = ec;
         for (int i = 0; i < 4; ++i) {

@@ -96,6 +96,7 @@ struct ProfileState {
     long long prep_rays = 0;     // rays traced while preparing candidates (discovery, edge prefilter)
     long long main_launches = 0;
     double kernel_ms[4] = {0, 0, 0, 0};       // los+transmission, reflection, diffraction, finalize
+    double diffract_vis_ms = 0.0;             // the visibility part of the diffraction time
     long long kernel_rays[3] = {0, 0, 0};     // los+transmission, reflection, diffraction
     long long chains[5] = {0, 0, 0, 0, 0};    // reflection candidates per depth (first transmitter)
     long long edges = 0;                      // diffraction edges kept by the prefilter (first transmitter)
