@@ -96,7 +96,10 @@ __global__ void __launch_bounds__(kBlock) k_discovery_trace(SceneDev sc, int cou
 }
 
 // key for unique chains at depth k: (prefix rank << 21) | group
-__global__ void k_chain_keys(int count, int depth, int k, const int* groups, const int* prefix_rank,
+// Key (prefix rank, group) packed as pr << gbits | g, gbits = bits of the
+// group count; rays without a hit at this depth get ~0 (sorted last: the sort
+// covers key_bits() low bits, above every valid key).
+__global__ void k_chain_keys(int count, int depth, int k, const int* groups, const int* prefix_rank, int gbits,
                              unsigned long long* keys, int* vals) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
@@ -104,7 +107,7 @@ __global__ void k_chain_keys(int count, int depth, int k, const int* groups, con
     const int pr = k == 0 ? 0 : prefix_rank[i];
     unsigned long long key;
     if (g < 0 || pr < 0) key = ~0ull;
-    else key = (static_cast<unsigned long long>(pr) << 21) | static_cast<unsigned long long>(g);
+    else key = (static_cast<unsigned long long>(pr) << gbits) | static_cast<unsigned long long>(g);
     keys[i] = key;
     vals[i] = i;
 }
@@ -404,6 +407,13 @@ struct ChainPlan {
     long long offset_int[kMaxDepth];
 };
 
+// bits needed to hold 0..n (n >= 0)
+static int bit_width(long long n) {
+    int b = 1;
+    while (b < 63 && (n >> b) != 0) ++b;
+    return b;
+}
+
 static long long seq_count(long long g, int d) {
     if (d > 1) {
         if (g <= 1) return 0;
@@ -593,6 +603,8 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                 else
                     k_discovery_trace<float><<<(rays + kBlock - 1) / kBlock, kBlock, smem, side>>>(sc, rays, md, dirs, txp, dg, err, prof.enabled ? ray_counter : nullptr);
                 note_launch();
+                const int gbits = bit_width(sc.num_groups);
+                const int key_bits = std::min(64, gbits + bit_width(rays) + 1);
                 unsigned long long* keys = reinterpret_cast<unsigned long long*>(base + L.disc_keys);
                 unsigned long long* keys2 = reinterpret_cast<unsigned long long*>(base + L.disc_keys2);
                 int* vals = reinterpret_cast<int*>(base + L.disc_vals);
@@ -605,9 +617,10 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                     const int depth = k + 1;
                     const bool use_disc = depth == 1 ? !pl.exhaustive_o1 : !pl.exhaustive_mb;
                     // ranks are needed for the next depth even when this depth is exhaustive
-                    k_chain_keys<<<(rays + B - 1) / B, B, 0, side>>>(rays, md, k, dg, rank, keys, vals);
+                    k_chain_keys<<<(rays + B - 1) / B, B, 0, side>>>(rays, md, k, dg, rank, gbits, keys, vals);
                     size_t tb = L.disc_temp_bytes;
-                    cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys2, vals, vals2, rays, 0, 64, side);
+                    // only the key's used bits (+1 so the ~0 of a missing hit stays above)
+                    cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys2, vals, vals2, rays, 0, key_bits, side);
                     k_chain_flags<<<(rays + B - 1) / B, B, 0, side>>>(rays, keys2, flags);
                     tb = L.disc_temp_bytes;
                     cub::DeviceScan::InclusiveSum(temp, tb, flags, scan, rays, side);
