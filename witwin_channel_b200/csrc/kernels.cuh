@@ -247,16 +247,66 @@ __global__ void __launch_bounds__(kCompBlock) k_los_trans(MainParams p) {
 
 // ------------------------------------------------------------------ reflection
 // Per-warp shared layout: queue A (3 ints/item), queue B (3 + 5 ints/item),
-// contribution buffer (32 items x NF x 3 floats).
+// queue F (3 + 5 ints/item), contribution buffer (32 items x NF x 3 floats).
 template <int NF>
 struct ReflShared {
     int qa[3 * kQueueCap];
     int qb[3 * kQueueCap];
     int qbf[kMaxDepth * kQueueCap];
+    int qf[3 * kQueueCap];
+    int qff[kMaxDepth * kQueueCap];
     float contrib[32 * NF * 3];
     int owner[32];
 };
 
+// Append the passing lanes' items (three ints plus kMaxDepth faces) to a
+// queue of `size` items; returns the new size.
+WCB_D int queue_push_faces(int* q, int* qfaces, int size, bool pass, int a, int b, int c,
+                           const int (&faces)[kMaxDepth]) {
+    const unsigned mask = __ballot_sync(kFull, pass);
+    if (pass) {
+        const int pos = size + __popc(mask & lanemask_lt());
+        q[3 * pos] = a;
+        q[3 * pos + 1] = b;
+        q[3 * pos + 2] = c;
+#pragma unroll
+        for (int k = 0; k < kMaxDepth; ++k) qfaces[kMaxDepth * pos + k] = faces[k];
+    }
+    __syncwarp();
+    return size + __popc(mask);
+}
+
+// Drop the first n items (n <= 32) of a queue with faces.
+WCB_D int queue_pop_faces(int* q, int* qfaces, int size, int n, int lane) {
+    const int rem = size - n;
+    int a0 = 0, a1 = 0, a2 = 0, fb[kMaxDepth];
+    if (lane < rem) {
+        a0 = q[3 * (n + lane)];
+        a1 = q[3 * (n + lane) + 1];
+        a2 = q[3 * (n + lane) + 2];
+#pragma unroll
+        for (int k = 0; k < kMaxDepth; ++k) fb[k] = qfaces[kMaxDepth * (n + lane) + k];
+    }
+    __syncwarp();
+    if (lane < rem) {
+        q[3 * lane] = a0;
+        q[3 * lane + 1] = a1;
+        q[3 * lane + 2] = a2;
+#pragma unroll
+        for (int k = 0; k < kMaxDepth; ++k) qfaces[kMaxDepth * lane + k] = fb[k];
+    }
+    __syncwarp();
+    return rem;
+}
+
+// Reflection in three queued stages per warp: A (FP64 back projection and
+// containment of prefiltered candidates), B (one visibility segment per item
+// and pass: an item whose segment is clear goes back to B for its next
+// segment, or to F after its last), F (Jones chain and accumulation of the
+// visible paths).  Testing one segment per pass keeps the warp's lanes on
+// the same kind of work: most candidates are blocked on their first segment
+// and leave after one traversal instead of idling while a visible path of
+// the same batch traces its remaining segments and its field.
 template <typename T, int NF>
 __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int stack_depth) {
     extern __shared__ int smem[];
@@ -286,15 +336,15 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
     T gain[NF];
     for (int f = 0; f < NF; ++f) { acc[f] = cx(T(0), T(0)); gain[f] = T(0); }
     unsigned long long rays = 0;
-    int qa = 0, qb = 0;
+    int qa = 0, qb = 0, qf = 0;
 
-    // stage B: visibility + field for 32 items (FP64 hits recomputed)
-    auto process_b = [&](int n) __attribute__((always_inline)) {
+    // stage F: field of up to 32 visible paths (FP64 hits recomputed)
+    auto process_f = [&](int n) __attribute__((always_inline)) {
         int it_lane = 0, c = 0, d = 1;
         if (lane < n) {
-            it_lane = sh->qb[3 * lane];
-            c = sh->qb[3 * lane + 1];
-            d = sh->qb[3 * lane + 2];
+            it_lane = sh->qf[3 * lane];
+            c = sh->qf[3 * lane + 1];
+            d = sh->qf[3 * lane + 2];
         }
         const float rx = __shfl_sync(kFull, Rf.x, it_lane);
         const float ry = __shfl_sync(kFull, Rf.y, it_lane);
@@ -302,59 +352,47 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
         const float px = __shfl_sync(kFull, rpol.x, it_lane);
         const float py = __shfl_sync(kFull, rpol.y, it_lane);
         const float pz = __shfl_sync(kFull, rpol.z, it_lane);
-        bool ok = lane < n;
+        const bool ok = lane < n;
         if (ok) {
             const V3<double> R = v3<double>(rx, ry, rz);
             const long long base = p.chain_offset[t * kMaxDepth + (d - 1)];
-            const int* groups = p.chain_groups + base + (long long)c * d;
             const double* planes = p.chain_planes + (base + (long long)c * d) * 4;
             const double* images = p.chain_images + (base + (long long)c * d) * 3;
             V3<double> hits[kMaxDepth];
             back_project(R, planes, images, d, hits);
             int faces[kMaxDepth];
-            for (int k = 0; k < d; ++k) faces[k] = sh->qbf[kMaxDepth * lane + k];
-            for (int s = 0; s <= d && ok; ++s) {
-                const V3<double> a = s == 0 ? S : hits[s - 1];
-                const V3<double> b = s == d ? R : hits[s];
-                Ignore ig = ignore_none();
-                ig.g0 = s > 0 ? groups[s - 1] : -1;
-                ig.g1 = s < d ? groups[s] : -1;
-                ++rays;
-                if (segment_blocked<T>(sc, cast3<T>(a), cast3<T>(b), ig, stack, err)) ok = false;
-            }
-            if (ok) {
-                const V3<double> img = v3(images[3 * (d - 1)], images[3 * (d - 1) + 1], images[3 * (d - 1) + 2]);
-                const double total = length(R - img);
-                const V3<T> RT = cast3<T>(R);
-                const V3<T> rx_pol = v3<T>(T(px), T(py), T(pz));
+            for (int k = 0; k < d; ++k) faces[k] = sh->qff[kMaxDepth * lane + k];
+            const V3<double> img = v3(images[3 * (d - 1)], images[3 * (d - 1) + 1], images[3 * (d - 1) + 2]);
+            const double total = length(R - img);
+            const V3<T> RT = cast3<T>(R);
+            const V3<T> rx_pol = v3<T>(T(px), T(py), T(pz));
 #pragma unroll 1
-                for (int f = 0; f < NF; ++f) {
-                    const double freq = p.freq[f];
-                    const T wl = T(kC0 / freq);
-                    V3<T> prev = ST;
-                    V3<T> incident = safe_normalize(cast3<T>(hits[0]) - prev, v3<T>(T(0), T(0), T(1)));
-                    C3<T> value = c3_from_real(transverse(incident, tx_pol));
-                    V3<T> outgoing = incident;
-                    for (int k = 0; k < d; ++k) {
-                        const V3<T> hit = cast3<T>(hits[k]);
-                        incident = safe_normalize(hit - prev, outgoing);
-                        const float* nf = sc.face_normal + 3 * faces[k];
-                        reflect_bounce(value, outgoing, incident, v3<T>(T(nf[0]), T(nf[1]), T(nf[2])),
-                                       face_slab<T>(p, f, faces[k]), freq, wl);
-                        prev = hit;
-                    }
-                    const V3<T> fdir = safe_normalize(RT - prev, outgoing);
-                    const T amp = T(1) / (T(2) * T(p.k[f]) * T(fmax(total, kUtdEps)));
-                    value = c3_scale(value, phasor_neg_kd<T>(p.k[f], total) * amp);
-                    const Cx<T> pf = project_receiver(value, fdir, rx_pol) * sqrt_p;
-                    sh->contrib[(lane * NF + f) * 3 + 0] = float(value_of(pf.re));
-                    sh->contrib[(lane * NF + f) * 3 + 1] = float(value_of(pf.im));
-                    sh->contrib[(lane * NF + f) * 3 + 2] = float(value_of(cabs2(pf)));
+            for (int f = 0; f < NF; ++f) {
+                const double freq = p.freq[f];
+                const T wl = T(kC0 / freq);
+                V3<T> prev = ST;
+                V3<T> incident = safe_normalize(cast3<T>(hits[0]) - prev, v3<T>(T(0), T(0), T(1)));
+                C3<T> value = c3_from_real(transverse(incident, tx_pol));
+                V3<T> outgoing = incident;
+                for (int k = 0; k < d; ++k) {
+                    const V3<T> hit = cast3<T>(hits[k]);
+                    incident = safe_normalize(hit - prev, outgoing);
+                    const float* nf = sc.face_normal + 3 * faces[k];
+                    reflect_bounce(value, outgoing, incident, v3<T>(T(nf[0]), T(nf[1]), T(nf[2])),
+                                   face_slab<T>(p, f, faces[k]), freq, wl);
+                    prev = hit;
                 }
-                int tt = 0, rr = 0;
-                tile_cell(p, tile, it_lane, &tt, &rr);
-                emit_row(p, t, rr, 1, d, faces, -1, float(total));
+                const V3<T> fdir = safe_normalize(RT - prev, outgoing);
+                const T amp = T(1) / (T(2) * T(p.k[f]) * T(fmax(total, kUtdEps)));
+                value = c3_scale(value, phasor_neg_kd<T>(p.k[f], total) * amp);
+                const Cx<T> pf = project_receiver(value, fdir, rx_pol) * sqrt_p;
+                sh->contrib[(lane * NF + f) * 3 + 0] = float(value_of(pf.re));
+                sh->contrib[(lane * NF + f) * 3 + 1] = float(value_of(pf.im));
+                sh->contrib[(lane * NF + f) * 3 + 2] = float(value_of(cabs2(pf)));
             }
+            int tt = 0, rr = 0;
+            tile_cell(p, tile, it_lane, &tt, &rr);
+            emit_row(p, t, rr, 1, d, faces, -1, float(total));
         }
         sh->owner[lane] = ok ? it_lane : -1;
         __syncwarp();
@@ -367,9 +405,48 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
             }
         }
         __syncwarp();
+        qf = queue_pop_faces(sh->qf, sh->qff, qf, n, lane);
     };
 
-    // stage A: FP64 back projection + containment for 32 items
+    // stage B: segment s of up to 32 items (the third int packs d | s << 4)
+    auto process_b = [&](int n) __attribute__((always_inline)) {
+        int it_lane = 0, c = 0, d = 1, s = 0, faces[kMaxDepth];
+        if (lane < n) {
+            it_lane = sh->qb[3 * lane];
+            c = sh->qb[3 * lane + 1];
+            const int ds = sh->qb[3 * lane + 2];
+            d = ds & 15;
+            s = ds >> 4;
+        }
+#pragma unroll
+        for (int k = 0; k < kMaxDepth; ++k) faces[k] = lane < n ? sh->qbf[kMaxDepth * lane + k] : 0;
+        const float rx = __shfl_sync(kFull, Rf.x, it_lane);
+        const float ry = __shfl_sync(kFull, Rf.y, it_lane);
+        const float rz = __shfl_sync(kFull, Rf.z, it_lane);
+        bool ok = lane < n;
+        if (ok) {
+            const V3<double> R = v3<double>(rx, ry, rz);
+            const long long base = p.chain_offset[t * kMaxDepth + (d - 1)];
+            const int* groups = p.chain_groups + base + (long long)c * d;
+            const double* planes = p.chain_planes + (base + (long long)c * d) * 4;
+            const double* images = p.chain_images + (base + (long long)c * d) * 3;
+            V3<double> hits[kMaxDepth];
+            back_project(R, planes, images, d, hits);
+            const V3<double> a = s == 0 ? S : hits[s - 1];
+            const V3<double> b = s == d ? R : hits[s];
+            Ignore ig = ignore_none();
+            ig.g0 = s > 0 ? groups[s - 1] : -1;
+            ig.g1 = s < d ? groups[s] : -1;
+            ++rays;
+            ok = !segment_blocked<T>(sc, cast3<T>(a), cast3<T>(b), ig, stack, err);
+        }
+        qb = queue_pop_faces(sh->qb, sh->qbf, qb, n, lane);
+        qb = queue_push_faces(sh->qb, sh->qbf, qb, ok && s < d, it_lane, c, d | ((s + 1) << 4), faces);
+        qf = queue_push_faces(sh->qf, sh->qff, qf, ok && s == d, it_lane, c, d, faces);
+    };
+
+    // stage A: FP64 back projection + containment for up to 32 items; the
+    // survivors enter queue B at segment 0
     auto process_a = [&](int n) __attribute__((always_inline)) {
         int it_lane = 0, c = 0, d = 1;
         if (lane < n) {
@@ -382,6 +459,8 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
         const float rz = __shfl_sync(kFull, Rf.z, it_lane);
         bool ok = lane < n;
         int faces[kMaxDepth];
+#pragma unroll
+        for (int k = 0; k < kMaxDepth; ++k) faces[k] = 0;
         if (ok) {
             const long long base = p.chain_offset[t * kMaxDepth + (d - 1)];
             const int* groups = p.chain_groups + base + (long long)c * d;
@@ -394,49 +473,18 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
                 ok = faces[k] >= 0;
             }
         }
-        // push survivors into queue B (faces stored beside the item)
-        const unsigned mask = __ballot_sync(kFull, ok);
-        if (ok) {
-            const int pos = qb + __popc(mask & lanemask_lt());
-            sh->qb[3 * pos] = it_lane;
-            sh->qb[3 * pos + 1] = c;
-            sh->qb[3 * pos + 2] = d;
-            for (int k = 0; k < d; ++k) sh->qbf[kMaxDepth * pos + k] = faces[k];
-        }
-        __syncwarp();
-        qb += __popc(mask);
-    };
-
-    // drop the first n items of queue B (items and their faces)
-    auto pop_b = [&](int n) __attribute__((always_inline)) {
-        const int rem = qb - n;
-        int a0 = 0, a1 = 0, a2 = 0, fb[kMaxDepth];
-        if (lane < rem) {
-            a0 = sh->qb[3 * (n + lane)];
-            a1 = sh->qb[3 * (n + lane) + 1];
-            a2 = sh->qb[3 * (n + lane) + 2];
-#pragma unroll
-            for (int k = 0; k < kMaxDepth; ++k) fb[k] = sh->qbf[kMaxDepth * (n + lane) + k];
-        }
-        __syncwarp();
-        if (lane < rem) {
-            sh->qb[3 * lane] = a0;
-            sh->qb[3 * lane + 1] = a1;
-            sh->qb[3 * lane + 2] = a2;
-#pragma unroll
-            for (int k = 0; k < kMaxDepth; ++k) sh->qbf[kMaxDepth * lane + k] = fb[k];
-        }
-        __syncwarp();
-        qb = rem;
+        qa = queue_pop(sh->qa, qa, n, lane);
+        qb = queue_push_faces(sh->qb, sh->qbf, qb, ok, it_lane, c, d, faces);
     };
 
     if ((p.components & 2) && sc.num_faces > 0) {
-        // One loop drives the three stages so each is inlined once: push
-        // prefiltered candidates into queue A, run stage A on a full (or the
-        // last) batch, then stage B on a full (or the last) batch.  Both
-        // queues hold fewer than 32 items at the top of the loop, so neither
-        // exceeds 63.  This warp takes every kSplitWarps-th candidate of the
-        // transmitter, counted across depths.
+        // One loop drives the stages so each is inlined once.  Each pass runs
+        // one step, full batches first and the latest stage first: F, then B,
+        // then A, then the next candidate into queue A; partial batches only
+        // once nothing upstream can fill them.  A stage runs only while the
+        // queues it feeds hold fewer than 32 items, so no queue exceeds 63.
+        // This warp takes every kSplitWarps-th candidate of the transmitter,
+        // counted across depths.
         int d = 1, c = 0, cnt = 0, global_c = 0;
         long long base = 0;
         auto enter_depth = [&]() __attribute__((always_inline)) {
@@ -451,7 +499,17 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
         };
         enter_depth();
         while (true) {
-            if (d <= p.max_depth) {
+            const bool cand_left = d <= p.max_depth;
+            int step;
+            if (qf >= 32) step = 3;
+            else if (qb >= 32) step = 2;
+            else if (qa >= 32) step = 1;
+            else if (cand_left) step = 0;
+            else if (qa > 0) step = 1;
+            else if (qb > 0) step = 2;
+            else if (qf > 0) step = 3;
+            else break;
+            if (step == 0) {
                 bool pass = active;
                 if (sizeof(T) == 4 && pass) pass = back_project_prefilter(sc, Rf, p.chain_pre + (base + c) * 2);
                 qa = queue_push(sh->qa, qa, pass, lane, c, d);
@@ -460,20 +518,13 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
                     ++d;
                     enter_depth();
                 }
+            } else if (step == 1) {
+                process_a(qa < 32 ? qa : 32);
+            } else if (step == 2) {
+                process_b(qb < 32 ? qb : 32);
+            } else {
+                process_f(qf < 32 ? qf : 32);
             }
-            const bool a_drained = d > p.max_depth;
-            if (qa >= 32 || (a_drained && qa > 0)) {
-                const int n = qa < 32 ? qa : 32;
-                process_a(n);
-                qa = queue_pop(sh->qa, qa, n, lane);
-            }
-            const bool b_drained = a_drained && qa == 0;
-            if (qb >= 32 || (b_drained && qb > 0)) {
-                const int n = qb < 32 ? qb : 32;
-                process_b(n);
-                pop_b(n);
-            }
-            if (b_drained && qb == 0) break;
         }
         // fixed-order reduction of the warps' partial sums, one write per cell
         for (int f = 0; f < NF; ++f) {
