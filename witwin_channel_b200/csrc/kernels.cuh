@@ -430,10 +430,8 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
             const int* groups = p.chain_groups + base + (long long)c * d;
             const double* planes = p.chain_planes + (base + (long long)c * d) * 4;
             const double* images = p.chain_images + (base + (long long)c * d) * 3;
-            V3<double> hits[kMaxDepth];
-            back_project(R, planes, images, d, hits);
-            const V3<double> a = s == 0 ? S : hits[s - 1];
-            const V3<double> b = s == d ? R : hits[s];
+            V3<double> a, b;
+            back_project_segment(S, R, planes, images, d, s, &a, &b);
             Ignore ig = ignore_none();
             ig.g0 = s > 0 ? groups[s - 1] : -1;
             ig.g1 = s < d ? groups[s] : -1;
@@ -466,11 +464,15 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int st
             const int* groups = p.chain_groups + base + (long long)c * d;
             const double* planes = p.chain_planes + (base + (long long)c * d) * 4;
             const double* images = p.chain_images + (base + (long long)c * d) * 3;
-            V3<double> hits[kMaxDepth];
-            ok = back_project(v3<double>(rx, ry, rz), planes, images, d, hits);
+            // hit k and its face, from the last bounce back (no hit array)
+            V3<double> x = v3<double>(rx, ry, rz);
             for (int k = d - 1; k >= 0 && ok; --k) {
-                faces[k] = resolve_in_group(sc, groups[k], hits[k]);
-                ok = faces[k] >= 0;
+                ok = back_project_step(x, planes, images, k);
+                const int f = ok ? resolve_in_group(sc, groups[k], x) : -1;
+                ok = f >= 0;
+#pragma unroll
+                for (int kk = 0; kk < kMaxDepth; ++kk)
+                    if (kk == k) faces[kk] = f;
             }
         }
         qa = queue_pop(sh->qa, qa, n, lane);
@@ -626,9 +628,11 @@ __global__ void __launch_bounds__(kSplitBlock, 4) k_diffract_vis(MainParams p, i
     if (p.ray_counter && p.freq_base == 0 && rays) atomicAdd(p.ray_counter, rays);
 }
 
-// UTD fields of the visible pairs of edges [j0, j0 + chunk).  Each warp takes
-// every kSplitWarps-th edge, queues its visible cells and evaluates full
-// batches of 32; per-cell sums are reduced over the warps in a fixed order.
+// UTD fields of the visible pairs of edges [j0, j0 + chunk).  The tile's
+// items are the set bits of its visibility words in (edge, lane) order; warp
+// w takes the contiguous w-th eighth of them, queues them and evaluates full
+// batches of 32, so the warps of a block finish together.  Per-cell sums are
+// reduced over the warps in a fixed order.
 // With more than one chunk the running sums (9 values per cell and
 // frequency) pass between chunks through `carry`; the chunk that reaches the
 // end of the transmitter's edge list writes the outputs.  Chunk 0 always
@@ -735,15 +739,51 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_diffract_utd(MainParams p, i
         __syncwarp();
     };
 
-    // one loop drives the queue so the UTD stage is inlined once
-    int j = j0 + warp;
-    while (true) {
-        if (j < jend) {
-            const unsigned word = vis_words[tile * chunk + (j - j0)];
-            qv = queue_push(sh->qv, qv, (word >> lane) & 1u, lane, j, 0);
-            j += kSplitWarps;
+    // this warp's share [lo, hi) of the tile's items
+    const unsigned* words = vis_words + tile * chunk;
+    const int nw = jend > j0 ? jend - j0 : 0;
+    int total = 0;
+    for (int b = 0; b < nw; b += 32) {
+        const int jj = b + lane;
+        total += int(__reduce_add_sync(kFull, jj < nw ? unsigned(__popc(words[jj])) : 0u));
+    }
+    const int lo = int((long long)total * warp / kSplitWarps);
+    const int hi = int((long long)total * (warp + 1) / kSplitWarps);
+    // skip, 32 words at a time, the words whose items all precede lo
+    int jj = 0, seen = 0;
+    for (; jj < nw; jj += 32) {
+        const unsigned c = jj + lane < nw ? unsigned(__popc(words[jj + lane])) : 0u;
+        const int group = int(__reduce_add_sync(kFull, c));
+        if (seen + group > lo) break;
+        seen += group;
+    }
+    if (jj < nw) {
+        // within this group of 32 words: the first word holding item lo
+        const int word_i = jj + lane;
+        const int c = word_i < nw ? __popc(words[word_i]) : 0;
+        int incl = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += v;
         }
-        const bool drained = j >= jend;
+        const unsigned past = __ballot_sync(kFull, seen + incl > lo);
+        const int first = __ffs(past) - 1;  // past != 0: the group holds item lo
+        const int before = __shfl_sync(kFull, incl - c, first);
+        jj += first;
+        seen += before;
+    }
+    // one loop walks the words and drives the queue so the UTD stage is
+    // inlined once
+    while (true) {
+        if (jj < nw && seen < hi) {
+            const unsigned word = words[jj];
+            const int idx = seen + __popc(word & lanemask_lt());
+            const bool mine = ((word >> lane) & 1u) && idx >= lo && idx < hi;
+            qv = queue_push(sh->qv, qv, mine, lane, j0 + jj, 0);
+            seen += __popc(word);
+            ++jj;
+        }
+        const bool drained = !(jj < nw && seen < hi);
         if (qv >= 32 || (drained && qv > 0)) {
             const int n = qv < 32 ? qv : 32;
             process_v(n);

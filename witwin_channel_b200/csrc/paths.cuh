@@ -52,18 +52,41 @@ WCB_D int resolve_in_group(const SceneDev& sc, int g, V3<double> p) {
 // planes[k] = (n, off); images[k] = image of the source after k+1 mirrors.
 // Writes the hit points, returns false when a back-projected line does not
 // cross its plane strictly between its ends.
+// One step: moves x to its hit on plane k along the line to image k; false
+// when that line does not cross the plane strictly between its ends.
+WCB_D bool back_project_step(V3<double>& x, const double* planes, const double* images, int k) {
+    const V3<double> n = v3(planes[4 * k], planes[4 * k + 1], planes[4 * k + 2]);
+    const double off = planes[4 * k + 3];
+    const V3<double> img = v3(images[3 * k], images[3 * k + 1], images[3 * k + 2]);
+    const double denom = dot(img - x, n);
+    if (denom == 0.0) return false;
+    const double t = (off - dot(x, n)) / denom;
+    if (!(t > kSegEps && t < 1.0 - kSegEps)) return false;
+    x = x + (img - x) * t;
+    return true;
+}
+
 WCB_D bool back_project(V3<double> R, const double* planes, const double* images, int depth, V3<double>* hits) {
     V3<double> x = R;
     for (int k = depth - 1; k >= 0; --k) {
-        const V3<double> n = v3(planes[4 * k], planes[4 * k + 1], planes[4 * k + 2]);
-        const double off = planes[4 * k + 3];
-        const V3<double> img = v3(images[3 * k], images[3 * k + 1], images[3 * k + 2]);
-        const double denom = dot(img - x, n);
-        if (denom == 0.0) return false;
-        const double t = (off - dot(x, n)) / denom;
-        if (!(t > kSegEps && t < 1.0 - kSegEps)) return false;
-        x = x + (img - x) * t;
+        if (!back_project_step(x, planes, images, k)) return false;
         hits[k] = x;
+    }
+    return true;
+}
+
+// Ends of segment s of a back-projected chain of `depth` bounces (S or hit
+// s-1, and hit s or R) with the same arithmetic as back_project and no hit
+// array; false when the back projection fails.
+WCB_D bool back_project_segment(V3<double> S, V3<double> R, const double* planes, const double* images, int depth,
+                                int s, V3<double>* a, V3<double>* b) {
+    V3<double> x = R;
+    *a = S;
+    *b = R;
+    for (int k = depth - 1; k >= 0 && k >= s - 1; --k) {
+        if (!back_project_step(x, planes, images, k)) return false;
+        if (k == s) *b = x;
+        if (k == s - 1) *a = x;
     }
     return true;
 }

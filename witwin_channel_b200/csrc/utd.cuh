@@ -291,8 +291,14 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
     const T tsT = T(t_star);
     const T tmax = T(ed.half_length), tmin = -T(ed.half_length);
     const T inv_sqrt2 = T(0.70710678118654752440);
-    const T hi_abs = fresnel_complement_abs(sigma * (tmax - tsT));
-    const T lo_abs = fresnel_complement_abs(-(sigma * (tmin - tsT)));
+    // both ends through one inlined copy of the Fresnel complement
+    T hi_abs = T(0), lo_abs = T(0);
+#pragma unroll 1
+    for (int e2 = 0; e2 < 2; ++e2) {
+        const T v = fresnel_complement_abs(e2 == 0 ? sigma * (tmax - tsT) : -(sigma * (tmin - tsT)));
+        if (e2 == 0) hi_abs = v;
+        else lo_abs = v;
+    }
     const T t_mono = s_min(s_max(T(1) - inv_sqrt2 * lo_abs - inv_sqrt2 * hi_abs, T(0)), T(1));
     T u;
     if (value_of(s_abs(tsT - tmax)) < value_of(s_abs(tsT - tmin))) u = sigma * (tsT - tmax);
@@ -303,13 +309,22 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
     const T delta_b = T(kCBlend) * unit;
     // face factors
     const T wavelength = T(G(kC0) / frequency);
-    Cx<T> r0_te, r0_tm, rn_te, rn_tm;
-    slab_fresnel(s_sin(phi_p), m0, frequency, wavelength, &r0_te, &r0_tm);
-    slab_fresnel(s_sin(npi - phi), mn, frequency, wavelength, &rn_te, &rn_tm);
+    Cx<T> r0_te, r0_tm, rn_te, rn_tm;  // faces 0 and n, through one inlined copy
+#pragma unroll 1
+    for (int face = 0; face < 2; ++face) {
+        Cx<T> te, tm;
+        slab_fresnel(s_sin(face == 0 ? phi_p : npi - phi), face == 0 ? m0 : mn, frequency, wavelength, &te, &tm);
+        if (face == 0) {
+            r0_te = te;
+            r0_tm = tm;
+        } else {
+            rn_te = te;
+            rn_tm = tm;
+        }
+    }
     const T bm = phi - phi_p;
     const T bp = phi + phi_p;
     auto mended = [&](T beta, int sgn, bool incident_group) __attribute__((always_inline)) -> Cx<T> {
-        const Cx<T> value = kp_term(beta, nn, kl, sgn);
         T b_star;
         if (incident_group) {
             b_star = value_of(s_abs(beta - T(kPi))) <= value_of(s_abs(beta + T(kPi))) ? T(kPi) : T(-kPi);
@@ -321,8 +336,17 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
         const T rw = delta / delta_w;
         T w = s_exp(-rw * rw);
         if (value_of(w) <= kWindowCutoff) w = T(0);
-        // the odd part vanishes outside the locality window: skip the mirror
-        const Cx<T> mirrored = value_of(w) > 0 ? kp_term(T(2) * b_star - beta, nn, kl, sgn) : value;
+        // the term and, inside the locality window, its mirror through one
+        // inlined copy of kp_term; outside the window the odd part vanishes
+        Cx<T> value = cx(T(0), T(0)), mirrored = cx(T(0), T(0));
+        const int nterms = value_of(w) > 0 ? 2 : 1;
+#pragma unroll 1
+        for (int m = 0; m < nterms; ++m) {
+            const Cx<T> v = kp_term(m == 0 ? beta : T(2) * b_star - beta, nn, kl, sgn);
+            if (m == 0) value = v;
+            else mirrored = v;
+        }
+        if (nterms == 1) mirrored = value;
         const Cx<T> odd = (value - mirrored) * (T(0.5) * w);
         const T rb = delta / delta_b;
         const T wb = s_exp(-rb * rb);
