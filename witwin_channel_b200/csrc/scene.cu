@@ -1,13 +1,11 @@
 // Scene compile: face planes, coplanar groups, diffraction edges and the
-// GPU LBVH (Morton codes -> radix sort -> Karras radix tree -> AABB refit).
+// BVH (binned SAH, built on the host and uploaded once per scene).
 //
 // Coplanar groups follow native/channel/kernels/paths.cu:3168-3190 (keys) and
 // paths.cu:3768-3912 (ordering); edge selection follows
 // native/channel/kernels/diffraction.cu:803-900 and the shared-boundary merge
-// and policy filter of witwin/channel/scene/resources.py:306-405.  The LBVH is
-// Karras, "Maximizing parallelism in the construction of BVHs, octrees, and
-// k-d trees" (HPG 2012).
-#include <cub/cub.cuh>
+// and policy filter of witwin/channel/scene/resources.py:306-405.
+#include <cuda_runtime.h>
 
 #include <algorithm>
 #include <array>
@@ -30,130 +28,162 @@ constexpr double kEndpointQuant = 1.0e-4;    // scene/resources.py:296
 constexpr double kNormalCosTol = 1.0 - 1.0e-5;
 constexpr double kPlaneTolerance = 1.0e-3;   // rayd/reflection.cpp:50
 
-// ------------------------------------------------------------ LBVH kernels
-__device__ __forceinline__ unsigned expand_bits(unsigned v) {
-    v = (v * 0x00010001u) & 0xFF0000FFu;
-    v = (v * 0x00000101u) & 0x0F00F00Fu;
-    v = (v * 0x00000011u) & 0xC30C30C3u;
-    v = (v * 0x00000005u) & 0x49249249u;
-    return v;
-}
+// ------------------------------------------------------------ BVH build
+// Binned surface-area-heuristic build on the host (Wald, "On fast
+// construction of SAH-based bounding volume hierarchies", 2007): each node's
+// triangles are binned by centroid into kSahBins slabs along each axis and
+// split where (area_left * count_left + area_right * count_right) is least;
+// ranges whose centroids coincide, and every node below kSahMaxDepth, split
+// at the median instead.  Leaves hold one triangle; node boxes are the exact
+// fp32 min/max of their triangles' vertices.  Nodes are stored depth first
+// with siblings adjacent; leaf slots follow the final triangle order.
+constexpr int kSahBins = 32;
+constexpr int kSahMaxDepth = kStackDepth - 8;
 
-__global__ void k_morton(int n, const float* vertices, const int* faces, float3 lo, float3 inv_ext,
-                         unsigned long long* keys) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int a = faces[3 * i], b = faces[3 * i + 1], c = faces[3 * i + 2];
-    float cx_ = (vertices[3 * a] + vertices[3 * b] + vertices[3 * c]) * (1.0f / 3.0f);
-    float cy_ = (vertices[3 * a + 1] + vertices[3 * b + 1] + vertices[3 * c + 1]) * (1.0f / 3.0f);
-    float cz_ = (vertices[3 * a + 2] + vertices[3 * b + 2] + vertices[3 * c + 2]) * (1.0f / 3.0f);
-    float x = fminf(fmaxf((cx_ - lo.x) * inv_ext.x * 1024.0f, 0.0f), 1023.0f);
-    float y = fminf(fmaxf((cy_ - lo.y) * inv_ext.y * 1024.0f, 0.0f), 1023.0f);
-    float z = fminf(fmaxf((cz_ - lo.z) * inv_ext.z * 1024.0f, 0.0f), 1023.0f);
-    unsigned code = (expand_bits(unsigned(x)) << 2) | (expand_bits(unsigned(y)) << 1) | expand_bits(unsigned(z));
-    keys[i] = (static_cast<unsigned long long>(code) << 32) | static_cast<unsigned>(i);
-}
-
-__device__ __forceinline__ int delta(const unsigned long long* keys, int n, int i, int j) {
-    if (j < 0 || j >= n) return -1;
-    return __clzll(keys[i] ^ keys[j]);
-}
-
-__global__ void k_karras(int n, const unsigned long long* keys, BvhNode* nodes, int* parent_internal,
-                         int* parent_leaf) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1) return;
-    const int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
-    const int dmin = delta(keys, n, i, i - d);
-    int lmax = 2;
-    while (delta(keys, n, i, i + lmax * d) > dmin) lmax *= 2;
-    int l = 0;
-    for (int t = lmax / 2; t >= 1; t /= 2) {
-        if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+struct BuildBox {
+    float lo[3], hi[3];
+    void reset() {
+        for (int k = 0; k < 3; ++k) { lo[k] = INFINITY; hi[k] = -INFINITY; }
     }
-    const int j = i + l * d;
-    const int dnode = delta(keys, n, i, j);
-    int s = 0;
-    int div = 2;
-    while (true) {
-        const int t = (l + div - 1) / div;
-        if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
-        if (t <= 1) break;
-        div *= 2;
+    void grow(const BuildBox& o) {
+        for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], o.lo[k]); hi[k] = std::max(hi[k], o.hi[k]); }
     }
-    const int gamma = i + s * d + min(d, 0);
-    const int left = (min(i, j) == gamma) ? ~gamma : gamma;
-    const int right = (max(i, j) == gamma + 1) ? ~(gamma + 1) : gamma + 1;
-    nodes[i].d = make_int4(left, right, 0, 0);
-    if (left < 0) parent_leaf[~left] = i; else parent_internal[left] = i;
-    if (right < 0) parent_leaf[~right] = i; else parent_internal[right] = i;
-}
-
-__global__ void k_leaves(int n, const unsigned long long* keys, const float* vertices, const int* faces,
-                         const int* face_group, float4* tri, float* leaf_box) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    const int f = static_cast<int>(keys[s] & 0xffffffffull);
-    const int a = faces[3 * f], b = faces[3 * f + 1], c = faces[3 * f + 2];
-    const float ax = vertices[3 * a], ay = vertices[3 * a + 1], az = vertices[3 * a + 2];
-    const float bx = vertices[3 * b], by = vertices[3 * b + 1], bz = vertices[3 * b + 2];
-    const float cx_ = vertices[3 * c], cy_ = vertices[3 * c + 1], cz_ = vertices[3 * c + 2];
-    tri[3 * s + 0] = make_float4(ax, ay, az, __int_as_float(f));
-    tri[3 * s + 1] = make_float4(bx, by, bz, __int_as_float(face_group[f]));
-    tri[3 * s + 2] = make_float4(cx_, cy_, cz_, 0.0f);
-    leaf_box[6 * s + 0] = fminf(ax, fminf(bx, cx_));
-    leaf_box[6 * s + 1] = fminf(ay, fminf(by, cy_));
-    leaf_box[6 * s + 2] = fminf(az, fminf(bz, cz_));
-    leaf_box[6 * s + 3] = fmaxf(ax, fmaxf(bx, cx_));
-    leaf_box[6 * s + 4] = fmaxf(ay, fmaxf(by, cy_));
-    leaf_box[6 * s + 5] = fmaxf(az, fmaxf(bz, cz_));
-}
-
-__device__ void child_box(const BvhNode* nodes, const float* leaf_box, int ref, float* out) {
-    if (ref < 0) {
-        const int s = ~ref;
-        for (int k = 0; k < 6; ++k) out[k] = __ldcg(leaf_box + 6 * s + k);
-        return;
+    double area() const {
+        const double dx = double(hi[0]) - lo[0], dy = double(hi[1]) - lo[1], dz = double(hi[2]) - lo[2];
+        return dx < 0 ? 0.0 : 2.0 * (dx * dy + dy * dz + dz * dx);
     }
-    const float4 a = __ldcg(&nodes[ref].a);
-    const float4 b = __ldcg(&nodes[ref].b);
-    const float4 c = __ldcg(&nodes[ref].c);
-    out[0] = fminf(a.x, b.z);
-    out[1] = fminf(a.y, b.w);
-    out[2] = fminf(a.z, c.x);
-    out[3] = fmaxf(a.w, c.y);
-    out[4] = fmaxf(b.x, c.z);
-    out[5] = fmaxf(b.y, c.w);
-}
+};
 
-__global__ void k_refit(int n, BvhNode* nodes, const int* parent_internal, const int* parent_leaf,
-                        const float* leaf_box, int* flags, int* depth_out) {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    int p = parent_leaf[s];
-    int depth = 0;
-    // depth: count internal ancestors of this leaf
-    for (int q = p; q >= 0; q = parent_internal[q]) ++depth;
-    atomicMax(depth_out, depth);
-    while (p >= 0) {
-        __threadfence();
-        const int old = atomicAdd(flags + p, 1);
-        if (old == 0) return;  // first arrival: the sibling finishes this node
-        const int4 d = __ldcg(&nodes[p].d);
-        float l[6], r[6];
-        child_box(nodes, leaf_box, d.x, l);
-        child_box(nodes, leaf_box, d.y, r);
-        nodes[p].a = make_float4(l[0], l[1], l[2], l[3]);
-        nodes[p].b = make_float4(l[4], l[5], r[0], r[1]);
-        nodes[p].c = make_float4(r[2], r[3], r[4], r[5]);
-        __threadfence();
-        p = parent_internal[p];
+struct BuildPrim {
+    BuildBox box;
+    float c[3];
+};
+
+// Writes `nodes` (max(F-1, 1) entries, F > 1) and `order` (slot -> face);
+// returns the largest number of internal ancestors of a leaf.
+static int build_bvh(const std::vector<float>& verts, const std::vector<int>& faces, int F, std::vector<BvhNode>& nodes,
+                     std::vector<int>& order) {
+    std::vector<BuildPrim> prim(F);
+    for (int f = 0; f < F; ++f) {
+        BuildBox bx;
+        bx.reset();
+        for (int v = 0; v < 3; ++v)
+            for (int k = 0; k < 3; ++k) {
+                const float x = verts[3 * faces[3 * f + v] + k];
+                bx.lo[k] = std::min(bx.lo[k], x);
+                bx.hi[k] = std::max(bx.hi[k], x);
+            }
+        prim[f].box = bx;
+        for (int k = 0; k < 3; ++k) prim[f].c[k] = 0.5f * (bx.lo[k] + bx.hi[k]);
     }
-}
-
-__global__ void k_fill_int(int n, int* p, int v) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = v;
+    order.resize(F);
+    for (int f = 0; f < F; ++f) order[f] = f;
+    nodes.assign(1, BvhNode{});
+    struct Task {
+        int begin, end, node, depth;
+    };
+    std::vector<Task> stack{{0, F, 0, 0}};
+    int max_depth = 0;
+    auto range_box = [&](int b, int e) {
+        BuildBox bx;
+        bx.reset();
+        for (int i = b; i < e; ++i) bx.grow(prim[order[i]].box);
+        return bx;
+    };
+    while (!stack.empty()) {
+        const Task t = stack.back();
+        stack.pop_back();
+        const int n = t.end - t.begin;
+        max_depth = std::max(max_depth, t.depth + 1);
+        // centroid bounds
+        float clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int i = t.begin; i < t.end; ++i)
+            for (int k = 0; k < 3; ++k) {
+                clo[k] = std::min(clo[k], prim[order[i]].c[k]);
+                chi[k] = std::max(chi[k], prim[order[i]].c[k]);
+            }
+        int mid = -1;
+        if (t.depth < kSahMaxDepth) {
+            double best = INFINITY;
+            int best_axis = -1, best_split = -1;
+            for (int k = 0; k < 3; ++k) {
+                const float ext = chi[k] - clo[k];
+                if (!(ext > 0.0f)) continue;
+                BuildBox bins[kSahBins];
+                int count[kSahBins] = {};
+                for (int q = 0; q < kSahBins; ++q) bins[q].reset();
+                const float scale = float(kSahBins) / ext;
+                for (int i = t.begin; i < t.end; ++i) {
+                    const BuildPrim& pr = prim[order[i]];
+                    const int q = std::min(kSahBins - 1, int((pr.c[k] - clo[k]) * scale));
+                    bins[q].grow(pr.box);
+                    ++count[q];
+                }
+                double right_area[kSahBins];
+                int right_count[kSahBins];
+                BuildBox acc;
+                acc.reset();
+                int cnt = 0;
+                for (int q = kSahBins - 1; q > 0; --q) {
+                    acc.grow(bins[q]);
+                    cnt += count[q];
+                    right_area[q] = acc.area();
+                    right_count[q] = cnt;
+                }
+                acc.reset();
+                cnt = 0;
+                for (int q = 1; q < kSahBins; ++q) {
+                    acc.grow(bins[q - 1]);
+                    cnt += count[q - 1];
+                    if (cnt == 0 || right_count[q] == 0) continue;
+                    const double cost = acc.area() * cnt + right_area[q] * right_count[q];
+                    if (cost < best) {
+                        best = cost;
+                        best_axis = k;
+                        best_split = q;
+                    }
+                }
+            }
+            if (best_axis >= 0) {
+                const int k = best_axis;
+                const float scale = float(kSahBins) / (chi[k] - clo[k]);
+                auto it = std::partition(order.begin() + t.begin, order.begin() + t.end, [&](int f) {
+                    return std::min(kSahBins - 1, int((prim[f].c[k] - clo[k]) * scale)) < best_split;
+                });
+                mid = int(it - order.begin());
+            }
+        }
+        if (mid <= t.begin || mid >= t.end) {
+            // median along the widest centroid extent (ties keep the face order)
+            int k = 0;
+            for (int q = 1; q < 3; ++q)
+                if (chi[q] - clo[q] > chi[k] - clo[k]) k = q;
+            mid = t.begin + n / 2;
+            std::stable_sort(order.begin() + t.begin, order.begin() + t.end,
+                             [&](int x, int y) { return prim[x].c[k] < prim[y].c[k]; });
+        }
+        int child[2];
+        const int rb[2] = {t.begin, mid}, re[2] = {mid, t.end};
+        BuildBox cb[2];
+        for (int s = 0; s < 2; ++s) {
+            cb[s] = range_box(rb[s], re[s]);
+            if (re[s] - rb[s] == 1) {
+                child[s] = ~rb[s];
+            } else {
+                child[s] = int(nodes.size());
+                nodes.push_back(BvhNode{});
+            }
+        }
+        BvhNode& nd = nodes[t.node];
+        nd.a = make_float4(cb[0].lo[0], cb[0].lo[1], cb[0].lo[2], cb[0].hi[0]);
+        nd.b = make_float4(cb[0].hi[1], cb[0].hi[2], cb[1].lo[0], cb[1].lo[1]);
+        nd.c = make_float4(cb[1].lo[2], cb[1].hi[0], cb[1].hi[1], cb[1].hi[2]);
+        nd.d = make_int4(child[0], child[1], 0, 0);
+        // right first so the left subtree is built (and laid out) next
+        for (int s = 1; s >= 0; --s)
+            if (child[s] >= 0) stack.push_back({rb[s], re[s], child[s], t.depth + 1});
+    }
+    return max_depth;
 }
 
 // ------------------------------------------------------------ host helpers
@@ -194,13 +224,6 @@ T* upload(SceneHandle* h, const std::vector<T>& v, cudaStream_t stream) {
     if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
     h->owned.push_back(d);
     if (!v.empty()) cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream);
-    return d;
-}
-
-void* alloc_owned(SceneHandle* h, size_t bytes) {
-    void* d = nullptr;
-    if (cudaMalloc(&d, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
-    h->owned.push_back(d);
     return d;
 }
 
@@ -526,58 +549,39 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
     sd.diagonal = V ? std::sqrt(double(hi[0] - lo[0]) * (hi[0] - lo[0]) + double(hi[1] - lo[1]) * (hi[1] - lo[1]) +
                                 double(hi[2] - lo[2]) * (hi[2] - lo[2]))
                     : 0.0;
-    // ---- LBVH
+    // ---- BVH (host binned SAH) and triangles in leaf order
     sd.root = INT_MIN;
     sd.max_depth = 0;
     if (F > 0) {
-        float4* tri = static_cast<float4*>(alloc_owned(h, size_t(F) * 3 * sizeof(float4)));
-        BvhNode* nodes = static_cast<BvhNode*>(alloc_owned(h, size_t(std::max(F - 1, 1)) * sizeof(BvhNode)));
-        unsigned long long* keys = nullptr;
-        unsigned long long* keys_sorted = nullptr;
-        int *parent_internal = nullptr, *parent_leaf = nullptr, *flags = nullptr, *depth = nullptr;
-        float* leaf_box = nullptr;
-        cudaMalloc(&keys, size_t(F) * 8);
-        cudaMalloc(&keys_sorted, size_t(F) * 8);
-        cudaMalloc(&parent_internal, size_t(std::max(F - 1, 1)) * 4);
-        cudaMalloc(&parent_leaf, size_t(F) * 4);
-        cudaMalloc(&flags, size_t(std::max(F - 1, 1)) * 4);
-        cudaMalloc(&leaf_box, size_t(F) * 24);
-        cudaMalloc(&depth, 4);
-        const int B = 256;
-        float3 flo = make_float3(lo[0], lo[1], lo[2]);
-        float3 inv = make_float3(1.0f / std::max(hi[0] - lo[0], 1e-6f), 1.0f / std::max(hi[1] - lo[1], 1e-6f),
-                                 1.0f / std::max(hi[2] - lo[2], 1e-6f));
-        k_morton<<<(F + B - 1) / B, B, 0, stream>>>(F, sd.vertices, sd.faces, flo, inv, keys);
-        note_launch();
-        size_t temp = 0;
-        cub::DeviceRadixSort::SortKeys(nullptr, temp, keys, keys_sorted, F, 0, 64, stream);
-        void* tmp = nullptr;
-        cudaMalloc(&tmp, std::max<size_t>(temp, 16));
-        cub::DeviceRadixSort::SortKeys(tmp, temp, keys, keys_sorted, F, 0, 64, stream);
-        k_fill_int<<<(F + B - 1) / B, B, 0, stream>>>(std::max(F - 1, 1), parent_internal, -1);
-        k_fill_int<<<(F + B - 1) / B, B, 0, stream>>>(F, parent_leaf, -1);
-        k_fill_int<<<(F + B - 1) / B, B, 0, stream>>>(std::max(F - 1, 1), flags, 0);
-        k_fill_int<<<1, 1, 0, stream>>>(1, depth, 0);
-        note_launch(4);
-        k_leaves<<<(F + B - 1) / B, B, 0, stream>>>(F, keys_sorted, sd.vertices, sd.faces, sd.face_group, tri, leaf_box);
-        note_launch();
-        if (F > 1) {
-            k_karras<<<(F - 1 + B - 1) / B, B, 0, stream>>>(F, keys_sorted, nodes, parent_internal, parent_leaf);
-            k_refit<<<(F + B - 1) / B, B, 0, stream>>>(F, nodes, parent_internal, parent_leaf, leaf_box, flags, depth);
-            note_launch(2);
-        }
+        std::vector<BvhNode> host_nodes;
+        std::vector<int> slot_face;
         int hdepth = 0;
-        cudaMemcpyAsync(&hdepth, depth, 4, cudaMemcpyDeviceToHost, stream);
-        cudaError_t err = cudaStreamSynchronize(stream);
-        cudaFree(keys); cudaFree(keys_sorted); cudaFree(parent_internal); cudaFree(parent_leaf);
-        cudaFree(flags); cudaFree(leaf_box); cudaFree(depth); cudaFree(tmp);
-        if (err != cudaSuccess) { scene_destroy(h); return 2; }
-        sd.tri = tri;
-        sd.nodes = nodes;
+        if (F > 1) {
+            hdepth = build_bvh(verts, faces, F, host_nodes, slot_face);
+        } else {
+            slot_face.assign(1, 0);
+            host_nodes.assign(1, BvhNode{});
+        }
+        if (hdepth >= kStackDepth) { scene_destroy(h); return 4; }
+        std::vector<float4> tri(size_t(F) * 3);
+        for (int sl = 0; sl < F; ++sl) {
+            const int f = slot_face[sl];
+            const float* a = &verts[3 * faces[3 * f]];
+            const float* b = &verts[3 * faces[3 * f + 1]];
+            const float* c = &verts[3 * faces[3 * f + 2]];
+            float fbits, gbits;
+            std::memcpy(&fbits, &f, 4);
+            std::memcpy(&gbits, &face_group[f], 4);
+            tri[3 * sl + 0] = make_float4(a[0], a[1], a[2], fbits);
+            tri[3 * sl + 1] = make_float4(b[0], b[1], b[2], gbits);
+            tri[3 * sl + 2] = make_float4(c[0], c[1], c[2], 0.0f);
+        }
+        sd.tri = upload(h, tri, stream);
+        sd.nodes = upload(h, host_nodes, stream);
+        if (sd.tri == nullptr || sd.nodes == nullptr) { scene_destroy(h); return 2; }
         sd.root = F > 1 ? 0 : ~0;
         sd.max_depth = hdepth;
         h->num_nodes = std::max(F - 1, 0);
-        if (hdepth >= kStackDepth) { scene_destroy(h); return 4; }
     }
     if (cudaStreamSynchronize(stream) != cudaSuccess) { scene_destroy(h); return 2; }
     *out = h;

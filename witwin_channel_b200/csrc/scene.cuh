@@ -1,4 +1,4 @@
-// Device-resident scene: triangles in Morton order, the LBVH, per-face
+// Device-resident scene: triangles in BVH leaf order, the BVH, per-face
 // tables, coplanar face groups and the selected diffraction edges.
 #pragma once
 
@@ -28,7 +28,7 @@ struct SceneDev {
     // geometry
     const float* vertices;     // (V,3)
     const int* faces;          // (F,3)
-    const float4* tri;         // (F*3) Morton order: v0|face, v1|group, v2|pad
+    const float4* tri;         // (F*3) leaf order: v0|face, v1|group, v2|pad
     const BvhNode* nodes;      // (F-1)
     // per face (original order)
     const float* face_normal;  // (F,3) unit, fp32
