@@ -6,7 +6,7 @@ its structure, surface id (the structure's ``surface_id`` or its index) and
 material row; materials are evaluated at the solve frequency with PEC
 realised as ``sigma_e = 1e9`` (``materials.py:28-60``) and thin-sheet layer
 stacks as a CSR table (``materials.py:123-145``).  Geometry-only results (the
-LBVH, coplanar groups, edges) are cached per scene and reused across
+BVH, coplanar groups, edges) are cached per scene and reused across
 frequencies and material changes.
 """
 

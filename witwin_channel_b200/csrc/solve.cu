@@ -11,7 +11,7 @@
 //     visibility prefilter, rayd/diffraction.cpp:380-403).
 // Main kernel: one thread per (transmitter, receiver cell).  Each thread walks
 // every candidate of its transmitter, traces the visibility segments through
-// the LBVH, evaluates the complex fields for every solve frequency and keeps
+// the BVH, evaluates the complex fields for every solve frequency and keeps
 // the per-slot coherent sums in registers; each output cell is written once.
 #include <cub/cub.cuh>
 

@@ -1,4 +1,4 @@
-// LBVH traversal: any-hit segment occlusion, closest hit, and ordered
+// BVH traversal: any-hit segment occlusion, closest hit, and ordered
 // all-hits along a segment.
 //
 // Each thread keeps its stack in shared memory, interleaved across the block
