@@ -161,38 +161,51 @@ class CompiledScene:
         return out
 
     def material_tables(self, frequencies: list[float], device: torch.device) -> MaterialTables:
+        """Material and layer tables at ``frequencies``: every value packed into
+        one float and one int buffer, each copied to the device once (pinned,
+        asynchronous), the tables being views of those buffers."""
         per_f = [self.material_values(f) for f in frequencies]
-
-        def stack(name: str) -> torch.Tensor:
-            return torch.tensor([v[name] for v in per_f], dtype=torch.float32, device=device).reshape(len(frequencies), -1)
-
-        counts = [len(rows) for rows in per_f[0]["layers"]] if per_f else []
+        nf = len(frequencies)
+        M = len(self.materials)
+        counts = [len(rows) for rows in per_f[0]["layers"]] if per_f else [0] * M
         offsets = []
         acc = 0
         for c in counts:
             offsets.append(acc)
             acc += c
-        lt, le, ls, lm = [], [], [], []
-        for v in per_f:
-            flat = [row for rows in v["layers"] for row in rows]
-            lt.append([r[0] for r in flat])
-            le.append([r[1] for r in flat])
-            ls.append([r[2] for r in flat])
-            lm.append([r[3] for r in flat])
-        nf = len(frequencies)
+        L = acc
+        floats: list[float] = []
+        for name in ("eps_r", "sigma_e", "mu_r", "gain", "thickness"):
+            for v in per_f:
+                floats.extend(v[name])
+        for col in range(4):
+            for v in per_f:
+                floats.extend(row[col] for rows in v["layers"] for row in rows)
+        ints = [int(getattr(m, "geometry_mode", "thin_sheet") == "volumetric") for m in self.materials]
+        ints += offsets + counts
+        fdev = to_device(floats, torch.float32, device)
+        idev = to_device(ints, torch.int32, device)
 
-        def t2(x):
-            return torch.tensor(x, dtype=torch.float32, device=device).reshape(nf, -1)
+        def fview(k: int, width: int, base: int = 0) -> torch.Tensor:
+            o = base + k * nf * width
+            return fdev[o:o + nf * width].view(nf, width)
 
-        vol = torch.tensor([int(getattr(m, "geometry_mode", "thin_sheet") == "volumetric") for m in self.materials],
-                           dtype=torch.int32, device=device)
+        lbase = 5 * nf * M
         return MaterialTables(
-            eps_r=stack("eps_r"), sigma_e=stack("sigma_e"), mu_r=stack("mu_r"), gain=stack("gain"),
-            thickness=stack("thickness"), volumetric=vol,
-            layer_offset=torch.tensor(offsets, dtype=torch.int32, device=device),
-            layer_count=torch.tensor(counts, dtype=torch.int32, device=device),
-            layer_thickness=t2(lt), layer_eps_r=t2(le), layer_sigma_e=t2(ls), layer_mu_r=t2(lm),
+            eps_r=fview(0, M), sigma_e=fview(1, M), mu_r=fview(2, M), gain=fview(3, M), thickness=fview(4, M),
+            volumetric=idev[0:M], layer_offset=idev[M:2 * M], layer_count=idev[2 * M:3 * M],
+            layer_thickness=fview(0, L, lbase), layer_eps_r=fview(1, L, lbase), layer_sigma_e=fview(2, L, lbase),
+            layer_mu_r=fview(3, L, lbase),
         )
+
+
+def to_device(values: list, dtype: torch.dtype, device: torch.device) -> torch.Tensor:
+    """One host-to-device copy of a flat list (through pinned memory, not
+    waited for on the host)."""
+    host = torch.tensor(values, dtype=dtype)
+    if device.type != "cuda":
+        return host.to(device)
+    return host.pin_memory().to(device, non_blocking=True)
 
 
 # compiled scenes keyed by the scene object's identity (scene types need not be

@@ -95,9 +95,10 @@ WCB_HD PathEval<T> eval_free_space(V3<T> source, V3<T> target, V3<T> tx_pol, V3<
 }
 
 // Rouard stack transmission for one wall (_reference_fields.py:196-273).
-// Layers ordered entry -> exit; returns t.
-template <typename T, typename F = double>
-WCB_HD Cx<T> stack_t(T cos_theta, const T* thickness, const T* eps_r, const T* sigma_e, const T* mu_r, int count,
+// Layers ordered entry -> exit; returns t.  The layer values are stored as S
+// and read as T (an FP64 solve reads the FP32 tables exactly widened).
+template <typename T, typename F = double, typename S = T>
+WCB_HD Cx<T> stack_t(T cos_theta, const S* thickness, const S* eps_r, const S* sigma_e, const S* mu_r, int count,
                      F frequency, int pol_tm) {
     if (count <= 0) return cx(T(1), T(0));
     const T omega = T(s_max(kTwoPi * frequency, kUtdSmallEps));
@@ -113,8 +114,8 @@ WCB_HD Cx<T> stack_t(T cos_theta, const T* thickness, const T* eps_r, const T* s
         return (eps_abs * omega) / kz;
     };
     auto medium = [&](int i, Cx<T>* eps_abs, Cx<T>* mu_abs, Cx<T>* kz) {
-        *eps_abs = cx(T(kEps0) * s_max(eps_r[i], T(kUtdSmallEps)), -s_max(sigma_e[i], T(0)) / omega);
-        *mu_abs = cx(T(kMu0) * s_max(mu_r[i], T(kUtdSmallEps)), T(0));
+        *eps_abs = cx(T(kEps0) * s_max(T(eps_r[i]), T(kUtdSmallEps)), -s_max(T(sigma_e[i]), T(0)) / omega);
+        *mu_abs = cx(T(kMu0) * s_max(T(mu_r[i]), T(kUtdSmallEps)), T(0));
         const Cx<T> kk = csqrt((*eps_abs) * (*mu_abs)) * omega;
         *kz = csqrt(kk * kk - cx(k_par * k_par, T(0)));
     };
@@ -127,7 +128,7 @@ WCB_HD Cx<T> stack_t(T cos_theta, const T* thickness, const T* eps_r, const T* s
     Cx<T> t_total = (y_below * T(2)) / (y_below + y_exit);
     const Cx<T> one = cx(T(1), T(0));
     for (int layer = count - 1; layer >= 0; --layer) {
-        const T th = s_max(thickness[layer], T(0));
+        const T th = s_max(T(thickness[layer]), T(0));
         // exp(-j kz th)
         const Cx<T> phase = cexp(cx(kz_below.im * th, -kz_below.re * th));
         const Cx<T> phase2 = phase * phase;
@@ -164,24 +165,26 @@ struct LayerTable {
 };
 
 // One wall of the straight thin-sheet chain (_reference_fields.py:307-333).
-template <typename T>
+template <typename T, typename S>
 WCB_HD void transmit_wall(C3<T>& value, T& carrier_shortening, V3<T> dir, V3<T> normal_in, int material,
-                          const LayerTable<T>& lt, double frequency) {
+                          const LayerTable<S>& lt, double frequency) {
     V3<T> n = safe_normalize(normal_in, v3<T>(T(0), T(0), T(1)));
     if (value_of(dot(dir, n)) > 0) n = -n;
     T ct = s_abs(dot(dir, n));
     ct = s_min(s_max(ct, T(kUtdSmallEps)), T(1));
     const int first = lt.offset[material];
     const int cnt = lt.count[material];
-    const Cx<T> t_te = stack_t<T>(ct, lt.thickness + first, lt.eps_r + first, lt.sigma_e + first, lt.mu_r + first, cnt, frequency, 0);
-    const Cx<T> t_tm = stack_t<T>(ct, lt.thickness + first, lt.eps_r + first, lt.sigma_e + first, lt.mu_r + first, cnt, frequency, 1);
+    const Cx<T> t_te = stack_t<T, double, S>(ct, lt.thickness + first, lt.eps_r + first, lt.sigma_e + first,
+                                             lt.mu_r + first, cnt, frequency, 0);
+    const Cx<T> t_tm = stack_t<T, double, S>(ct, lt.thickness + first, lt.eps_r + first, lt.sigma_e + first,
+                                             lt.mu_r + first, cnt, frequency, 1);
     const V3<T> s_axis = safe_normalize(cross(n, dir), stable_perp_basis(dir, n));
     const V3<T> p_axis = safe_normalize(cross(s_axis, dir), stable_perp_basis(dir, s_axis));
     const Cx<T> e_s = c3_dot(value, s_axis);
     const Cx<T> e_p = c3_dot(value, p_axis);
     value = c3_axis(s_axis, t_te * e_s) + c3_axis(p_axis, t_tm * e_p);
     T wall = T(0);
-    for (int i = 0; i < cnt; ++i) wall = wall + s_max(lt.thickness[first + i], T(0));
+    for (int i = 0; i < cnt; ++i) wall = wall + s_max(T(lt.thickness[first + i]), T(0));
     carrier_shortening = carrier_shortening + wall * ct;
 }
 

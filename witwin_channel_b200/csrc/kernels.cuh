@@ -33,21 +33,12 @@ WCB_D Slab<T> face_slab(const MainParams& p, int f_index, int face) {
     return Slab<T>{T(p.mat_eps_r[o]), T(p.mat_sigma_e[o]), T(p.mat_mu_r[o]), T(p.mat_gain[o]), T(p.mat_thickness[o])};
 }
 
-template <typename T>
-WCB_D LayerTable<T> layer_table_f(const MainParams& p, int f_index);
-
-template <>
-WCB_D LayerTable<float> layer_table_f<float>(const MainParams& p, int f_index) {
+// Layer tables of frequency f_index (FP32 values; an FP64 solve widens them
+// on load, which is exact).
+WCB_D LayerTable<float> layer_table_f(const MainParams& p, int f_index) {
     const long long o = (long long)f_index * p.num_layers;
     return LayerTable<float>{p.layer_offset, p.layer_count, p.layer_thickness + o, p.layer_eps_r + o,
                              p.layer_sigma_e + o, p.layer_mu_r + o};
-}
-
-template <>
-WCB_D LayerTable<double> layer_table_f<double>(const MainParams& p, int f_index) {
-    const long long o = (long long)f_index * p.num_layers;
-    return LayerTable<double>{p.layer_offset, p.layer_count, p.layer_thickness64 + o, p.layer_eps_r64 + o,
-                              p.layer_sigma_e64 + o, p.layer_mu_r64 + o};
 }
 
 WCB_D void emit_row(const MainParams& p, int t, int r, int cid, int depth, const int* seq, int edge, float length) {
@@ -224,7 +215,7 @@ __global__ void __launch_bounds__(kCompBlock) k_los_trans(MainParams p) {
                     for (int f = 0; f < NF; ++f) {
                         C3<T> value = c3_from_real(transverse(dir, tx_pol));
                         T shorten = T(0);
-                        const LayerTable<T> lt = layer_table_f<T>(p, f);
+                        const LayerTable<float> lt = layer_table_f(p, f);
                         for (int i = 0; i < hl.count; ++i) {
                             const float* nf = sc.face_normal + 3 * hl.face[i];
                             transmit_wall(value, shorten, dir, v3<T>(T(nf[0]), T(nf[1]), T(nf[2])),

@@ -40,9 +40,22 @@ constexpr long long kOrder1ExhaustiveLimit = 4096;      // interactions/reflecti
 constexpr long long kMultibounceExhaustiveLimit = 100000;  // interactions/reflection.py:31
 
 // ------------------------------------------------------------ discovery
-__global__ void k_fibonacci(int count, float* dirs) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
+// Slot j of the discovery rays holds Fibonacci-lattice direction i = perm(j).
+// The rays are split into bands of `band` consecutive indices (a Fibonacci
+// number F_m near sqrt(32 pi count)); within a band the azimuth of index
+// b0 + o is 2 pi frac(o / golden) up to a constant, whose order follows
+// o * F_{m-1} mod F_m, so slot k of the band takes o = k * inv mod F_m (inv =
+// F_{m-1}^-1 mod F_m).  A warp's 32 rays then leave in neighbouring
+// directions and trace together; the tail band keeps the identity order.
+// The chain tables depend only on the set of rays, not on their slots.
+__global__ void k_fibonacci(int count, float* dirs, int band, int inv) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    long long i = j;
+    if (band > 1) {
+        const int b = j / band;
+        if (b < count / band) i = (long long)b * band + ((long long)(j - b * band) * inv) % band;
+    }
     const double golden = 1.618033988749894848204586834365638118;
     const double idx = double(i);
     const double az = idx / golden;
@@ -51,9 +64,40 @@ __global__ void k_fibonacci(int count, float* dirs) {
     const double phi = 2.0 * kPi * az_u;
     const double z = 1.0 - 2.0 * ev;
     const double radial = sqrt(fmax(1.0 - z * z, 0.0));
-    dirs[3 * i + 0] = float(radial * cos(phi));
-    dirs[3 * i + 1] = float(radial * sin(phi));
-    dirs[3 * i + 2] = float(z);
+    dirs[3 * j + 0] = float(radial * cos(phi));
+    dirs[3 * j + 1] = float(radial * sin(phi));
+    dirs[3 * j + 2] = float(z);
+}
+
+// Band size and multiplier of the coherent ray order for `count` rays (band
+// 0: identity order).
+static void fibonacci_bands(int count, int* band, int* inv) {
+    *band = 0;
+    *inv = 1;
+    if (count < 256) return;
+    const double target = std::sqrt(32.0 * kPi * double(count));
+    long long prev = 1, cur = 2;
+    while (cur < target) {
+        const long long next = prev + cur;
+        prev = cur;
+        cur = next;
+    }
+    if (cur - target > target - prev) {  // the nearer Fibonacci number
+        const long long p2 = cur - prev;
+        cur = prev;
+        prev = p2;
+    }
+    if (cur > count || cur < 2) return;
+    // inverse of prev modulo cur (consecutive Fibonacci numbers are coprime)
+    long long r0 = cur, r1 = prev, t0 = 0, t1 = 1;
+    while (r1 != 0) {
+        const long long q = r0 / r1;
+        long long tmp = r0 - q * r1; r0 = r1; r1 = tmp;
+        tmp = t0 - q * t1; t0 = t1; t1 = tmp;
+    }
+    if (r0 != 1) return;
+    *band = int(cur);
+    *inv = int(((t0 % cur) + cur) % cur);
 }
 
 template <typename G>
@@ -250,10 +294,6 @@ __global__ void k_compact_flags(int n, const int* flags, int* list, int* count) 
 }
 
 // ------------------------------------------------------------ main kernel
-__global__ void k_to_double(long long n, const float* in, double* out) {
-    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n) out[i] = in[i];
-}
 
 
 // Start/end events of the four per-cell kernels (LoS+transmission,
@@ -456,7 +496,6 @@ struct WorkspaceLayout {
     size_t edge_flags, edge_list, edge_count;
     size_t diff_words, diff_carry;
     size_t overflow;
-    size_t layers64;
     size_t total;
     long long chain_ints_per_tx;
 };
@@ -506,7 +545,6 @@ static WorkspaceLayout layout_for(const SceneDev& sc, const wcb_solve_desc& d, c
     const long long cells = (long long)T * (d.rx_kind == 1 ? (long long)d.grid_rows * d.grid_cols : d.num_rx);
     L.diff_carry = take(dp.chunks > 1 ? size_t(cells) * kMaxNF * 9 * 8 : 0);
     L.overflow = take(64);
-    L.layers64 = 0;
     L.total = o;
     return L;
 }
@@ -589,7 +627,9 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         const bool need_disc = !(pl.exhaustive_o1 && (d->max_depth < 2 || pl.exhaustive_mb));
         float* dirs = reinterpret_cast<float*>(base + L.disc_dirs);
         if (need_disc) {
-            k_fibonacci<<<(rays + B - 1) / B, B, 0, side>>>(rays, dirs);
+            int band = 0, inv = 1;
+            fibonacci_bands(rays, &band, &inv);
+            k_fibonacci<<<(rays + B - 1) / B, B, 0, side>>>(rays, dirs, band, inv);
             note_launch();
         }
         // exhaustive tables are identical for every tx: generate per tx
@@ -730,29 +770,6 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     p.overflow_counter = overflow;
     p.ray_counter = prof.enabled ? main_ray_counter : nullptr;
     p.num_freq_total = d->num_freq;
-    // FP64 mode: double copies of the layer tables
-    double* layers64 = nullptr;
-    if (fp64 && m->num_layers > 0) {
-        const long long n = (long long)m->num_layers * d->num_freq;
-        if (cudaMallocAsync(&layers64, size_t(n) * 4 * 8, stream) != cudaSuccess) {
-            if (side != stream) {
-                cudaEventRecord(join, side);
-                cudaStreamWaitEvent(stream, join, 0);
-                cudaEventDestroy(fork);
-                cudaEventDestroy(join);
-            }
-            return 2;
-        }
-        const float* src[4] = {m->layer_thickness, m->layer_eps_r, m->layer_sigma_e, m->layer_mu_r};
-        for (int q = 0; q < 4; ++q) {
-            k_to_double<<<int((n + B - 1) / B), B, 0, stream>>>(n, src[q], layers64 + q * n);
-            note_launch();
-        }
-        p.layer_thickness64 = layers64;
-        p.layer_eps_r64 = layers64 + n;
-        p.layer_sigma_e64 = layers64 + 2 * n;
-        p.layer_mu_r64 = layers64 + 3 * n;
-    }
     const long long tiles = tiles_per_tx(p) * T;
     const long long blocks = (tiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const int sdepth = std::max(8, std::min(kStackDepth, sc.max_depth + 2));
@@ -789,12 +806,6 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         q.layer_eps_r = m->layer_eps_r ? m->layer_eps_r + lo : nullptr;
         q.layer_sigma_e = m->layer_sigma_e ? m->layer_sigma_e + lo : nullptr;
         q.layer_mu_r = m->layer_mu_r ? m->layer_mu_r + lo : nullptr;
-        if (layers64) {
-            q.layer_thickness64 = p.layer_thickness64 + lo;
-            q.layer_eps_r64 = p.layer_eps_r64 + lo;
-            q.layer_sigma_e64 = p.layer_sigma_e64 + lo;
-            q.layer_mu_r64 = p.layer_mu_r64 + lo;
-        }
         if (fb > 0) q.rows = nullptr;  // geometry rows are emitted once
         if (blocks <= 0) continue;
         ComponentEvents* evp = prof.enabled ? &cev : nullptr;
@@ -869,7 +880,6 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         cudaEventDestroy(fork);
         cudaEventDestroy(join);
     }
-    if (layers64) cudaFreeAsync(layers64, stream);
     if (cudaGetLastError() != cudaSuccess) return 2;
     return 0;
 }

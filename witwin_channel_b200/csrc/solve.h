@@ -56,10 +56,6 @@ struct MainParams {
     const float* layer_eps_r;
     const float* layer_sigma_e;
     const float* layer_mu_r;
-    const double* layer_thickness64;
-    const double* layer_eps_r64;
-    const double* layer_sigma_e64;
-    const double* layer_mu_r64;
     int components;
     int max_depth;
     int coherent;

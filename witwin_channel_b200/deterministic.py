@@ -167,10 +167,17 @@ def _validate(scene: Any, config: Config) -> None:
 def _endpoints(scene: Any, device: torch.device) -> engine.Endpoints:
     txs = scene.transmitters
     if txs:
-        pos = torch.stack([t.position.detach().to(torch.float32).reshape(3) for t in txs]).to(device).contiguous()
-        pw = torch.tensor([float(t.power_w.detach()) if isinstance(t.power_w, torch.Tensor) else float(t.power_w)
-                           for t in txs], dtype=torch.float32, device=device)
-        pol = torch.stack([t.polarization.detach().to(torch.float32).reshape(3) for t in txs]).to(device).contiguous()
+        # positions, powers and polarisations in one host buffer and one copy
+        T = len(txs)
+        host = torch.empty(7 * T, dtype=torch.float32)
+        host[:3 * T] = torch.stack([t.position.detach().to(torch.float32).reshape(3) for t in txs]).reshape(-1)
+        host[3 * T:4 * T] = torch.tensor([float(t.power_w.detach()) if isinstance(t.power_w, torch.Tensor)
+                                          else float(t.power_w) for t in txs], dtype=torch.float32)
+        host[4 * T:] = torch.stack([t.polarization.detach().to(torch.float32).reshape(3) for t in txs]).reshape(-1)
+        buf = host.pin_memory().to(device, non_blocking=True)
+        pos = buf[:3 * T].view(T, 3)
+        pw = buf[3 * T:4 * T]
+        pol = buf[4 * T:].view(T, 3)
     else:
         pos = torch.zeros((0, 3), dtype=torch.float32, device=device)
         pw = torch.zeros((0,), dtype=torch.float32, device=device)
