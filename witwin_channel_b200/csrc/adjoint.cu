@@ -45,6 +45,15 @@ __global__ void k_vjp_count(AdjParams p, int* keys, int* idx) {
     atomicAdd(p.comp_counts + rank, 1);
 }
 
+// work items of each ordered record of one component: its parameters, or one
+// for a parameterless record whose FP64 field is wanted
+__global__ void k_vjp_work(AdjParams p, int* work) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= p.order_count) return;
+    const long long i = p.order[p.order_begin + j];
+    work[j] = max(p.counts[i], p.row_field ? 1 : 0);
+}
+
 // One block per run of equal ids in the id-sorted pairs (a parameter's
 // contributions): each thread sums a fixed strided subset in record order,
 // then a fixed-shape block tree; the result does not depend on timing, so
@@ -91,11 +100,12 @@ VjpLayout vjp_layout(long long K, long long pairs) {
     L.keys2 = take(k * 4);
     L.order = take(k * 4);
     L.order2 = take(k * 4);
-    size_t scan_b = 0, group_b = 0;
+    size_t scan_b = 0, group_b = 0, work_b = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, scan_b, (int*)nullptr, (long long*)nullptr, int(k));
     cub::DeviceRadixSort::SortPairs(nullptr, group_b, (int*)nullptr, (int*)nullptr, (int*)nullptr, (int*)nullptr,
                                     int(k), 0, 5);
-    L.scan_bytes = std::max(scan_b, group_b);
+    cub::DeviceScan::ExclusiveSum(nullptr, work_b, (int*)nullptr, (int*)nullptr, int(k));
+    L.scan_bytes = std::max(std::max(scan_b, group_b), work_b);
     L.scan_tmp = take(L.scan_bytes);
     L.ids = take(m * 4);
     L.ids2 = take(m * 4);
@@ -290,7 +300,23 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
                 case 0: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 0><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
                 case 1: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 1><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
                 case 5: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 5><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
-                default: wcb::adj::launch_vjp_diffraction(p, s); break;
+                default: {
+                    // one thread per (record, parameter): work per record, its prefix, the total
+                    int* work = keys;
+                    int* pair_base = keys2;
+                    wcb::adj::k_vjp_work<<<g, wcb::adj::kBlock, 0, s>>>(p, work);
+                    size_t wb = L.scan_bytes;
+                    if (cub::DeviceScan::ExclusiveSum(b + L.scan_tmp, wb, work, pair_base, int(p.order_count), s) !=
+                        cudaSuccess)
+                        return WCB_ERR_CUDA;
+                    int tail[2] = {0, 0};
+                    cudaMemcpyAsync(&tail[0], pair_base + p.order_count - 1, 4, cudaMemcpyDeviceToHost, s);
+                    cudaMemcpyAsync(&tail[1], work + p.order_count - 1, 4, cudaMemcpyDeviceToHost, s);
+                    if (cudaStreamSynchronize(s) != cudaSuccess) return WCB_ERR_CUDA;
+                    wcb::adj::launch_vjp_diffraction(p, pair_base, (long long)tail[0] + tail[1], s);
+                    wcb::note_launch(2);
+                    break;
+                }
             }
             wcb::note_launch();
         }

@@ -416,7 +416,54 @@ __global__ void __launch_bounds__(kBlock) k_vjp_rows(AdjParams p) {
     }
 }
 
-void launch_vjp_diffraction(const AdjParams& p, cudaStream_t s);
+// The same contributions with one thread per (record, parameter): each
+// thread carries a single tangent lane through the record's evaluation.  The
+// lanes of a dual number never mix, so every contribution is bit-identical to
+// the N-lane kernel's; the one-lane evaluation holds far fewer live values
+// per thread, which pays for the repeated value part on the heavy UTD
+// records.  `pair_base` is the exclusive prefix over the component's ordered
+// records of their work items (parameters, or one for a parameterless record
+// whose FP64 field is wanted; k_vjp_work in adjoint.cu).
+
+template <int COMP>
+__global__ void __launch_bounds__(kBlock, 4) k_vjp_pairs(AdjParams p, const int* pair_base, long long total) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    // the last ordered record whose work range starts at or before t
+    long long lo = 0, hi = p.order_count - 1;
+    while (lo < hi) {
+        const long long mid = (lo + hi + 1) >> 1;
+        if (pair_base[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    const long long i = p.order[p.order_begin + lo];
+    const RowRec row = p.rows[p.selected[i]];
+    if (row.component != COMP) return;
+    ParamList pl;
+    build_params(p, row, pl);
+    const int q = int(t - pair_base[lo]);
+    Window<1> w;
+    w.n = q < pl.n ? 1 : 0;
+    w.id[0] = q < pl.n ? pl.id[q] : -1;
+    const Cx<Dual<1>> pf = eval_record<1, COMP>(p, row, w);
+    if (q == 0 && p.row_field) {
+        p.row_field[2 * i] = pf.re.v;
+        p.row_field[2 * i + 1] = pf.im.v;
+    }
+    if (q < pl.n) {
+        const double gg = p.g_gain ? p.g_gain[i] : 0.0;
+        const double gr = p.g_re ? p.g_re[i] : 0.0;
+        const double gi = p.g_im ? p.g_im[i] : 0.0;
+        const double dre = pf.re.d[0], dim = pf.im.d[0];
+        const double dg = 2.0 * (pf.re.v * dre + pf.im.v * dim);
+        double c = gg * dg + gr * dre + gi * dim;
+        if (!isfinite(c)) c = 0.0;
+        p.out_ids[p.offsets[i] + q] = unsigned(w.id[0]);
+        p.out_vals[p.offsets[i] + q] = c;
+    }
+}
+
+void launch_vjp_diffraction(const AdjParams& p, const int* pair_base, long long total, cudaStream_t s);
 
 }  // namespace adj
 }  // namespace wcb

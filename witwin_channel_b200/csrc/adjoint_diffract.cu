@@ -5,9 +5,10 @@
 namespace wcb {
 namespace adj {
 
-void launch_vjp_diffraction(const AdjParams& p, cudaStream_t s) {
-    if (p.order_count <= 0) return;
-    k_vjp_rows<kLanes, 2><<<unsigned((p.order_count + kBlock - 1) / kBlock), kBlock, 0, s>>>(p);
+// One thread per (record, parameter) over the diffraction records.
+void launch_vjp_diffraction(const AdjParams& p, const int* pair_base, long long total, cudaStream_t s) {
+    if (p.order_count <= 0 || total <= 0) return;
+    k_vjp_pairs<2><<<unsigned((total + kBlock - 1) / kBlock), kBlock, 0, s>>>(p, pair_base, total);
 }
 
 }  // namespace adj
