@@ -22,11 +22,22 @@ struct Ignore {
 };
 WCB_HD Ignore ignore_none() { return Ignore{-1, -1, -1, -1}; }
 
+// A ray with its watertight-test constants: the axis permutation (kz = the
+// largest |d| component, kx and ky the next two, swapped when d[kz] < 0) and
+// the shear Sx = d[kx]/d[kz], Sy = d[ky]/d[kz], Sz = 1/d[kz], computed once per
+// ray instead of once per triangle test.
 template <typename G>
 struct Ray {
     V3<G> o, d, inv;
     G tmin, tmax;
+    G Sx, Sy, Sz;
+    int kx, ky, kz;
 };
+
+template <typename G>
+WCB_D G comp3(const V3<G>& v, int i) {
+    return i == 0 ? v.x : (i == 1 ? v.y : v.z);
+}
 
 template <typename G>
 WCB_D Ray<G> make_ray(V3<G> o, V3<G> d, G tmin, G tmax) {
@@ -39,6 +50,18 @@ WCB_D Ray<G> make_ray(V3<G> o, V3<G> d, G tmin, G tmax) {
     r.inv.z = s_abs(d.z) > G(1e-30) ? G(1) / d.z : (d.z >= G(0) ? big : -big);
     r.tmin = tmin;
     r.tmax = tmax;
+    const G adx = s_abs(d.x), ady = s_abs(d.y), adz = s_abs(d.z);
+    int kz = adx > ady ? (adx > adz ? 0 : 2) : (ady > adz ? 1 : 2);
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    if (comp3(d, kz) < G(0)) { const int t = kx; kx = ky; ky = t; }
+    const G dz = comp3(d, kz);
+    r.Sx = comp3(d, kx) / dz;
+    r.Sy = comp3(d, ky) / dz;
+    r.Sz = G(1) / dz;
+    r.kx = kx;
+    r.ky = ky;
+    r.kz = kz;
     return r;
 }
 
@@ -61,14 +84,9 @@ WCB_D G tri_hit(const Ray<G>& r, float4 a4, float4 b4, float4 c4) {
     const V3<G> A0 = v3<G>(G(a4.x), G(a4.y), G(a4.z)) - r.o;
     const V3<G> B0 = v3<G>(G(b4.x), G(b4.y), G(b4.z)) - r.o;
     const V3<G> C0 = v3<G>(G(c4.x), G(c4.y), G(c4.z)) - r.o;
-    const G adx = s_abs(r.d.x), ady = s_abs(r.d.y), adz = s_abs(r.d.z);
-    int kz = adx > ady ? (adx > adz ? 0 : 2) : (ady > adz ? 1 : 2);
-    int kx = kz + 1 == 3 ? 0 : kz + 1;
-    int ky = kx + 1 == 3 ? 0 : kx + 1;
-    auto comp = [](const V3<G>& v, int i) -> G { return i == 0 ? v.x : (i == 1 ? v.y : v.z); };
-    if (comp(r.d, kz) < G(0)) { int t = kx; kx = ky; ky = t; }
-    const G dz = comp(r.d, kz);
-    const G Sx = comp(r.d, kx) / dz, Sy = comp(r.d, ky) / dz, Sz = G(1) / dz;
+    const int kx = r.kx, ky = r.ky, kz = r.kz;
+    const G Sx = r.Sx, Sy = r.Sy, Sz = r.Sz;
+    auto comp = [](const V3<G>& v, int i) -> G { return comp3(v, i); };
     const G Ax = comp(A0, kx) - Sx * comp(A0, kz), Ay = comp(A0, ky) - Sy * comp(A0, kz);
     const G Bx = comp(B0, kx) - Sx * comp(B0, kz), By = comp(B0, ky) - Sy * comp(B0, kz);
     const G Cx_ = comp(C0, kx) - Sx * comp(C0, kz), Cy = comp(C0, ky) - Sy * comp(C0, kz);
