@@ -262,3 +262,17 @@ def test_diffraction_edge_chunks_match_one_chunk(monkeypatch):
         b = b.double().cpu()
         assert float(a.abs().max()) > 0
         assert torch.all((a - b).abs() <= 1e-5 * a.abs() + 1e-6 * float(a.abs().max()))
+
+
+def test_chain_dedup_bitmap_equals_sort(monkeypatch):
+    """Discovery-mode chains (16 boxes, depth 3: too many group sequences for
+    the exhaustive tables) deduplicated through the bitmap and through the
+    radix sort give the same chain tables, hence bit-identical maps."""
+    scene, freq = scenes.small_city(n_boxes=16, seed=5, grid=(12, 10))
+    cfg = Config(components={"los", "reflection"}, max_depth=3, coherent=True)
+    a = solve(scene, cfg, reference_frequency_hz=freq)
+    monkeypatch.setenv("WCB_CHAIN_BITMAP_BITS", "0")
+    b = solve(scene, cfg, reference_frequency_hz=freq)
+    assert float(a.path_gain.max()) > 0
+    assert torch.equal(a.path_gain, b.path_gain)
+    assert torch.equal(a.component_power["reflection"], b.component_power["reflection"])

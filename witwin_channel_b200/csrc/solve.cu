@@ -186,6 +186,59 @@ __global__ void k_chain_emit(int count, int depth, int k, const unsigned long lo
     }
 }
 
+// Bitmap form of the same dedup for small key spaces: bit (pr * G + g) is set
+// for every ray's key; the unique keys in ascending order are the set bits in
+// bit order, so a key's rank is the popcount of the bits below it (a scan of
+// per-word popcounts plus the word's lower bits).  The ray that sets a bit
+// writes that chain's groups (every ray with the key has the same group
+// sequence), so the chain table equals the sorted form's.
+__global__ void k_chain_bits(int count, int depth, int k, const int* groups, const int* prefix_rank, int G,
+                             unsigned* bits, int* first) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int g = groups[size_t(i) * depth + k];
+    const int pr = k == 0 ? 0 : prefix_rank[i];
+    if (g < 0 || pr < 0) {
+        first[i] = 0;
+        return;
+    }
+    const long long key = (long long)pr * G + g;
+    const unsigned bit = 1u << unsigned(key & 31);
+    const unsigned old = atomicOr(bits + (key >> 5), bit);
+    first[i] = (old & bit) == 0u;
+}
+
+__global__ void k_word_popc(long long words, const unsigned* bits, int* out) {
+    const long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (w < words) out[w] = __popc(bits[w]);
+}
+
+__global__ void k_chain_bits_emit(int count, int depth, int k, const int* groups, int* rank_io, int G,
+                                  const unsigned* bits, const int* word_prefix, const int* first, int* chain_groups,
+                                  int chain_cap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int g = groups[size_t(i) * depth + k];
+    const int pr = k == 0 ? 0 : rank_io[i];
+    if (g < 0 || pr < 0) {
+        rank_io[i] = -1;
+        return;
+    }
+    const long long key = (long long)pr * G + g;
+    const long long w = key >> 5;
+    const int rank = word_prefix[w] + __popc(bits[w] & ((1u << unsigned(key & 31)) - 1u));
+    rank_io[i] = rank;
+    if (chain_groups != nullptr && first[i] && rank < chain_cap) {
+        for (int c = 0; c <= k; ++c) chain_groups[size_t(rank) * (k + 1) + c] = groups[size_t(i) * depth + c];
+    }
+}
+
+__global__ void k_chain_bits_count(long long words, const unsigned* bits, const int* word_prefix, int chain_cap,
+                                   int* chain_count) {
+    const int total = word_prefix[words - 1] + __popc(bits[words - 1]);
+    *chain_count = min(total, chain_cap);
+}
+
 // exhaustive adjacent-distinct sequences (paths.cu:364-406)
 __global__ void k_exhaustive_chains(long long total, int depth, int groups_n, int* chain_groups) {
     long long row = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -447,6 +500,35 @@ struct ChainPlan {
     long long offset_int[kMaxDepth];
 };
 
+// Chain keys held in a bitmap when their space (prefix ranks x groups) is at
+// most this many bits (8 MiB).  The environment variable
+// WCB_CHAIN_BITMAP_BITS lowers the limit (0 keeps every depth on the sort;
+// tests compare the two forms).
+constexpr long long kChainBitmapBits = 1ll << 26;
+
+static long long chain_bitmap_limit() {
+    const char* v = std::getenv("WCB_CHAIN_BITMAP_BITS");
+    if (v != nullptr) {
+        const long long n = std::atoll(v);
+        if (n >= 0 && n < kChainBitmapBits) return n;
+    }
+    return kChainBitmapBits;
+}
+
+// Size of the key space of depth k (0-based): the prefix chains at depth k-1
+// number at most min(rays, G^k); 0 when it exceeds the bitmap limit.
+static long long chain_key_bits(long long G, int rays, int k) {
+    const long long limit = chain_bitmap_limit();
+    if (G <= 0 || limit <= 0) return 0;
+    long long prefixes = 1;
+    for (int q = 0; q < k; ++q) {
+        if (prefixes > (long long)rays / G + 1) { prefixes = rays; break; }
+        prefixes = std::min<long long>(prefixes * G, rays);
+    }
+    if (prefixes > limit / G) return 0;
+    return prefixes * G;
+}
+
 // bits needed to hold 0..n (n >= 0)
 static int bit_width(long long n) {
     int b = 1;
@@ -491,7 +573,7 @@ static ChainPlan make_plan(const SceneDev& sc, int max_depth, int rays) {
 struct WorkspaceLayout {
     size_t chain_counts, chain_offsets, chain_groups, chain_planes, chain_images, chain_pre;
     size_t disc_dirs, disc_groups, disc_keys, disc_keys2, disc_vals, disc_vals2, disc_flags, disc_scan, disc_rank,
-        disc_temp;
+        disc_temp, disc_bits, disc_word_count, disc_word_prefix;
     size_t disc_temp_bytes;
     size_t edge_flags, edge_list, edge_count;
     size_t diff_words, diff_carry;
@@ -526,13 +608,25 @@ static WorkspaceLayout layout_for(const SceneDev& sc, const wcb_solve_desc& d, c
     L.disc_flags = take(nr * 4);
     L.disc_scan = take(nr * 4);
     L.disc_rank = take(nr * 4);
+    // bitmap dedup: the largest key space any depth uses in that form
+    long long max_bits = 0;
+    if (nr)
+        for (int k = 0; k < md; ++k) {
+            const long long kb = chain_key_bits(sc.num_groups, int(nr), k);
+            if (kb > 0) max_bits = std::max(max_bits, kb);
+        }
+    const size_t bm_words = size_t((max_bits + 31) / 32);
+    L.disc_bits = take(bm_words * 4);
+    L.disc_word_count = take(bm_words * 4);
+    L.disc_word_prefix = take(bm_words * 4);
     size_t tb = 0;
     if (nr) {
-        size_t a = 0, b = 0;
+        size_t a = 0, b = 0, c = 0;
         cub::DeviceRadixSort::SortPairs(nullptr, a, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
                                         (int*)nullptr, (int*)nullptr, int(nr), 0, 64);
         cub::DeviceScan::InclusiveSum(nullptr, b, (int*)nullptr, (int*)nullptr, int(nr));
-        tb = std::max(a, b);
+        if (bm_words) cub::DeviceScan::ExclusiveSum(nullptr, c, (int*)nullptr, (int*)nullptr, int(bm_words));
+        tb = std::max(a, std::max(b, c));
     }
     L.disc_temp_bytes = tb;
     L.disc_temp = take(tb);
@@ -657,6 +751,28 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                     const int depth = k + 1;
                     const bool use_disc = depth == 1 ? !pl.exhaustive_o1 : !pl.exhaustive_mb;
                     // ranks are needed for the next depth even when this depth is exhaustive
+                    int* cgrp = use_disc ? chain_groups + offs[t * kMaxDepth + k] : nullptr;
+                    int* ccount = use_disc ? chain_counts + t * kMaxDepth + k : nullptr;
+                    const long long kbits = chain_key_bits(sc.num_groups, rays, k);
+                    if (kbits > 0) {
+                        // small key space: bitmap dedup
+                        const long long words = (kbits + 31) / 32;
+                        unsigned* bits = reinterpret_cast<unsigned*>(base + L.disc_bits);
+                        int* wpre = reinterpret_cast<int*>(base + L.disc_word_prefix);
+                        int* wcnt = reinterpret_cast<int*>(base + L.disc_word_count);
+                        cudaMemsetAsync(bits, 0, size_t(words) * 4, side);
+                        k_chain_bits<<<(rays + B - 1) / B, B, 0, side>>>(rays, md, k, dg, rank, sc.num_groups, bits,
+                                                                         flags);
+                        k_word_popc<<<unsigned((words + B - 1) / B), B, 0, side>>>(words, bits, wcnt);
+                        size_t tb = L.disc_temp_bytes;
+                        cub::DeviceScan::ExclusiveSum(temp, tb, wcnt, wpre, int(words), side);
+                        k_chain_bits_emit<<<(rays + B - 1) / B, B, 0, side>>>(rays, md, k, dg, rank, sc.num_groups,
+                                                                              bits, wpre, flags, cgrp,
+                                                                              use_disc ? int(pl.cap[k]) : 0);
+                        if (ccount) k_chain_bits_count<<<1, 1, 0, side>>>(words, bits, wpre, int(pl.cap[k]), ccount);
+                        note_launch(ccount ? 5 : 4);
+                        continue;
+                    }
                     k_chain_keys<<<(rays + B - 1) / B, B, 0, side>>>(rays, md, k, dg, rank, gbits, keys, vals);
                     size_t tb = L.disc_temp_bytes;
                     // only the key's used bits (+1 so the ~0 of a missing hit stays above)
@@ -664,8 +780,6 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                     k_chain_flags<<<(rays + B - 1) / B, B, 0, side>>>(rays, keys2, flags);
                     tb = L.disc_temp_bytes;
                     cub::DeviceScan::InclusiveSum(temp, tb, flags, scan, rays, side);
-                    int* cgrp = use_disc ? chain_groups + offs[t * kMaxDepth + k] : nullptr;
-                    int* ccount = use_disc ? chain_counts + t * kMaxDepth + k : nullptr;
                     k_chain_emit<<<(rays + B - 1) / B, B, 0, side>>>(rays, md, k, keys2, vals2, flags, scan, dg, rank,
                                                                        cgrp, use_disc ? int(pl.cap[k]) : 0, ccount);
                     note_launch(3);
