@@ -210,17 +210,23 @@ def to_device(values: list, dtype: torch.dtype, device: torch.device) -> torch.T
 
 # compiled scenes keyed by the scene object's identity (scene types need not be
 # hashable); an entry dies with its scene through the weak reference's callback
-_CACHE: dict[int, tuple[Any, tuple, "CompiledScene"]] = {}
+_CACHE: dict[int, tuple[Any, tuple, "CompiledScene", list]] = {}
 
 
-def _geometry_token(scene: Any) -> tuple:
+def _geometry_token(scene: Any) -> tuple[tuple, list]:
+    """Identity and in-place version of every structure's geometry and
+    material, plus the objects themselves: the cache entry keeps them alive,
+    so an id in a stored token cannot be reused by a replacement object."""
+    refs: list = []
     parts = []
     for st in scene.structures:
-        v = st.vertices
-        parts.append((id(v), getattr(v, "_version", 0), tuple(v.shape), id(st.faces), id(st.material),
-                      st.surface_id))
-    parts.append(tuple(sorted((k, id(v)) for k, v in getattr(scene, "metadata", {}).items())))
-    return tuple(parts)
+        g = getattr(st, "geometry", st)
+        v, f, m = g.vertices, g.faces, st.material
+        refs.append((v, f, m))
+        parts.append((id(v), getattr(v, "_version", 0), id(f), id(m), st.surface_id))
+    md = getattr(scene, "metadata", None)
+    parts.append(tuple(sorted((k, id(x)) for k, x in md.items())) if md else ())
+    return tuple(parts), refs
 
 
 def compile_scene(scene: Any, device: torch.device | None = None) -> CompiledScene:
@@ -228,7 +234,7 @@ def compile_scene(scene: Any, device: torch.device | None = None) -> CompiledSce
 
     if device is None or (device.type == "cuda" and device.index is None):
         device = torch.device("cuda", torch.cuda.current_device())
-    token = _geometry_token(scene)
+    token, refs = _geometry_token(scene)
     scene_key = id(scene)
     cached = _CACHE.get(scene_key)
     if cached is not None and cached[0] is not None and cached[0]() is scene and cached[1] == token \
@@ -275,7 +281,7 @@ def compile_scene(scene: Any, device: torch.device | None = None) -> CompiledSce
     except TypeError:  # not weak-referenceable: compile on every call
         ref = None
     if ref is not None:
-        _CACHE[scene_key] = (ref, token, compiled)
+        _CACHE[scene_key] = (ref, token, compiled, refs)
     return compiled
 
 
