@@ -65,13 +65,28 @@ WCB_D Ray<G> make_ray(V3<G> o, V3<G> d, G tmin, G tmax) {
     return r;
 }
 
+// Three-operand min/max (PTX ISA, sm_100a): the same value as two nested
+// two-operand ones, in one instruction.
+WCB_D float fmax3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+WCB_D float fmin3(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+WCB_D double fmax3(double a, double b, double c) { return fmax(fmax(a, b), c); }
+WCB_D double fmin3(double a, double b, double c) { return fmin(fmin(a, b), c); }
+
 template <typename G>
 WCB_D bool box_hit(const Ray<G>& r, G lx, G ly, G lz, G hx, G hy, G hz, G tmax, G* tnear) {
     G t0x = (lx - r.o.x) * r.inv.x, t1x = (hx - r.o.x) * r.inv.x;
     G t0y = (ly - r.o.y) * r.inv.y, t1y = (hy - r.o.y) * r.inv.y;
     G t0z = (lz - r.o.z) * r.inv.z, t1z = (hz - r.o.z) * r.inv.z;
-    G tn = s_max(s_max(s_min(t0x, t1x), s_min(t0y, t1y)), s_max(s_min(t0z, t1z), r.tmin));
-    G tf = s_min(s_min(s_max(t0x, t1x), s_max(t0y, t1y)), s_min(s_max(t0z, t1z), tmax));
+    G tn = fmax3(s_min(t0x, t1x), s_min(t0y, t1y), s_max(s_min(t0z, t1z), r.tmin));
+    G tf = fmin3(s_max(t0x, t1x), s_max(t0y, t1y), s_min(s_max(t0z, t1z), tmax));
     // conservative widening (Ize, "Robust BVH ray traversal", 2013)
     tf = tf * (sizeof(G) == 4 ? G(1.0000004) : G(1.000000000000001));
     *tnear = tn;
