@@ -22,6 +22,40 @@ constexpr double kUtdEps = 1.0e-10;       // field kernels' length floor
 constexpr double kUtdSmallEps = 1.0e-6;   // field kernels' normalisation floor
 
 // ---------------------------------------------------------------- scalars
+// Out-of-line copies of the longer math-library routines.  Every call site of
+// sin, cos, sincos, exp (FP64), atan2, acos or hypot would otherwise inline
+// the whole routine, and the special-function-heavy kernels (the UTD and its
+// dual-number derivative) then no longer fit the instruction cache; a call
+// site now branches to the one copy its translation unit holds.  Device code
+// only; the values are the library's own.
+#ifdef __CUDA_ARCH__
+namespace ool {
+struct SinCosD { double s, c; };
+struct SinCosF { float s, c; };
+__device__ __noinline__ inline double sin_d(double x) { return ::sin(x); }
+__device__ __noinline__ inline double cos_d(double x) { return ::cos(x); }
+__device__ __noinline__ inline SinCosD sincos_d(double x) {
+    SinCosD r;
+    ::sincos(x, &r.s, &r.c);
+    return r;
+}
+__device__ __noinline__ inline double exp_d(double x) { return ::exp(x); }
+__device__ __noinline__ inline double atan2_d(double y, double x) { return ::atan2(y, x); }
+__device__ __noinline__ inline double acos_d(double x) { return ::acos(x); }
+__device__ __noinline__ inline double hypot_d(double a, double b) { return ::hypot(a, b); }
+__device__ __noinline__ inline float sin_f(float x) { return ::sinf(x); }
+__device__ __noinline__ inline float cos_f(float x) { return ::cosf(x); }
+__device__ __noinline__ inline SinCosF sincos_f(float x) {
+    SinCosF r;
+    ::sincosf(x, &r.s, &r.c);
+    return r;
+}
+__device__ __noinline__ inline float atan2_f(float y, float x) { return ::atan2f(y, x); }
+}  // namespace ool
+#define WCB_MATH(dev, host) dev
+#else
+#define WCB_MATH(dev, host) host
+#endif
 WCB_HD float s_sqrt(float x) { return sqrtf(x); }
 WCB_HD double s_sqrt(double x) { return sqrt(x); }
 WCB_HD float s_abs(float x) { return fabsf(x); }
@@ -31,15 +65,16 @@ WCB_HD double s_max(double a, double b) { return fmax(a, b); }
 WCB_HD float s_min(float a, float b) { return fminf(a, b); }
 WCB_HD double s_min(double a, double b) { return fmin(a, b); }
 WCB_HD float s_exp(float x) { return expf(x); }
-WCB_HD double s_exp(double x) { return exp(x); }
-WCB_HD float s_cos(float x) { return cosf(x); }
-WCB_HD double s_cos(double x) { return cos(x); }
-WCB_HD float s_sin(float x) { return sinf(x); }
-WCB_HD double s_sin(double x) { return sin(x); }
-WCB_HD float s_atan2(float y, float x) { return atan2f(y, x); }
-WCB_HD double s_atan2(double y, double x) { return atan2(y, x); }
+WCB_HD double s_exp(double x) { return WCB_MATH(ool::exp_d(x), exp(x)); }
+WCB_HD float s_cos(float x) { return WCB_MATH(ool::cos_f(x), cosf(x)); }
+WCB_HD double s_cos(double x) { return WCB_MATH(ool::cos_d(x), cos(x)); }
+WCB_HD float s_sin(float x) { return WCB_MATH(ool::sin_f(x), sinf(x)); }
+WCB_HD double s_sin(double x) { return WCB_MATH(ool::sin_d(x), sin(x)); }
+WCB_HD float s_atan2(float y, float x) { return WCB_MATH(ool::atan2_f(y, x), atan2f(y, x)); }
+WCB_HD double s_atan2(double y, double x) { return WCB_MATH(ool::atan2_d(y, x), atan2(y, x)); }
 WCB_HD float s_hypot(float a, float b) { return hypotf(a, b); }
-WCB_HD double s_hypot(double a, double b) { return hypot(a, b); }
+WCB_HD double s_hypot(double a, double b) { return WCB_MATH(ool::hypot_d(a, b), hypot(a, b)); }
+WCB_HD double s_acos(double a) { return WCB_MATH(ool::acos_d(fmin(fmax(a, -1.0), 1.0)), acos(fmin(fmax(a, -1.0), 1.0))); }
 WCB_HD float s_floor(float x) { return floorf(x); }
 WCB_HD double s_floor(double x) { return floor(x); }
 WCB_HD float s_round(float x) { return rintf(x); }
@@ -48,14 +83,18 @@ WCB_HD double value_of(double x) { return x; }
 WCB_HD float value_of(float x) { return x; }
 WCB_HD void s_sincos(float x, float* s, float* c) {
 #ifdef __CUDA_ARCH__
-    sincosf(x, s, c);
+    const ool::SinCosF r = ool::sincos_f(x);
+    *s = r.s;
+    *c = r.c;
 #else
     *s = sinf(x); *c = cosf(x);
 #endif
 }
 WCB_HD void s_sincos(double x, double* s, double* c) {
 #ifdef __CUDA_ARCH__
-    sincos(x, s, c);
+    const ool::SinCosD r = ool::sincos_d(x);
+    *s = r.s;
+    *c = r.c;
 #else
     *s = sin(x); *c = cos(x);
 #endif

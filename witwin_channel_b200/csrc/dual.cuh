@@ -133,29 +133,32 @@ template <int N>
 WCB_HD Dual<N> s_min(const Dual<N>& a, double b) { return a.v <= b ? a : Dual<N>(b); }
 template <int N>
 WCB_HD Dual<N> s_exp(const Dual<N>& a) {
-    const double e = exp(a.v);
+    const double e = s_exp(a.v);
     return chain(e, e, a);
 }
 template <int N>
-WCB_HD Dual<N> s_cos(const Dual<N>& a) { return chain(cos(a.v), -sin(a.v), a); }
+WCB_HD Dual<N> s_cos(const Dual<N>& a) {
+    double sv, cv;
+    s_sincos(a.v, &sv, &cv);
+    return chain(cv, -sv, a);
+}
 template <int N>
-WCB_HD Dual<N> s_sin(const Dual<N>& a) { return chain(sin(a.v), cos(a.v), a); }
+WCB_HD Dual<N> s_sin(const Dual<N>& a) {
+    double sv, cv;
+    s_sincos(a.v, &sv, &cv);
+    return chain(sv, cv, a);
+}
 template <int N>
 WCB_HD void s_sincos(const Dual<N>& a, Dual<N>* s, Dual<N>* c) {
     double sv, cv;
-#ifdef __CUDA_ARCH__
-    sincos(a.v, &sv, &cv);
-#else
-    sv = sin(a.v);
-    cv = cos(a.v);
-#endif
+    s_sincos(a.v, &sv, &cv);
     *s = chain(sv, cv, a);
     *c = chain(cv, -sv, a);
 }
 template <int N>
 WCB_HD Dual<N> s_atan2(const Dual<N>& y, const Dual<N>& x) {
     Dual<N> r;
-    r.v = atan2(y.v, x.v);
+    r.v = s_atan2(y.v, x.v);
     const double den = x.v * x.v + y.v * y.v;
     const double gx = den > 0.0 ? -y.v / den : 0.0;
     const double gy = den > 0.0 ? x.v / den : 0.0;
@@ -166,7 +169,7 @@ WCB_HD Dual<N> s_atan2(const Dual<N>& y, const Dual<N>& x) {
 template <int N>
 WCB_HD Dual<N> s_hypot(const Dual<N>& a, const Dual<N>& b) {
     Dual<N> r;
-    r.v = hypot(a.v, b.v);
+    r.v = s_hypot(a.v, b.v);
     const double ga = r.v > 0.0 ? a.v / r.v : 0.0;
     const double gb = r.v > 0.0 ? b.v / r.v : 0.0;
 #pragma unroll
@@ -182,9 +185,8 @@ template <int N>
 WCB_HD Dual<N> s_acos(const Dual<N>& a) {
     const double x = fmin(fmax(a.v, -1.0), 1.0);
     const double den = sqrt(fmax(1.0 - x * x, 0.0));
-    return chain(acos(x), (den > 0.0 && fabs(a.v) < 1.0) ? -1.0 / den : 0.0, a);
+    return chain(s_acos(x), (den > 0.0 && fabs(a.v) < 1.0) ? -1.0 / den : 0.0, a);
 }
-WCB_HD double s_acos(double a) { return acos(fmin(fmax(a, -1.0), 1.0)); }
 
 // exp(-j k d) with the product reduced mod 2*pi on the value (a constant
 // shift, so the tangents are those of -k*d).
