@@ -204,6 +204,13 @@ __global__ void k_chain_bits(int count, int depth, int k, const int* groups, con
     }
     const long long key = (long long)pr * G + g;
     const unsigned bit = 1u << unsigned(key & 31);
+    // most keys are already set by a ray of the same chain: read first (bits
+    // are only ever set, so a set bit read here is final) and take the
+    // atomic only for keys not seen set
+    if (__ldcg(bits + (key >> 5)) & bit) {
+        first[i] = 0;
+        return;
+    }
     const unsigned old = atomicOr(bits + (key >> 5), bit);
     first[i] = (old & bit) == 0u;
 }
