@@ -204,15 +204,16 @@ __global__ void k_chain_bits(int count, int depth, int k, const int* groups, con
     }
     const long long key = (long long)pr * G + g;
     const unsigned bit = 1u << unsigned(key & 31);
-    // most keys are already set by a ray of the same chain: read first (bits
-    // are only ever set, so a set bit read here is final) and take the
-    // atomic only for keys not seen set
-    if (__ldcg(bits + (key >> 5)) & bit) {
-        first[i] = 0;
-        return;
-    }
-    const unsigned old = atomicOr(bits + (key >> 5), bit);
-    first[i] = (old & bit) == 0u;
+    // one lane per distinct key of the warp (neighbouring rays share chains);
+    // it reads the word first (bits are only ever set, so a set bit read here
+    // is final) and takes the atomic only for a key not seen set
+    const unsigned same = __match_any_sync(__activemask(), key);
+    const int leader = __ffs(same) - 1;
+    const int lane = threadIdx.x & 31;
+    unsigned old = bit;
+    if (lane == leader && !(__ldcg(bits + (key >> 5)) & bit)) old = atomicOr(bits + (key >> 5), bit);
+    old = __shfl_sync(same, old, leader);
+    first[i] = lane == leader && (old & bit) == 0u;
 }
 
 __global__ void k_word_popc(long long words, const unsigned* bits, int* out) {
