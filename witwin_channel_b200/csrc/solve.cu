@@ -101,7 +101,7 @@ static void fibonacci_bands(int count, int* band, int* inv) {
 }
 
 template <typename G>
-__global__ void __launch_bounds__(kBlock) k_discovery_trace(SceneDev sc, int count, int depth, const float* dirs,
+__global__ void __launch_bounds__(kBlock, sizeof(G) == 4 ? 8 : 4) k_discovery_trace(SceneDev sc, int count, int depth, const float* dirs,
                                                             const float* tx, int* groups_out, int* err,
                                                             unsigned long long* ray_counter) {
     extern __shared__ int stack[];
@@ -709,7 +709,9 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         for (int k = 0; k < kMaxDepth; ++k) offs[t * kMaxDepth + k] = t * L.chain_ints_per_tx + pl.offset_int[k];
     cudaMemcpyAsync(chain_offsets, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, stream);
     const int B = 256;
-    const size_t smem = size_t(kStackDepth) * kBlock * 4;
+    // traversal stacks: a descent pushes at most one entry per tree level, so
+    // the measured BVH depth (+2) bounds them
+    const size_t smem = size_t(std::max(8, std::min(kStackDepth, sc.max_depth + 2))) * kBlock * 4;
     int* err = out->status;
     // The reflection candidates (discovery, chain tables) and the reflection
     // kernel run on a side stream, overlapping the edge prefilter, the LoS and
