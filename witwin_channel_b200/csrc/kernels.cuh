@@ -299,7 +299,7 @@ WCB_D int queue_pop_faces(int* q, int* qfaces, int size, int n, int lane) {
 // and leave after one traversal instead of idling while a visible path of
 // the same batch traces its remaining segments and its field.
 template <typename T, int NF>
-__global__ void __launch_bounds__(kSplitBlock, 2) k_reflect(MainParams p, int stack_depth) {
+__global__ void __launch_bounds__(kSplitBlock, sizeof(T) == 4 ? 3 : 2) k_reflect(MainParams p, int stack_depth) {
     extern __shared__ int smem[];
     int* stack = smem;
     const int lane = threadIdx.x & 31;
