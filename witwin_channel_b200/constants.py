@@ -37,12 +37,23 @@ PHASE_CONVENTION = {
 
 NARROWBAND_FREQUENCY_OFFSET_LAW = "H(f_ref+df) = C(f_ref)*exp(-j*2*pi*df*delay_s)"
 
+# The cost of the narrowband law as published by the reference consumer
+# contract (witwin/channel/constants.py:70-75): free-space spreading, the slab
+# fringe scale of the material response, and the dispersion the law drops.
+NARROWBAND_FREQUENCY_OFFSET_ERROR_LAW = (
+    "relative_error = O(df/f_ref) spreading"
+    " + O(df/df_fringe) material"
+    " + zeroth_order dispersion;"
+    " df_fringe = c/(2*Re(sqrt(eps_r))*thickness_m*cos(theta_t))"
+)
+
 __all__ = [
     "C0",
     "EPS0",
     "ETA0",
     "FREE_SPACE_AMPLITUDE",
     "MU0",
+    "NARROWBAND_FREQUENCY_OFFSET_ERROR_LAW",
     "NARROWBAND_FREQUENCY_OFFSET_LAW",
     "PEC_EFFECTIVE_SIGMA_E",
     "PHASE_CONVENTION",
