@@ -324,6 +324,23 @@ int wcb_field_transmission_sequence(int64_t n, int32_t depth, const float* sourc
 int wcb_field_project_complex3(int64_t n, const float* field_vector, const float* direction, const float* rx_pol,
                                float* coefficient, float* path_gain, void* stream);
 
+/* Line-of-sight Jones operator between per-endpoint transverse frames
+ * (replaces consumer_los_jones, witwin/channel/propagation/consumer.py:2037-2093,
+ * and its kernel native/channel/kernels/los.cu:2001-2078).  Row i takes pair
+ * p = pair_index[i]: source p % num_sources, sink p / num_sources.  Reference
+ * bases are (num_sources,2,3) and (num_sinks,2,3) f32; each endpoint's frame
+ * is its first vector made transverse to the LoS direction and unit, and
+ * direction x that vector turned to the side of its second vector.  Outputs
+ * (N rows): matrix (N,2,2) complex64 interleaved, matrix[i][a][b] the
+ * unit-excitation response of sink frame vector a to source frame vector b;
+ * source_basis, sink_basis (N,2,3) the frames used.  A pair outside
+ * [0, num_sources*num_sinks) writes NaN to its row and sets bit 0 of *status
+ * (status may be NULL). */
+int wcb_los_jones(const int64_t* pair_index, int64_t num_rows, const float* source_positions, int64_t num_sources,
+                  const float* sink_positions, int64_t num_sinks, const float* source_reference_basis,
+                  const float* sink_reference_basis, double frequency_hz, float* matrix, float* source_basis,
+                  float* sink_basis, int32_t* status, void* stream);
+
 /* Measurement: when enabled, wcb_solve brackets its candidate preparation and
  * its main kernel with CUDA events on the solve stream and counts the rays
  * (segment visibility / penetration queries) the main kernel traces.

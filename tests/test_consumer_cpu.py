@@ -36,12 +36,13 @@ def test_capability_record_is_frozen_and_truthful():
     assert caps is c.capabilities()
     assert caps.contract_version == c.CONTRACT_VERSION == 6
     assert caps.components == c.COMPONENTS == frozenset({"los", "reflection", "transmission", "diffraction"})
-    assert caps.responses == frozenset({"scalar_transport", "complex3_transport"})
-    assert caps.responses < c.RESPONSES
+    assert caps.responses == c.RESPONSES
     assert caps.ad_modes == frozenset({"none"})
     for response in caps.responses:
-        assert caps.components_for(response) == c.COMPONENTS
+        want = frozenset({"los"}) if response == "polarimetric_transport" else c.COMPONENTS
+        assert caps.components_for(response) == want
         assert caps.ad_modes_for(response) == frozenset({"none"})
+    assert caps.supports_los_jones
     for component in c.COMPONENTS:
         assert caps.ad_modes_for_component(component) == frozenset({"none"})
     assert caps.material_leaves_for("los") == ()
@@ -149,3 +150,19 @@ def test_interaction_flags_follow_the_reference_law(width):
     got = c._interaction_types(comps, depth, width)
     assert got.dtype == torch.int32 and tuple(got.shape) == (64, width)
     assert got.tolist() == _interaction_flags_restated(comps.tolist(), depth.tolist(), width)
+
+
+def test_los_jones_input_checks_before_any_launch():
+    pair = torch.zeros(1, dtype=torch.int64)
+    pos = torch.zeros((1, 3), dtype=torch.float32)
+    basis = torch.zeros((1, 2, 3), dtype=torch.float32)
+    kw = dict(pair_index=pair, source_positions=pos, sink_positions=pos, source_reference_basis=basis,
+              sink_reference_basis=basis, frequency_hz=1.0e9)
+    with pytest.raises(TypeError):
+        c.consumer_los_jones(**{**kw, "pair_index": [0]})
+    with pytest.raises(RuntimeError, match="does not support AD"):
+        c.consumer_los_jones(**{**kw, "source_positions": pos.clone().requires_grad_()})
+    with pytest.raises(TypeError):
+        c.consumer_los_jones(**{**kw, "pair_index": pair.int()})
+    with pytest.raises(ValueError, match="CUDA"):
+        c.consumer_los_jones(**kw)

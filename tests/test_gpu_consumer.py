@@ -192,3 +192,106 @@ def test_empty_batches_and_refusals():
         c.evaluate(scene, _request(sources, sinks, freq, {"los"}, 0))
     with pytest.raises(ValueError):
         _request(sinks, sinks, freq, {"los"}, 0)  # a source batch needs powers_w
+
+
+def _free_space_scalar(frequency_hz: float, distance_m: float) -> complex:
+    k = 2.0 * math.pi * frequency_hz / C0
+    return complex(math.cos(-k * distance_m), math.sin(-k * distance_m)) / (2.0 * k * distance_m)
+
+
+def test_los_jones_rotated_basis_closed_form():
+    """Source frame (x, y), sink frame (y, -x) on a link along +z: the operator
+    is [[0, s], [-s, 0]] with s the free-space scalar (the reference's analytic
+    case, ``tests/propagation/consumer/test_los_jones.py``)."""
+    dev = torch.device("cuda", 0)
+    rows = c.consumer_los_jones(
+        pair_index=torch.tensor([0], dtype=torch.int64, device=dev),
+        source_positions=torch.tensor([[0.0, 0.0, 0.0]], device=dev),
+        sink_positions=torch.tensor([[0.0, 0.0, 2.0]], device=dev),
+        source_reference_basis=torch.tensor([[[1.0, 0.0, 0.0], [0.0, 1.0, 0.0]]], device=dev),
+        sink_reference_basis=torch.tensor([[[0.0, 1.0, 0.0], [-1.0, 0.0, 0.0]]], device=dev),
+        frequency_hz=1.0e9)
+    s = _free_space_scalar(1.0e9, 2.0)
+    want = torch.tensor([[[0.0j, s], [-s, 0.0j]]], dtype=torch.complex64, device=dev)
+    torch.testing.assert_close(rows.matrix, want, rtol=2.0e-5, atol=2.0e-7)
+    torch.testing.assert_close(rows.source_basis.cpu(), torch.tensor([[[1.0, 0.0, 0.0], [0.0, 1.0, 0.0]]]))
+    torch.testing.assert_close(rows.sink_basis.cpu(), torch.tensor([[[0.0, 1.0, 0.0], [-1.0, 0.0, 0.0]]]))
+    assert rows.native_launch_count == 1
+    empty = c.consumer_los_jones(
+        pair_index=torch.empty((0,), dtype=torch.int64, device=dev),
+        source_positions=torch.zeros((1, 3), device=dev), sink_positions=torch.ones((1, 3), device=dev),
+        source_reference_basis=torch.zeros((1, 2, 3), device=dev), sink_reference_basis=torch.zeros((1, 2, 3), device=dev),
+        frequency_hz=1.0e9)
+    assert tuple(empty.matrix.shape) == (0, 2, 2) and empty.native_launch_count == 0
+
+
+def test_los_jones_flags_a_pair_outside_the_batches():
+    dev = torch.device("cuda", 0)
+    with pytest.raises(IndexError):
+        c.consumer_los_jones(
+            pair_index=torch.tensor([0, 4], dtype=torch.int64, device=dev),
+            source_positions=torch.zeros((2, 3), device=dev), sink_positions=torch.ones((2, 3), device=dev),
+            source_reference_basis=torch.tensor([[[1.0, 0, 0], [0, 1.0, 0]]] * 2, device=dev),
+            sink_reference_basis=torch.tensor([[[1.0, 0, 0], [0, 1.0, 0]]] * 2, device=dev), frequency_hz=1.0e9)
+
+
+def _frame_restated(ref: np.ndarray, d: np.ndarray) -> np.ndarray:
+    first, second = ref[0], ref[1]
+    u = first - d * (first @ d)
+    u = u / np.linalg.norm(u)
+    v = np.cross(d, u)
+    v = v / np.linalg.norm(v)
+    return np.stack([u, -v if v @ second < 0 else v])
+
+
+def test_polarimetric_evaluate_matches_frames_and_scalar_response():
+    f = 3.5e9
+    dev = torch.device("cuda", 0)
+    g = torch.Generator().manual_seed(5)
+    src_pos = torch.tensor([[0.0, 0.0, 1.0], [1.0, -2.0, 3.0]])
+    snk_pos = torch.tensor([[7.0, 3.0, 1.5], [-4.0, 6.0, 2.0], [2.0, 9.0, -1.0]])
+    src_ref = torch.randn((2, 2, 3), generator=g)
+    snk_ref = torch.randn((3, 2, 3), generator=g)
+    src_pol = torch.randn((2, 3), generator=g)
+    snk_pol = torch.randn((3, 3), generator=g)
+
+    def batch(pos, pol, ref, ids, powers=None):
+        return c.EndpointBatch(stable_ids=torch.tensor(ids, dtype=torch.int64, device=dev),
+                               positions_m=pos.to(dev).contiguous(), polarizations=pol.to(dev).contiguous(),
+                               polarization_basis=ref.to(dev).contiguous(),
+                               powers_w=None if powers is None else torch.tensor(powers, device=dev))
+
+    sources = batch(src_pos, src_pol, src_ref, [1, 2], [1.0, 4.0])
+    sinks = batch(snk_pos, snk_pol, snk_ref, [7, 8, 9])
+    compiled = compile_scene(Scene(structures=[], endpoints=[]), dev)
+    out = c.evaluate(compiled, _request(sources, sinks, f, {"los"}, 0, response="polarimetric_transport"))
+    p = out.paths
+    assert p.path_count == 6 and isinstance(p.transport, c.JonesTransport)
+    scalar = c.evaluate(compiled, _request(sources, sinks, f, {"los"}, 0)).paths.transport.coefficient.cpu().numpy()
+    M = p.transport.matrix.cpu().numpy()
+    sb = p.transport.source_basis.cpu().numpy()
+    kb = p.transport.sink_basis.cpu().numpy()
+    for k in range(6):
+        t, r = int(p.topology.source_index[k]), int(p.topology.sink_index[k])
+        off = (snk_pos[r] - src_pos[t]).double().numpy()
+        dist = float(np.linalg.norm(off))
+        d = off / dist
+        fs = _frame_restated(src_ref[t].double().numpy(), d)
+        fk = _frame_restated(snk_ref[r].double().numpy(), d)
+        np.testing.assert_allclose(sb[k], fs, atol=2e-6)
+        np.testing.assert_allclose(kb[k], fk, atol=2e-6)
+        s = _free_space_scalar(f, dist)
+        np.testing.assert_allclose(M[k], s * (fk @ fs.T), rtol=0, atol=2e-5 * abs(s))
+        # the operator reproduces the scalar response of the endpoint polarisations
+        # (transverse parts in the two frames), times the source amplitude
+        a = fs @ src_pol[t].double().numpy()
+        b = fk @ snk_pol[r].double().numpy()
+        want = math.sqrt([1.0, 4.0][t]) * (b @ M[k].astype(np.complex128) @ a)
+        assert abs(scalar[k] - want) <= 1e-4 * abs(s) * math.sqrt([1.0, 4.0][t]) * (
+            np.linalg.norm(src_pol[t].numpy()) * np.linalg.norm(snk_pol[r].numpy()))
+    with pytest.raises(NotImplementedError):
+        c.evaluate(compiled, _request(sources, sinks, f, {"los", "reflection"}, 1, response="polarimetric_transport"))
+    no_basis = c.EndpointBatch(stable_ids=sinks.stable_ids, positions_m=sinks.positions_m,
+                               polarizations=sinks.polarizations)
+    with pytest.raises(ValueError):
+        c.evaluate(compiled, _request(sources, no_basis, f, {"los"}, 0, response="polarimetric_transport"))

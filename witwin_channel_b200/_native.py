@@ -156,6 +156,7 @@ EXPORTED_SYMBOLS = (
     "wcb_field_reflection_sequence",
     "wcb_field_transmission_sequence",
     "wcb_field_project_complex3",
+    "wcb_los_jones",
     "wcb_profile_enable",
     "wcb_profile_read",
     "wcb_build_info",
@@ -226,6 +227,8 @@ def load() -> ctypes.CDLL:
     lib.wcb_field_transmission_sequence.argtypes = [ctypes.c_int64, ctypes.c_int32] + [_vp] * 8 + [
         ctypes.POINTER(Materials), ctypes.c_double] + [_vp] * 7 + [_vp]
     lib.wcb_field_project_complex3.argtypes = [ctypes.c_int64] + [_vp] * 5 + [_vp]
+    lib.wcb_los_jones.argtypes = [_vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp, _vp,
+                                  ctypes.c_double, _vp, _vp, _vp, _vp, _vp]
     lib.wcb_profile_enable.argtypes = [ctypes.c_int32]
     lib.wcb_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double)]
     lib.wcb_build_info.argtypes = [ctypes.c_char_p, ctypes.c_int64]

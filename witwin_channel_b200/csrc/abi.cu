@@ -144,6 +144,22 @@ int wcb_field_free_space(int64_t n, const float* source, const float* target, co
                                  path_field, path_gain, path_length, delay, direction, as_stream(stream));
 }
 
+int wcb_los_jones(const int64_t* pair_index, int64_t num_rows, const float* source_positions, int64_t num_sources,
+                  const float* sink_positions, int64_t num_sinks, const float* source_reference_basis,
+                  const float* sink_reference_basis, double frequency_hz, float* matrix, float* source_basis,
+                  float* sink_basis, int32_t* status, void* stream) {
+    if (num_rows < 0 || !(frequency_hz > 0.0)) return WCB_ERR_INVALID_ARGUMENT;
+    if (num_rows == 0) return WCB_OK;
+    if (pair_index == nullptr || source_positions == nullptr || sink_positions == nullptr ||
+        source_reference_basis == nullptr || sink_reference_basis == nullptr || matrix == nullptr ||
+        source_basis == nullptr || sink_basis == nullptr || num_sources <= 0 || num_sinks <= 0 ||
+        num_sources > INT64_MAX / num_sinks)
+        return WCB_ERR_INVALID_ARGUMENT;
+    return wcb::los_jones(num_rows, pair_index, source_positions, num_sources, sink_positions, num_sinks,
+                          source_reference_basis, sink_reference_basis, frequency_hz, matrix, source_basis, sink_basis,
+                          status, as_stream(stream));
+}
+
 int wcb_field_reflection_sequence(int64_t n, int32_t depth, const float* source, const float* target,
                                   const float* positions, const float* normals, const float* tx_power,
                                   const float* tx_pol, const float* rx_pol, const float* eps_r, const float* sigma_e,

@@ -608,6 +608,74 @@ __global__ void k_field_project(long long n, const float* fv, const float* dir, 
     if (pg) pg[i] = cabs2(c);
 }
 
+// Transverse frame of one endpoint for the propagation direction `dir`
+// (consumer_los_jones, los.cu:1964-1980): u is the first reference vector made
+// transverse and unit (falling back to the transverse part of the second, then
+// to a fixed axis); v = dir x u, turned to the side of the second vector.
+WCB_D void endpoint_frame(const float* ref, long long e, V3<float> dir, V3<float>* u, V3<float>* v) {
+    const V3<float> first = v3(ref[6 * e], ref[6 * e + 1], ref[6 * e + 2]);
+    const V3<float> second = v3(ref[6 * e + 3], ref[6 * e + 4], ref[6 * e + 5]);
+    const V3<float> fallback = stable_perp_basis(dir, second);
+    const V3<float> fu = safe_normalize(transverse(dir, first), fallback);
+    V3<float> fv = safe_normalize(cross(dir, fu), fallback);
+    if (dot(fv, second) < 0.f) fv = fv * -1.f;
+    *u = fu;
+    *v = fv;
+}
+
+WCB_D void store_frame(float* dst, long long i, V3<float> u, V3<float> v) {
+    dst[6 * i] = u.x;
+    dst[6 * i + 1] = u.y;
+    dst[6 * i + 2] = u.z;
+    dst[6 * i + 3] = v.x;
+    dst[6 * i + 4] = v.y;
+    dst[6 * i + 5] = v.z;
+}
+
+// LoS Jones operator rows: row i takes pair p (source p % S, sink p / S),
+// evaluates the unit-excitation free-space field of both source frame
+// vectors (FP64 length and phase, as the LoS kernel) and projects each on
+// both sink frame vectors: matrix[i][a][b] = response of sink vector a to
+// source vector b.  A pair outside [0, S*R) writes NaN and sets status bit 0.
+__global__ void k_los_jones(long long n, const long long* pair, const float* src, long long num_src, const float* snk,
+                            long long num_snk, const float* src_ref, const float* snk_ref, double freq, float* matrix,
+                            float* src_basis, float* snk_basis, int* status) {
+    const long long stride = (long long)blockDim.x * gridDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
+        const long long p = pair[i];
+        if (p < 0 || p >= num_src * num_snk) {
+            const float nan = __int_as_float(0x7fc00000);
+            for (int j = 0; j < 8; ++j) matrix[8 * i + j] = nan;
+            for (int j = 0; j < 6; ++j) {
+                src_basis[6 * i + j] = nan;
+                snk_basis[6 * i + j] = nan;
+            }
+            if (status) atomicOr(status, 1);
+            continue;
+        }
+        const long long t = p % num_src;
+        const long long r = p / num_src;
+        const V3<double> S = v3<double>(src[3 * t], src[3 * t + 1], src[3 * t + 2]);
+        const V3<double> R = v3<double>(snk[3 * r], snk[3 * r + 1], snk[3 * r + 2]);
+        const double k = kTwoPi * freq / kC0;
+        const double dist = length(R - S);
+        const V3<float> Sf = cast3<float>(S);
+        const V3<float> Rf = cast3<float>(R);
+        const V3<float> dir = safe_normalize(Rf - Sf, v3<float>(0.f, 0.f, 1.f));
+        V3<float> su, sv, ru, rv;
+        endpoint_frame(src_ref, t, dir, &su, &sv);
+        endpoint_frame(snk_ref, r, dir, &ru, &rv);
+        const PathEval<float> eu = eval_free_space(Sf, Rf, su, ru, k, dist);
+        const PathEval<float> ev = eval_free_space(Sf, Rf, sv, ru, k, dist);
+        store_c(matrix, 4 * i + 0, eu.coefficient);
+        store_c(matrix, 4 * i + 1, ev.coefficient);
+        store_c(matrix, 4 * i + 2, project_receiver(eu.field, eu.direction, rv));
+        store_c(matrix, 4 * i + 3, project_receiver(ev.field, ev.direction, rv));
+        store_frame(src_basis, i, su, sv);
+        store_frame(snk_basis, i, ru, rv);
+    }
+}
+
 }  // namespace
 
 int rows_evaluate(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m, int fi, const void* rows,
@@ -711,6 +779,18 @@ int field_transmission(int64_t n, int depth, const float* s, const float* t, con
 int field_project(int64_t n, const float* fv, const float* dir, const float* rp, float* c, float* pg, cudaStream_t stream) {
     if (n <= 0) return 0;
     k_field_project<<<int((n + kB - 1) / kB), kB, 0, stream>>>(n, fv, dir, rp, c, pg);
+    note_launch();
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int los_jones(int64_t n, const int64_t* pair, const float* src, int64_t num_src, const float* snk, int64_t num_snk,
+              const float* src_ref, const float* snk_ref, double f, float* matrix, float* src_basis, float* snk_basis,
+              int* status, cudaStream_t stream) {
+    if (n <= 0) return 0;
+    // grid-stride: at most 8 blocks of 256 per SM on the 148 SMs
+    const long long blocks = std::min<long long>((n + kB - 1) / kB, 148LL * 8);
+    k_los_jones<<<int(blocks), kB, 0, stream>>>(n, reinterpret_cast<const long long*>(pair), src, num_src, snk, num_snk,
+                                                src_ref, snk_ref, f, matrix, src_basis, snk_basis, status);
     note_launch();
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }

@@ -18,11 +18,12 @@ source_index``), and rows of one pair keep the canonical order.  The packing
 is index arithmetic on device tensors.
 
 What this engine advertises is what it does: components LoS, reflection,
-transmission and diffraction; the scalar and complex3 responses; AD mode
-"none".  The polarimetric (Jones) response, AD modes other than "none", the
-fixed-topology replay (``prepare_fixed_topology`` / ``reevaluate``), wideband
-offsets and the time-varying route are not advertised, and requests for them
-fail before any native work.
+transmission and diffraction; the scalar and complex3 responses, and the
+polarimetric (LoS Jones) response through the native ``wcb_los_jones``
+(``consumer_los_jones``, ``:2037-2093``); AD mode "none".  AD modes other than
+"none", the fixed-topology replay (``prepare_fixed_topology`` /
+``reevaluate``), wideband offsets and the time-varying route are not
+advertised, and requests for them fail before any native work.
 """
 
 from __future__ import annotations
@@ -66,8 +67,14 @@ WORLD_VERSION_DOMAINS: tuple[str, ...] = (
     "geometry_version",
 )
 
-# What this engine produces (a subset of the vocabulary above).
-_SUPPORTED_RESPONSES: frozenset[str] = frozenset({"scalar_transport", "complex3_transport"})
+# What this engine produces (a subset of the vocabulary above); the
+# polarimetric (Jones) response is line-of-sight only, as in the reference.
+_SUPPORTED_RESPONSES: frozenset[str] = RESPONSES
+_RESPONSE_COMPONENTS: tuple[tuple[str, frozenset[str]], ...] = (
+    ("complex3_transport", COMPONENTS),
+    ("polarimetric_transport", frozenset({"los"})),
+    ("scalar_transport", COMPONENTS),
+)
 _SUPPORTED_AD_MODES: frozenset[str] = frozenset({"none"})
 
 _COMPONENT_MATERIAL_LEAVES: tuple[tuple[str, tuple[str, ...]], ...] = (
@@ -378,8 +385,9 @@ class Complex3Transport:
 @dataclass(frozen=True, slots=True, eq=False)
 class JonesTransport:
     """Source-basis to sink-basis complex 2 x 2 operator (reference
-    ``consumer.py:878-913``).  The record is part of the contract; this engine
-    does not produce it (the polarimetric response is not advertised)."""
+    ``consumer.py:878-913``): ``matrix[k, i, j]`` is the response of sink
+    basis vector ``i`` to source basis vector ``j`` at unit excitation (no
+    transmitter power, no antenna pattern)."""
 
     matrix: torch.Tensor
     source_basis: torch.Tensor
@@ -525,13 +533,13 @@ _CAPABILITIES = PropagationCapabilities(
     ad_modes=_SUPPORTED_AD_MODES,
     world_motions=frozenset(),
     world_version_domains=WORLD_VERSION_DOMAINS,
-    response_components=tuple((response, COMPONENTS) for response in sorted(_SUPPORTED_RESPONSES)),
+    response_components=_RESPONSE_COMPONENTS,
     response_ad_modes=tuple((response, _SUPPORTED_AD_MODES) for response in sorted(_SUPPORTED_RESPONSES)),
     component_ad_modes=tuple((component, _SUPPORTED_AD_MODES) for component in sorted(COMPONENTS)),
     fixed_topology_components=frozenset(),
     fixed_topology_responses=frozenset(),
     supports_fixed_topology=False,
-    supports_los_jones=False,
+    supports_los_jones=True,
     fixed_topology_row_validity_components=frozenset(),
     polarimetric_frozen_ad_inputs=("tx_power", "mu_r", "source_basis", "sink_basis", "endpoint_polarizations"),
     supports_slot_batching=False,
@@ -593,6 +601,88 @@ class PropagationEvaluation:
     diagnostics: PropagationDiagnostics
 
 
+# --- LoS Jones operator -------------------------------------------------------------
+
+
+@dataclass(frozen=True, slots=True)
+class LoSJonesRows:
+    """Output of :func:`consumer_los_jones` (reference ``consumer.py:1798-1803``)."""
+
+    matrix: torch.Tensor
+    source_basis: torch.Tensor
+    sink_basis: torch.Tensor
+    native_launch_count: int
+
+
+def consumer_los_jones(*, pair_index: torch.Tensor, source_positions: torch.Tensor, sink_positions: torch.Tensor,
+                       source_reference_basis: torch.Tensor, sink_reference_basis: torch.Tensor,
+                       frequency_hz: float, _check_pairs: bool = True) -> LoSJonesRows:
+    """Primal LoS transport between row-specific transverse bases (reference
+    ``consumer.py:2037-2093``), one native ``wcb_los_jones`` launch.  Row ``k``
+    takes ``pair_index[k] = sink * source_count + source``.  A pair index out of
+    range raises ``IndexError`` after the launch (the kernel flags it; the
+    check reads one status word)."""
+
+    tensors = (pair_index, source_positions, sink_positions, source_reference_basis, sink_reference_basis)
+    if any(not isinstance(value, torch.Tensor) for value in tensors):
+        raise TypeError("LoS Jones inputs must be torch tensors")
+    if any(value.requires_grad for value in tensors):
+        raise RuntimeError("LoS Jones transport does not support AD")
+    pair = _require_tensor("pair_index", pair_index, dtype=torch.int64, ndim=1)
+    device = pair.device
+    if device.type != "cuda":
+        raise ValueError("LoS Jones inputs must be CUDA tensors")
+    src = _require_tensor("source_positions", source_positions, dtype=torch.float32, ndim=2, device=device)
+    snk = _require_tensor("sink_positions", sink_positions, dtype=torch.float32, ndim=2, device=device)
+    if src.shape[1:] != (3,) or snk.shape[1:] != (3,):
+        raise ValueError("source_positions and sink_positions must have shape (N, 3)")
+    S, R = int(src.shape[0]), int(snk.shape[0])
+    _require_tensor("source_reference_basis", source_reference_basis, dtype=torch.float32, shape=(S, 2, 3),
+                    device=device)
+    _require_tensor("sink_reference_basis", sink_reference_basis, dtype=torch.float32, shape=(R, 2, 3),
+                    device=device)
+    frequency = float(frequency_hz)
+    if not (frequency > 0.0 and math.isfinite(frequency)):
+        raise ValueError("frequency_hz must be a positive finite float")
+    N = int(pair.shape[0])
+    matrix = torch.empty((N, 2, 2), dtype=torch.complex64, device=device)
+    source_basis = torch.empty((N, 2, 3), dtype=torch.float32, device=device)
+    sink_basis = torch.empty((N, 2, 3), dtype=torch.float32, device=device)
+    if N == 0:
+        return LoSJonesRows(matrix=matrix, source_basis=source_basis, sink_basis=sink_basis, native_launch_count=0)
+    if S == 0 or R == 0:
+        raise IndexError("pair_index addresses an empty endpoint batch")
+    lib = _native.load()
+    status = torch.zeros(1, dtype=torch.int32, device=device)
+    keep = [x.contiguous() for x in (pair, src, snk, source_reference_basis, sink_reference_basis)]
+    with torch.cuda.device(device):
+        _native.check(lib.wcb_los_jones(_native.ptr(keep[0]), N, _native.ptr(keep[1]), S, _native.ptr(keep[2]), R,
+                                        _native.ptr(keep[3]), _native.ptr(keep[4]), frequency, _native.ptr(matrix),
+                                        _native.ptr(source_basis), _native.ptr(sink_basis), _native.ptr(status),
+                                        _native.stream_handle(device)), "wcb_los_jones")
+    if _check_pairs and int(status.item()) != 0:
+        raise IndexError(f"pair_index outside [0, {S * R})")
+    return LoSJonesRows(matrix=matrix, source_basis=source_basis, sink_basis=sink_basis, native_launch_count=1)
+
+
+def _require_polarimetric_inputs(request: PropagationRequest) -> None:
+    """The polarimetric response needs both reference bases and takes them,
+    the powers and the polarizations as primal-only (reference
+    ``consumer.py:3186-3244``)."""
+
+    if request.sources.polarization_basis is None or request.sinks.polarization_basis is None:
+        raise ValueError("polarimetric_transport requires source and sink polarization_basis tensors")
+    for name, value in (("sources.polarization_basis", request.sources.polarization_basis),
+                        ("sinks.polarization_basis", request.sinks.polarization_basis),
+                        ("sources.powers_w", request.sources.powers_w),
+                        ("sources.polarizations", request.sources.polarizations),
+                        ("sinks.polarizations", request.sinks.polarizations),
+                        ("sources.positions_m", request.sources.positions_m),
+                        ("sinks.positions_m", request.sinks.positions_m)):
+        if value is not None and value.requires_grad:
+            raise NotImplementedError(f"polarimetric_transport {name} is primal-only")
+
+
 # --- evaluate ---------------------------------------------------------------------
 
 
@@ -613,6 +703,8 @@ def _preflight(compiled: object, request: object) -> float:
                                   f"{sorted(request.components - response_components)}")
     if request.ad_mode not in _CAPABILITIES.ad_modes_for(request.response):
         raise NotImplementedError(f"{request.response} does not support AD mode {request.ad_mode!r}")
+    if request.response == "polarimetric_transport":
+        _require_polarimetric_inputs(request)
     frequency = request.reference_frequency_hz
     if isinstance(frequency, torch.Tensor) and frequency.requires_grad:
         raise NotImplementedError("a differentiable reference frequency needs an AD mode this engine does not offer")
@@ -712,6 +804,15 @@ def evaluate(compiled_scene: CompiledScene, request: PropagationRequest) -> Prop
         )
         if request.response == "scalar_transport":
             transport: PropagationTransport = ScalarTransport(coefficient=take(ev["path_field"], torch.complex64))
+        elif request.response == "polarimetric_transport":
+            # LoS rows only (preflighted): one fused launch over the compact pairs
+            jones = consumer_los_jones(pair_index=pair_index, source_positions=sources.positions_m,
+                                       sink_positions=sinks.positions_m,
+                                       source_reference_basis=sources.polarization_basis,
+                                       sink_reference_basis=sinks.polarization_basis, frequency_hz=frequency,
+                                       _check_pairs=False)
+            transport = JonesTransport(matrix=jones.matrix, source_basis=jones.source_basis,
+                                       sink_basis=jones.sink_basis)
         else:
             # the row kernel's complex3 vector is at unit excitation; the
             # published field carries the source amplitude sqrt(powers_w)
@@ -751,6 +852,7 @@ __all__ = [
     "Complex3Transport",
     "EndpointBatch",
     "JonesTransport",
+    "LoSJonesRows",
     "PropagationCapabilities",
     "PropagationConvention",
     "PropagationDiagnostics",
@@ -761,6 +863,7 @@ __all__ = [
     "PropagationTopology",
     "ScalarTransport",
     "capabilities",
+    "consumer_los_jones",
     "evaluate",
     "native_frequency_resolution_hz",
 ]
