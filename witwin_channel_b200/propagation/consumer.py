@@ -816,7 +816,8 @@ def evaluate(compiled_scene: CompiledScene, request: PropagationRequest) -> Prop
         else:
             # the row kernel's complex3 vector is at unit excitation; the
             # published field carries the source amplitude sqrt(powers_w)
-            amplitude = torch.sqrt(sources.powers_w.index_select(0, tx.to(torch.int64)))
+            # (a negative power counts as zero, as in the row kernel)
+            amplitude = torch.sqrt(torch.clamp(sources.powers_w.index_select(0, tx.to(torch.int64)), min=0.0))
             field = take(ev["field_xyz"], torch.complex64) * amplitude.view(-1, 1)
             transport = Complex3Transport(field=field.contiguous(), direction=direction)
     paths = PropagationPathBatch(pair_count=S * R, path_count=int(order.numel()), pair_index=pair_index,
