@@ -86,7 +86,7 @@ def test_los_rows_closed_form_pair_order_and_complex3():
     # complex3: the excited world field projected on the sink polarisation is the scalar coefficient
     out3 = c.evaluate(compiled, _request(sources, sinks, f, {"los"}, 0, response="complex3_transport"))
     field = out3.paths.transport.field.cpu()
-    proj = (field * sinks.polarizations.cpu()[out3.paths.topology.sink_index.long()].to(torch.complex64)).sum(-1)
+    proj = (field * sinks.polarizations.cpu()[out3.paths.topology.sink_index.cpu().long()].to(torch.complex64)).sum(-1)
     np.testing.assert_allclose(proj.numpy(), coef.numpy(), rtol=1e-5, atol=1e-9 * float(coef.abs().max()))
     assert torch.equal(out3.paths.transport.direction, out.paths.geometry.field_direction)
 
@@ -182,10 +182,12 @@ def test_empty_batches_and_refusals():
     assert out.paths.path_count == 0 and out.paths.pair_count == 0
     assert out.paths.pair_offsets.tolist() == [0]
     assert tuple(out.paths.topology.primitive_sequence.shape) == (0, 1)
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(ValueError):  # the polarimetric response needs both reference bases
         c.evaluate(compiled, _request(sources, sinks, freq, {"los"}, 0, response="polarimetric_transport"))
     with pytest.raises(NotImplementedError):
         c.evaluate(compiled, _request(sources, sinks, freq, {"los"}, 0, ad_mode="vjp"))
+    with pytest.raises(NotImplementedError):
+        c.evaluate(compiled, _request(sources, sinks, freq, {"los"}, 0, ad_mode="jvp"))
     with pytest.raises(ValueError):
         c.evaluate(compiled, _request(sources, sinks, freq, {"reflection"}, 0))
     with pytest.raises(TypeError):
