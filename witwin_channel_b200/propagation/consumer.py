@@ -715,6 +715,10 @@ def _preflight(compiled: object, request: object) -> float:
     return _frequency_value(frequency)
 
 
+# Sources the canonical record key orders directly (its 11-bit source field).
+_CANONICAL_SOURCE_LIMIT = 2048
+
+
 def _interaction_types(component_id: torch.Tensor, depth: torch.Tensor, width: int) -> torch.Tensor:
     """Per-slot interaction flags of each row (reference ``propagation/topology.py:89-107``):
     reflection 1 on every active slot, diffraction 2 on slot 0, transmission 4 on
@@ -766,11 +770,14 @@ def evaluate(compiled_scene: CompiledScene, request: PropagationRequest) -> Prop
                                   max_depth=width, coherent=True)
         dec = engine.decode_rows(rows, selected)
         table = _path_table(dec, ev, width, compiled, include_fields=True)
-        # sink-major, source-minor pair order; a stable sort keeps the canonical
-        # order of the rows inside each pair
+        # sink-major, source-minor pair order.  The canonical selection key
+        # leads with (sink, source) and holds the source in 11 bits, so up to
+        # 2048 sources the selected rows (a global limit keeps a prefix)
+        # already come in this order; beyond that a stable sort restores it
+        # and keeps the canonical order of the rows inside each pair.
         pair = table.rx_id.to(torch.int64) * S + table.tx_id.to(torch.int64)
-        order = torch.argsort(pair, stable=True)
-        pair_index = pair[order].contiguous()
+        order = None if S <= _CANONICAL_SOURCE_LIMIT else torch.argsort(pair, stable=True)
+        pair_index = (pair if order is None else pair[order]).contiguous()
         # per-pair counts by a scatter (no host read of the largest pair)
         counts = torch.zeros(S * R, dtype=torch.int64, device=device)
         counts.index_add_(0, pair_index, torch.ones_like(pair_index))
@@ -778,7 +785,7 @@ def evaluate(compiled_scene: CompiledScene, request: PropagationRequest) -> Prop
         pair_offsets[1:] = torch.cumsum(counts, 0)
 
         def take(x: torch.Tensor, dtype: torch.dtype) -> torch.Tensor:
-            return x.index_select(0, order).to(dtype).contiguous()
+            return (x if order is None else x.index_select(0, order)).to(dtype).contiguous()
 
         tx = take(table.tx_id, torch.int32)
         rx = take(table.rx_id, torch.int32)
@@ -820,7 +827,7 @@ def evaluate(compiled_scene: CompiledScene, request: PropagationRequest) -> Prop
             amplitude = torch.sqrt(torch.clamp(sources.powers_w.index_select(0, tx.to(torch.int64)), min=0.0))
             field = take(ev["field_xyz"], torch.complex64) * amplitude.view(-1, 1)
             transport = Complex3Transport(field=field.contiguous(), direction=direction)
-    paths = PropagationPathBatch(pair_count=S * R, path_count=int(order.numel()), pair_index=pair_index,
+    paths = PropagationPathBatch(pair_count=S * R, path_count=int(pair_index.numel()), pair_index=pair_index,
                                  pair_offsets=pair_offsets, topology=topology, geometry=geometry, transport=transport)
     # host observations: the solve's record count (8 bytes) and status word
     # (4 bytes); the selection's kept count (4 bytes, one read and two stream
