@@ -119,6 +119,9 @@ typedef struct {
     int32_t coherent;
     int32_t precision;       /* WCB_PRECISION_* */
     int32_t discovery_rays;  /* 0 selects the default 262144 */
+    int32_t stack_entries;   /* traversal stack entries per thread; 0 = the scene's BVH depth + 2.  A smaller
+                                value makes descents that need more drop the far subtree and set status bit 0
+                                (a failure-path test hook: results are then incomplete) */
 } wcb_solve_desc;
 
 /* Per-cell outputs, all device, NF-major:
@@ -130,7 +133,12 @@ typedef struct {
  * rows: optional compact path records (wcb_row, 48 bytes each); row_count is
  * a device int64 that receives the number of valid paths (it may exceed
  * row_capacity, in which case the call returns WCB_ERR_CAPACITY).
- * status: device int32 receiving device failure bits. */
+ * status: device int32 receiving device failure bits (bit 0: a traversal
+ * stack overflowed).
+ * transmission_overflow: optional device int64 receiving the number of
+ * transmitter-receiver segments that cross more than max_depth walls; such a
+ * segment yields no transmission path (the reference flags it in its capacity
+ * failure state, runtime.py:1280-1290 SEGMENT_PENETRATION_FAILURE). */
 typedef struct {
     void* path_gain;
     void* field;
@@ -141,6 +149,7 @@ typedef struct {
     int64_t row_capacity;
     int64_t* row_count;
     int32_t* status;
+    int64_t* transmission_overflow;
 } wcb_outputs;
 
 /* Compact path record (the frozen topology of one path). */
@@ -166,7 +175,9 @@ int wcb_solve(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_mate
  * (shortest kept, NaN drops the group) and applies max_paths (-1 = none;
  * scope 0 global, 1 per pair).  Writes the selected record indices in
  * canonical order to `selected` (capacity num_rows) and their count to
- * *num_selected (host). */
+ * *num_selected (host).  The sort key keeps every field at full width (any
+ * number of sources, sinks and object ids).  Reads counts back and
+ * synchronises `stream` before returning. */
 int wcb_rows_select(const void* rows, int64_t num_rows, int32_t width, int64_t max_paths, int32_t scope,
                     int64_t* selected, int64_t* num_selected, void* workspace, int64_t workspace_bytes, void* stream);
 int wcb_rows_select_workspace_size(int64_t num_rows, int64_t* bytes);
@@ -178,11 +189,13 @@ int wcb_rows_select_workspace_size(int64_t num_rows, int64_t* bytes);
  * synchronise the device, hosts with pools frozen after start-up.  The
  * scratch is a fixed WCB_ROWS_SELECT_NOALLOC_SCRATCH_BYTES array in the
  * library's device image; inputs whose wcb_rows_select_workspace_size exceeds
- * it (above 597,120 records) return WCB_ERR_CAPACITY before any work.  The first
- * call on a device looks the array up and may load the library's module:
- * make it before any stream capture.  All calls on a device share the array
- * (each call rewrites what it reads), so calls that overlap in time race:
- * serialise them. */
+ * it (above 597,120 records) return WCB_ERR_CAPACITY before any work.  Every
+ * call looks up the array's address on the current device; the first lookup
+ * on a device may load the library's module there.  The call reads its counts
+ * back and synchronises `stream` before returning: it blocks the calling
+ * thread and cannot run inside a stream capture.  All calls on a device share
+ * the array (each call rewrites what it reads), so calls that overlap in time
+ * race: serialise them. */
 #define WCB_ROWS_SELECT_NOALLOC_SCRATCH_BYTES (32ll << 20)
 int wcb_rows_select_noalloc(const void* rows, int64_t num_rows, int32_t width, int64_t max_paths, int32_t scope,
                             int64_t* selected, int64_t* num_selected, void* stream);
@@ -285,6 +298,20 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
                  const double* grad_path_gain, const double* grad_field_real, const double* grad_field_imag,
                  int32_t want, const uint8_t* vertex_mask, double* grad_out, int64_t grad_size, double* row_field,
                  void* workspace, int64_t workspace_bytes, void* stream);
+
+/* Fixed-topology JVP of selected path records (replaces the reference's
+ * forward-mode companions run inside the forward pass for ad_mode="jvp":
+ * deterministic.py:733-742, kernels/fields.py field Functions' jvp,
+ * native/channel/kernels/fields.cu:1193-1356 and :2183).  `tangent` is a dense
+ * FP64 tangent vector over the layout of wcb_rows_vjp_layout (tangent_size >=
+ * layout[8]); each record is re-evaluated once in FP64 with one dual lane
+ * seeded by it.  Writes row_field_tangent (K,2) FP64, the directional
+ * derivative of each record's powered path field (real, imag), and optionally
+ * row_field (K,2) FP64, the re-evaluated field.  No workspace, no host sync. */
+int wcb_rows_jvp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_materials* materials,
+                 int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
+                 const double* tangent, int64_t tangent_size, double* row_field, double* row_field_tangent,
+                 void* stream);
 
 /* Channel frequency response of path records (replaces PathResult.cfr,
  * path.py:646-656): per (tx, rx) cell and subcarrier k,

@@ -109,6 +109,23 @@ def slab_fresnel(cos_theta, eps_r, sigma_e, mu_r, gain, thickness, frequency):
     return r_te, r_tm
 
 
+def halfspace_fresnel(cos_theta, eps_r, sigma_e, mu_r, gain, frequency):
+    """Interface (half-space) Fresnel coefficients ``gain * (r_te, r_tm)``: the
+    slab law above without the Fabry-Perot layer term.  The wedge faces of
+    first-order diffraction take this form, with the cosine given by the wedge
+    angles (the reference's design notes,
+    ``docs/dev/plans/07-channel-native-differentiable-solver-plan.md:57``)."""
+    omega = max(2.0 * np.pi * frequency, SMALL_EPS)
+    ct = np.clip(np.abs(cos_theta), SMALL_EPS, 1.0)
+    sin2 = np.maximum(1.0 - ct * ct, 0.0)
+    eta = np.maximum(eps_r, SMALL_EPS) - 1.0j * np.maximum(sigma_e, 0.0) / (omega * VACUUM_PERMITTIVITY)
+    mu = np.maximum(mu_r, SMALL_EPS)
+    root = np.sqrt(eta * mu - sin2 + 0.0j)
+    r_te = gain * (mu * ct - root) / (mu * ct + root)
+    r_tm = gain * (eta * ct - root) / (eta * ct + root)
+    return r_te, r_tm
+
+
 def reflection_sequence(source, target, positions, normals, tx_power, tx_pol, rx_pol,
                         eps_r, sigma_e, mu_r, gain, thickness, frequency) -> dict:
     """General-depth specular chain (``_reference_fields.py:118-186``; ``fields.cu:113-204``).

@@ -411,9 +411,7 @@ def tx_edge_visible(tris, S, eg, e, wavelength) -> bool:
     L = eg["length"][e]
     n = int(min(max(np.ceil(L / wavelength), 4), 16))
     e_hat, t0, _ = utd.edge_frame(eg, e)
-    bis = eg["n0"][e] + eg["n1"][e]
-    bl = np.linalg.norm(bis)
-    bis = bis / bl if bl > 1e-6 else -t0
+    bis = utd.exterior_bisector(eg, e)
     c = eg["edge_pos"][e]
     ts = -0.5 * L + (np.arange(n) + 0.5) / n * L
     pts = c[None] + ts[:, None] * e_hat[None] + utd.RAY_BIAS * bis[None]
@@ -438,11 +436,36 @@ def _finish(rows: Rows, arrays, width, frequency, max_paths, scope, T, R) -> dic
         seq[i, : len(s)] = s
     prim = np.where(np.isin(cid, (1, 5)), seq[:, 0] if width > 0 else -1, -1) if K else np.zeros(0, dtype=np.int64)
     length = np.asarray(rows.length, dtype=np.float64)
-    # canonical order (valid, rx, tx, depth, cid, seq[0..w-1], prim, edge):
-    # evaluated_paths.cu:669-710
+    keep = select_records(tx, rx, cid, depth, edge, seq, length, max_paths=max_paths, scope=scope)
+    out = _evaluate(rows, keep, arrays, width, frequency)
+    out.update({
+        "tx_id": tx[keep], "rx_id": rx[keep], "component_id": cid[keep], "depth": depth[keep],
+        "edge_id": edge[keep], "primitive_id": prim[keep], "primitive_sequence": seq[keep],
+    })
+    fmid = arrays["face_material"]
+    ms = np.where(out["primitive_sequence"] >= 0, fmid[np.maximum(out["primitive_sequence"], 0)] if fmid.size else -1, -1)
+    out["material_sequence"] = ms
+    out["material_id"] = np.where(out["primitive_id"] >= 0, fmid[np.maximum(out["primitive_id"], 0)] if fmid.size else -1, -1)
+    return out
+
+
+def select_records(tx, rx, cid, depth, edge, seq, length, *, max_paths=None, scope="global") -> np.ndarray:
+    """Canonical order, identity dedup and max_paths over path records
+    (int64 arrays; ``seq`` is ``(K, width)`` with -1 padding).  Returns the
+    kept record indices in canonical order.
+
+    * order: (rx, tx, depth, component, seq[0..w-1], primitive, edge)
+      ascending, stable (``evaluated_paths.cu:669-710``);
+    * dedup: rows with one identity (tx, rx, per-slot event type and object
+      id) keep the shortest, the first on ties; a NaN length drops the group
+      (``evaluated_paths.cu:127-309``);
+    * max_paths: a global prefix, or the first max_paths rows of each
+      (rx, tx) pair."""
+    K = len(tx)
+    width = seq.shape[1] if seq.ndim == 2 else 0
+    prim = np.where(np.isin(cid, (1, 5)), seq[:, 0] if width > 0 else -1, -1) if K else np.zeros(0, dtype=np.int64)
     keys = [edge, prim] + [seq[:, c] for c in range(width - 1, -1, -1)] + [cid, depth, tx, rx]
     order = np.lexsort(keys) if K else np.zeros(0, dtype=np.int64)
-    # dedup by identity, keep shortest (first on ties): evaluated_paths.cu:127-309
     keep = []
     i = 0
     while i < len(order):
@@ -468,16 +491,7 @@ def _finish(rows: Rows, arrays, width, frequency, max_paths, scope, T, R) -> dic
                 if counts[key] <= max_paths:
                     sel.append(r)
             keep = np.asarray(sel, dtype=np.int64)
-    out = _evaluate(rows, keep, arrays, width, frequency)
-    out.update({
-        "tx_id": tx[keep], "rx_id": rx[keep], "component_id": cid[keep], "depth": depth[keep],
-        "edge_id": edge[keep], "primitive_id": prim[keep], "primitive_sequence": seq[keep],
-    })
-    fmid = arrays["face_material"]
-    ms = np.where(out["primitive_sequence"] >= 0, fmid[np.maximum(out["primitive_sequence"], 0)] if fmid.size else -1, -1)
-    out["material_sequence"] = ms
-    out["material_id"] = np.where(out["primitive_id"] >= 0, fmid[np.maximum(out["primitive_id"], 0)] if fmid.size else -1, -1)
-    return out
+    return keep
 
 
 def _identity(r, tx, rx, cid, depth, edge, seq, width):

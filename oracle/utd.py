@@ -14,8 +14,27 @@ reflection factors and the finite-edge rules the reference documents in
       locality window ``w``, corner sigmoid ``gamma(u)``, monotone truncation
       ``T_mono`` and the boundary-distance blend ``B`` with ``C_BLEND = 0.35``.
 
+Three conventions of the reference's ray-tracing library are taken from the
+reference's own call sites of it:
+
+* the wedge frame is ``t0 = normalize(n0 x edge_dir)`` with the edge record's
+  own direction (vertex v0 -> v1), and ``phi = atan2(d.n0, d.t0)``
+  (``native/channel/kernels/diffraction.cu:450-452``, which states that it
+  makes the same calls as the pair evaluation).  For an interior wedge the
+  ordered normals make ``t0`` point into face 0; for a boundary half-plane
+  (``n1 = -n0``) it may point away from the sheet, and the library then
+  evaluates the half-plane on that side of the edge line;
+* a half-plane's second face has no material (``diffraction.cu:365-377``:
+  an absent face carries the vacuum record), so its reflection factor
+  ``R_n`` is zero;
+* the face factors are interface (half-space) Fresnel coefficients at the
+  wedge angles ``sin(phi')`` and ``sin(n*pi - phi)``
+  (``docs/dev/plans/07-channel-native-differentiable-solver-plan.md:57``).
+
 The Keller stationary point and the edge numbering reproduce the reference's
-single-wedge golden lengths exactly; its amplitudes are pinned only loosely.
+single-wedge golden lengths exactly.  Its gains: edge 1 within 0.05 dB,
+edges 2 and 5 about 1.4-1.7 dB above the golden (the residue sits in the
+library's unshipped pair evaluation).
 """
 
 from __future__ import annotations
@@ -66,17 +85,28 @@ def term(beta: float, n: float, kl: float, sign: int) -> complex:
 
 
 def edge_frame(edge: dict, e: int):
-    """Unit edge direction ``e_hat``, face-0 tangent ``t0`` (into face 0) and
-    ``n0`` with ``t0 = n0 x e_hat``, so ``phi = atan2(d.n0, d.t0)`` runs from
-    face 0 (0) through the exterior to face n (``n*pi``)."""
+    """Unit edge direction ``e_hat`` (the record's v0 -> v1), face-0 tangent
+    ``t0 = normalize(n0 x e_hat)`` and ``n0``, so ``phi = atan2(d.n0, d.t0)``
+    runs from the face-0 side (0) through the exterior to face n (``n*pi``)
+    (``native/channel/kernels/diffraction.cu:450-452``)."""
     e_hat = edge["edge_dir"][e].copy()
     n0 = edge["n0"][e]
     t0 = np.cross(n0, e_hat)
-    t0 /= np.linalg.norm(t0)
-    if np.dot(edge["opp0"][e] - edge["edge_pos"][e], t0) < 0.0:
-        e_hat = -e_hat
-        t0 = -t0
+    t0 /= max(np.linalg.norm(t0), 1e-12)
     return e_hat, t0, n0
+
+
+def exterior_bisector(edge: dict, e: int) -> np.ndarray:
+    """Unit offset direction of the visibility points (F4): the exterior
+    bisector ``normalize(n0 + n1)``; for a half-plane (``n1 = -n0``) the
+    in-plane direction pointing away from the sheet."""
+    bis = edge["n0"][e] + edge["n1"][e]
+    bl = np.linalg.norm(bis)
+    if bl > 1e-6:
+        return bis / bl
+    _, t0, _ = edge_frame(edge, e)
+    into = np.dot(edge["opp0"][e] - edge["edge_pos"][e], t0) > 0.0
+    return -t0 if into else t0
 
 
 def _angle(d: np.ndarray, t0: np.ndarray, n0: np.ndarray) -> float:
@@ -128,10 +158,7 @@ def diffraction_field(S, R, tx_pol, edge: dict, e: int, mats: dict, frequency: f
     t_star = stationary_point(S, R, c, e_hat)
     q = c + t_star * e_hat
     tc = min(max(t_star, t_min), t_max)
-    bis = edge["n0"][e] + edge["n1"][e]
-    bl = np.linalg.norm(bis)
-    bis = bis / bl if bl > 1e-6 else -t0
-    q_vis = c + tc * e_hat + RAY_BIAS * bis
+    q_vis = c + tc * e_hat + RAY_BIAS * exterior_bisector(edge, e)
     sp_vec = q - S
     s_vec = R - q
     s_p = max(np.linalg.norm(sp_vec), MIN_DISTANCE)
@@ -167,13 +194,16 @@ def diffraction_field(S, R, tx_pol, edge: dict, e: int, mats: dict, frequency: f
     delta_w = 4.0 * unit
     delta_b = C_BLEND * unit
     # face reflection factors (Luebbers): 0-face at grazing phi', n-face at n*pi - phi
+    # face factors: interface Fresnel at the wedge angles; a half-plane's
+    # second face is absent (R_n = 0)
     f0 = edge["wedge_face0"][e]
     f1 = edge["wedge_face1"][e]
-    r0 = em.slab_fresnel(np.array(np.sin(phi_p)), *(mats[x][f0] for x in ("eps_r", "sigma_e", "mu_r", "gain", "thickness")), frequency)
-    if f1 >= 0:
-        rn = em.slab_fresnel(np.array(np.sin(n * np.pi - phi)), *(mats[x][f1] for x in ("eps_r", "sigma_e", "mu_r", "gain", "thickness")), frequency)
+    keys = ("eps_r", "sigma_e", "mu_r", "gain")
+    r0 = em.halfspace_fresnel(np.array(np.sin(phi_p)), *(mats[x][f0] for x in keys), frequency)
+    if f1 >= 0 and edge["face1"][e] >= 0:
+        rn = em.halfspace_fresnel(np.array(np.sin(n * np.pi - phi)), *(mats[x][f1] for x in keys), frequency)
     else:
-        rn = em.slab_fresnel(np.array(np.sin(n * np.pi - phi)), *(mats[x][f0] for x in ("eps_r", "sigma_e", "mu_r", "gain", "thickness")), frequency)
+        rn = (0.0j, 0.0j)
     bm = phi - phi_p
     bp = phi + phi_p
 

@@ -126,4 +126,6 @@ def main(root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_field_vectors.py <path to the reference checkout>")
+    main(Path(sys.argv[1]))

@@ -106,6 +106,11 @@ def test_single_wedge_edges_and_lengths_golden():
     # return_field=False exports zero-phase fields (deterministic.py:473-478)
     _compare_paths(res, ref, phases=False)
     assert torch.all(res.paths.phase_rad == 0)
+    # golden gains (test_diffraction_single_wedge.py:64-79) of edges 1, 2, 5;
+    # edge 0 is a ~3e-18 null at the reference's float32 floor
+    golden = np.array([2.980571e-18, 2.680186e-11, 1.471983e-08, 6.686395e-09])
+    db = 10.0 * np.log10(p.path_gain.double().cpu().numpy() / golden)[1:]
+    assert abs(db[0]) <= 0.1 and np.all(np.abs(db[1:]) <= 2.0), db
 
 
 def test_los_grid_layout_matches_closed_form():

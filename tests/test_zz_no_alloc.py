@@ -100,6 +100,28 @@ def test_matches_workspace_entry_two_calls(max_paths, scope):
         assert torch.equal(got, expected)
 
 
+def test_call_allocates_nothing():
+    """After a warm-up call, a second call on a stream the caller already owns
+    leaves the device's free memory and torch's allocation counters as they
+    were: the selection's scratch all comes from the fixed array."""
+    rows = _rows(50000, seed=21)
+    selected = torch.full((50000,), -7, dtype=torch.int64, device="cuda")
+    rc, first = _select_noalloc(rows, 3, -1, 0, selected)
+    assert rc == _native.WCB_OK
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    stats_before = torch.cuda.memory_stats()
+    rc, second = _select_noalloc(rows, 3, -1, 0, selected)
+    assert rc == _native.WCB_OK
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    stats_after = torch.cuda.memory_stats()
+    assert free_after == free_before
+    for key in ("allocation.all.allocated", "segment.all.allocated"):
+        assert stats_after.get(key, 0) == stats_before.get(key, 0), key
+    assert torch.equal(first, second)
+
+
 def test_small_after_large_and_empty():
     big = _rows(150000, seed=5)
     small = _rows(700, seed=6)

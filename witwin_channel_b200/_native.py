@@ -82,6 +82,7 @@ class SolveDesc(ctypes.Structure):
         ("coherent", ctypes.c_int32),
         ("precision", ctypes.c_int32),
         ("discovery_rays", ctypes.c_int32),
+        ("stack_entries", ctypes.c_int32),
     ]
 
 
@@ -96,6 +97,7 @@ class Outputs(ctypes.Structure):
         ("row_capacity", ctypes.c_int64),
         ("row_count", _vp),
         ("status", _vp),
+        ("transmission_overflow", _vp),
     ]
 
 
@@ -150,6 +152,7 @@ EXPORTED_SYMBOLS = (
     "wcb_rows_vjp_layout",
     "wcb_rows_vjp_workspace_size",
     "wcb_rows_vjp",
+    "wcb_rows_jvp",
     "wcb_cfr_workspace_size",
     "wcb_cfr",
     "wcb_field_free_space",
@@ -219,6 +222,8 @@ def load() -> ctypes.CDLL:
     lib.wcb_rows_vjp.argtypes = [_vp, ctypes.POINTER(SolveDesc), ctypes.POINTER(Materials), ctypes.c_int32, _vp, _vp,
                                  ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int32, _vp, _vp, ctypes.c_int64, _vp, _vp,
                                  ctypes.c_int64, _vp]
+    lib.wcb_rows_jvp.argtypes = [_vp, ctypes.POINTER(SolveDesc), ctypes.POINTER(Materials), ctypes.c_int32, _vp, _vp,
+                                 ctypes.c_int64, _vp, ctypes.c_int64, _vp, _vp, _vp]
     lib.wcb_cfr_workspace_size.argtypes = [ctypes.c_int32, ctypes.c_int32, _i64p]
     lib.wcb_cfr.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                             ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int32, _vp, _vp, ctypes.c_int64, _vp]

@@ -16,6 +16,14 @@ giving gradients for mesh vertices, per-material eps_r / sigma_e (and layer
 values), the carrier frequency, Tx positions and point-receiver positions.
 Material values that depend on the frequency or on other tensors chain
 through torch autograd as usual.
+
+Forward mode (``ad_mode="jvp"``; the reference runs its dual companions
+inside the forward, ``deterministic.py:733-742``) uses the same frozen
+forward: when the scene values are ``torch.autograd.forward_ad`` dual
+tensors, the autograd Function's ``jvp`` packs their tangents into the same
+parameter layout, re-evaluates every record once with one FP64 dual lane
+seeded by it (``wcb_rows_jvp``) and scatters the records' field and gain
+tangents to the cells with the accumulation's pushforward.
 """
 
 from __future__ import annotations
@@ -24,11 +32,12 @@ import ctypes
 from dataclasses import dataclass
 from typing import Any
 
+import numpy as np
 import torch
 
 from . import _native, engine
 from .compiler import compile_scene
-from .kernels import ACCUM_FIELDS, _forward, deterministic_accumulate_flat_backward
+from .kernels import ACCUM_FIELDS, _forward, deterministic_accumulate_flat_backward, deterministic_accumulate_flat_jvp
 
 WANT_TX, WANT_RX, WANT_FREQ, WANT_VERTICES, WANT_MATERIALS = 1, 2, 4, 8, 16
 
@@ -45,10 +54,28 @@ class _State:
     rows: torch.Tensor
     selected: torch.Tensor
     flat: dict              # valid, tx, rx, cid (int32) of the selected records
-    saved64: list           # per frequency: FP64 accumulation outputs (linearisation point)
+    saved64: list           # per frequency: FP64 accumulation outputs (linearisation point), made on first use
     outputs32: list         # per frequency: FP32 accumulation outputs (the returned values)
     layer_counts: list
     vertex_mask: torch.Tensor | None = None
+    param_total: int = 0    # length of the native parameter layout
+
+
+def _linearisation(state: _State, fi: int) -> dict:
+    """FP64 cell accumulation of the records' FP64 re-evaluated fields at
+    frequency ``fi``: the point the derivatives of |sum field|^2 are taken at.
+    (The FP32 forward values would do for most losses, but a loss whose cell
+    terms cancel amplifies their rounding into the gradient.)  Computed once
+    per frequency by one zero-tangent ``wcb_rows_jvp`` pass and cached."""
+    if state.saved64[fi] is None:
+        zero = torch.zeros(max(state.param_total, 1), dtype=torch.float64, device=state.rows.device)
+        field, _ = rows_jvp(state, fi, zero)
+        re, im = field[:, 0].contiguous(), field[:, 1].contiguous()
+        gain = (re * re + im * im).contiguous()
+        f_ = state.flat
+        state.saved64[fi] = _forward(f_["valid"], f_["tx"], f_["rx"], f_["cid"], gain, re, im, state.ep.num_tx,
+                                     state.ep.num_rx, state.coherent, 0)
+    return state.saved64[fi]
 
 
 def _as_f64(x, device) -> torch.Tensor:
@@ -130,6 +157,39 @@ def rows_vjp(state: _State, freq_index: int, g_gain: torch.Tensor | None, g_re: 
 _VJP_WORKSPACE = engine.Workspace()
 
 
+def _param_total(compiled, ep, mats, frequencies, bits, config) -> int:
+    lib = _native.load()
+    desc, keep = engine.make_desc(ep, frequencies, bits, config.max_depth, config.coherent)
+    ms = mats.as_struct()
+    layout = (ctypes.c_int64 * 9)()
+    _native.check(lib.wcb_rows_vjp_layout(compiled.native.handle, ctypes.byref(desc), ctypes.byref(ms), layout),
+                  "wcb_rows_vjp_layout")
+    del keep
+    return int(layout[8])
+
+
+def rows_jvp(state: _State, freq_index: int, tangent: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor]:
+    """Per-record FP64 path field and its directional derivative ((K,2) each)
+    for a dense FP64 tangent over the native parameter layout (``wcb_rows_jvp``)."""
+    lib = _native.load()
+    device = state.rows.device
+    desc, keep = engine.make_desc(state.ep, state.frequencies, state.components, state.max_depth, state.coherent)
+    ms = state.mats.as_struct()
+    K = int(state.selected.shape[0])
+    field = torch.zeros((max(K, 1), 2), dtype=torch.float64, device=device)
+    dfield = torch.zeros((max(K, 1), 2), dtype=torch.float64, device=device)
+    tangent = tangent.to(device=device, dtype=torch.float64).contiguous()
+    _native.check(
+        lib.wcb_rows_jvp(state.compiled.native.handle, ctypes.byref(desc), ctypes.byref(ms), int(freq_index),
+                         _native.ptr(state.rows) if K else None, _native.ptr(state.selected) if K else None, K,
+                         _native.ptr(tangent), tangent.numel(), _native.ptr(field), _native.ptr(dfield),
+                         _native.stream_handle(device)),
+        "wcb_rows_jvp",
+    )
+    del keep
+    return field[:K], dfield[:K]
+
+
 class _SolveFunction(torch.autograd.Function):
     """Cell outputs (NF,T,R) / (NF,6,T,R) of the frozen-topology solve as a
     function of the scene values."""
@@ -166,7 +226,7 @@ class _SolveFunction(torch.autograd.Function):
             gf = [None if g is None else g[fi].to(torch.float64).contiguous() for g in grads]
             if all(g is None for g in gf):
                 continue
-            s = state.saved64[fi]
+            s = _linearisation(state, fi)
             per_row = deterministic_accumulate_flat_backward(
                 f_["valid"], f_["tx"], f_["rx"], f_["cid"], s["component_field_real"], s["component_field_imag"],
                 s["field_total_real"], s["field_total_imag"], s["power_total"], grad_power_total=gf[0],
@@ -183,6 +243,46 @@ class _SolveFunction(torch.autograd.Function):
             acc[6] += parts[6].reshape(ctx.shapes[6])
             acc[7] += parts[7].reshape(ctx.shapes[7])
         return (None,) + tuple(a if needs[i + 1] else None for i, a in enumerate(acc))
+
+    @staticmethod
+    def jvp(ctx, _t_state, *tangents):
+        """Forward mode: the inputs' tangents, laid out like the VJP gradient,
+        seed one FP64 dual lane per record (``wcb_rows_jvp``); the records'
+        field and gain tangents are scattered to the cells by the flat
+        accumulation's pushforward."""
+        state: _State = ctx.state
+        if all(t is None for t in tangents):
+            return (None,) * len(ACCUM_FIELDS)
+        dev = state.rows.device
+        T, R = state.ep.num_tx, state.ep.num_rx
+        shapes = ctx.shapes
+
+        def part(i, fi=None):
+            shape = shapes[i] if fi is None else shapes[i][1:]
+            t = tangents[i]
+            if t is None:
+                return torch.zeros(int(np.prod(shape)), dtype=torch.float64, device=dev)
+            t = t if fi is None else t[fi]
+            return t.reshape(-1).to(device=dev, dtype=torch.float64)
+
+        f_ = state.flat
+        per_freq = []
+        for fi in range(len(state.frequencies)):
+            tf = tangents[5]
+            t_freq = torch.zeros(1, dtype=torch.float64, device=dev) if tf is None else \
+                tf[fi:fi + 1].to(device=dev, dtype=torch.float64)
+            tangent = torch.cat([part(0), part(1, fi), part(2, fi), part(3, fi), part(4, fi), t_freq, part(6),
+                                 part(7)])
+            field, dfield = rows_jvp(state, fi, tangent)
+            t_re, t_im = dfield[:, 0].contiguous(), dfield[:, 1].contiguous()
+            t_gain = (2.0 * (field[:, 0] * t_re + field[:, 1] * t_im)).contiguous()
+            s = _linearisation(state, fi)
+            out = deterministic_accumulate_flat_jvp(
+                f_["valid"], f_["tx"], f_["rx"], f_["cid"], s["component_field_real"], s["component_field_imag"],
+                s["power_total"], tangent_path_gain=t_gain, tangent_field_real=t_re, tangent_field_imag=t_im,
+                num_tx=T, num_rx=R, coherent=state.coherent)
+            per_freq.append(out)
+        return tuple(torch.stack([o[k] for o in per_freq]).to(torch.float32) for k in ACCUM_FIELDS)
 
 
 def vjp_forward(scene: Any, config, frequencies_hz) -> dict:
@@ -221,14 +321,14 @@ def vjp_forward(scene: Any, config, frequencies_hz) -> dict:
         g32, r32, i32 = ev["path_gain"].contiguous(), pf.real.contiguous(), pf.imag.contiguous()
         outputs32.append(_forward(flat["valid"], flat["tx"], flat["rx"], flat["cid"], g32, r32, i32, T, R,
                                   config.coherent, 0))
-        saved64.append(_forward(flat["valid"], flat["tx"], flat["rx"], flat["cid"], g32.double(), r32.double(),
-                                i32.double(), T, R, config.coherent, 0))
+        saved64.append(None)
         evs.append(ev)
     inputs = _differentiable_inputs(scene, compiled, freqs_t, device)
     state = _State(compiled=compiled, ep=ep, mats=mats, frequencies=frequencies, components=bits,
                    max_depth=config.max_depth, coherent=config.coherent, rows=rows, selected=selected, flat=flat,
                    saved64=saved64, outputs32=outputs32, layer_counts=inputs["layer_counts"],
-                   vertex_mask=inputs["vertex_mask"])
+                   vertex_mask=inputs["vertex_mask"], param_total=_param_total(compiled, ep, mats, frequencies,
+                                                                               bits, config))
     out = _SolveFunction.apply(state, inputs["vertices"], inputs["eps_r"], inputs["sigma_e"], inputs["layer_eps_r"],
                                inputs["layer_sigma_e"], inputs["frequency"], inputs["tx"], inputs["rx"])
     result = dict(zip(ACCUM_FIELDS, out))
@@ -244,6 +344,7 @@ def solve_vjp(scene: Any, config, reference_frequency_hz):
         _OPTIONAL_COMPONENTS,
         _SLOTS,
         Result,
+        _component_counts,
         _layout,
         _metadata,
         _path_table,
@@ -262,11 +363,11 @@ def solve_vjp(scene: Any, config, reference_frequency_hz):
     comp_fields = {n: _layout(torch.complex(cfr[_SLOTS[n]], cfi[_SLOTS[n]]), rx) for n in names} \
         if config.return_field else {n: torch.empty((0,), dtype=torch.complex64, device=device) for n in names}
     dec = v["dec"]
-    counts = {name: int((dec["component_id"] == c).sum().item())
-              for name, c in (("los", 0), ("reflection", 1), ("diffraction", 2), ("transmission", 5))}
+    counts = _component_counts(dec["component_id"])
     paths = _path_table(dec, v["evaluations"][0], v["width"], v["compiled"], config.return_field) \
         if config.export_paths else None
-    meta = _metadata(config, counts, v["count"], _native.launch_count() - launches0, {"ad": "fixed-topology vjp"})
+    meta = _metadata(config, counts, v["count"], _native.launch_count() - launches0,
+                     {"ad": f"fixed-topology {config.ad_mode}"})
     return Result(
         path_gain=_layout(pt, rx),
         field=_layout(torch.complex(ftr, fti), rx) if config.return_field

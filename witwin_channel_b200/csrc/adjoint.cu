@@ -137,6 +137,58 @@ long long max_params_per_row(int max_depth, int max_layers) {
     return std::min<long long>(kMaxParams, std::max(refl, std::max(trans, diff)));
 }
 
+// Scene, endpoint, material (at freq_index) and parameter-layout fields of
+// the derivative kernels' parameters.
+void fill_params(AdjParams& p, const SceneHandle* h, const wcb_solve_desc* desc, const wcb_materials* materials,
+                 int freq_index, const void* rows, const int64_t* selected, long long K, const int64_t* layout) {
+    std::memset(&p, 0, sizeof(p));
+    p.sc = h->dev;
+    p.edge_slot = h->edge_slot;
+    p.edge_topo = h->edge_topo;
+    p.tx_pos = desc->tx_pos;
+    p.tx_power = desc->tx_power;
+    p.tx_pol = desc->tx_pol;
+    p.rx_kind = desc->rx_kind;
+    p.rx_pos = desc->rx_pos;
+    for (int i = 0; i < 3; ++i) {
+        p.grid_origin[i] = desc->grid_origin[i];
+        p.grid_x[i] = desc->grid_x_axis[i];
+        p.grid_y[i] = desc->grid_y_axis[i];
+    }
+    p.grid_rows = desc->grid_rows;
+    p.grid_cols = desc->grid_cols;
+    p.grid_spacing[0] = desc->grid_spacing[0];
+    p.grid_spacing[1] = desc->grid_spacing[1];
+    p.rx_pol = desc->rx_pol;
+    p.rx_pol_stride = desc->rx_pol_stride;
+    p.freq = desc->frequency_hz[freq_index];
+    const int M = materials->num_materials;
+    const int NL = materials->num_layers;
+    p.num_materials = M;
+    p.eps_r = materials->eps_r + (long long)freq_index * M;
+    p.sigma_e = materials->sigma_e + (long long)freq_index * M;
+    p.mu_r = materials->mu_r + (long long)freq_index * M;
+    p.gain = materials->gain + (long long)freq_index * M;
+    p.thickness = materials->thickness + (long long)freq_index * M;
+    p.num_layers = NL;
+    p.layer_offset = materials->layer_offset;
+    p.layer_count = materials->layer_count;
+    p.layer_thickness = materials->layer_thickness + (long long)freq_index * NL;
+    p.layer_eps_r = materials->layer_eps_r + (long long)freq_index * NL;
+    p.layer_sigma_e = materials->layer_sigma_e + (long long)freq_index * NL;
+    p.layer_mu_r = materials->layer_mu_r + (long long)freq_index * NL;
+    p.rows = static_cast<const RowRec*>(rows);
+    p.selected = reinterpret_cast<const long long*>(selected);
+    p.count = K;
+    p.base_meps = int(layout[1]);
+    p.base_msig = int(layout[2]);
+    p.base_leps = int(layout[3]);
+    p.base_lsig = int(layout[4]);
+    p.gid_freq = int(layout[5]);
+    p.base_tx = int(layout[6]);
+    p.base_rx = int(layout[7]);
+}
+
 }  // namespace adj
 }  // namespace wcb
 
@@ -190,7 +242,6 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
     if (rc != WCB_OK) return rc;
     if (grad_size < layout[8]) return WCB_ERR_CAPACITY;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const wcb::SceneHandle* h = scene->h;
     const long long K = num_selected;
     const long long P = layout[8];
     if (K == 0) {
@@ -200,57 +251,12 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
     if (workspace == nullptr || workspace_bytes < (long long)L.ids) return WCB_ERR_CAPACITY;
     char* b = static_cast<char*>(workspace);
     wcb::adj::AdjParams p;
-    std::memset(&p, 0, sizeof(p));
-    p.sc = h->dev;
-    p.edge_slot = h->edge_slot;
-    p.edge_topo = h->edge_topo;
-    p.tx_pos = desc->tx_pos;
-    p.tx_power = desc->tx_power;
-    p.tx_pol = desc->tx_pol;
-    p.rx_kind = desc->rx_kind;
-    p.rx_pos = desc->rx_pos;
-    for (int i = 0; i < 3; ++i) {
-        p.grid_origin[i] = desc->grid_origin[i];
-        p.grid_x[i] = desc->grid_x_axis[i];
-        p.grid_y[i] = desc->grid_y_axis[i];
-    }
-    p.grid_rows = desc->grid_rows;
-    p.grid_cols = desc->grid_cols;
-    p.grid_spacing[0] = desc->grid_spacing[0];
-    p.grid_spacing[1] = desc->grid_spacing[1];
-    p.rx_pol = desc->rx_pol;
-    p.rx_pol_stride = desc->rx_pol_stride;
-    p.freq = desc->frequency_hz[freq_index];
-    const int M = materials->num_materials;
-    const int NL = materials->num_layers;
-    p.num_materials = M;
-    p.eps_r = materials->eps_r + (long long)freq_index * M;
-    p.sigma_e = materials->sigma_e + (long long)freq_index * M;
-    p.mu_r = materials->mu_r + (long long)freq_index * M;
-    p.gain = materials->gain + (long long)freq_index * M;
-    p.thickness = materials->thickness + (long long)freq_index * M;
-    p.num_layers = NL;
-    p.layer_offset = materials->layer_offset;
-    p.layer_count = materials->layer_count;
-    p.layer_thickness = materials->layer_thickness + (long long)freq_index * NL;
-    p.layer_eps_r = materials->layer_eps_r + (long long)freq_index * NL;
-    p.layer_sigma_e = materials->layer_sigma_e + (long long)freq_index * NL;
-    p.layer_mu_r = materials->layer_mu_r + (long long)freq_index * NL;
-    p.rows = static_cast<const wcb::RowRec*>(rows);
-    p.selected = reinterpret_cast<const long long*>(selected);
-    p.count = K;
+    wcb::adj::fill_params(p, scene->h, desc, materials, freq_index, rows, selected, K, layout);
     p.g_gain = grad_path_gain;
     p.g_re = grad_field_real;
     p.g_im = grad_field_imag;
     p.want = want;
     p.vertex_mask = vertex_mask;
-    p.base_meps = int(layout[1]);
-    p.base_msig = int(layout[2]);
-    p.base_leps = int(layout[3]);
-    p.base_lsig = int(layout[4]);
-    p.gid_freq = int(layout[5]);
-    p.base_tx = int(layout[6]);
-    p.base_rx = int(layout[7]);
     p.counts = reinterpret_cast<int*>(b + L.counts);
     long long* offsets = reinterpret_cast<long long*>(b + L.offsets);
     p.offsets = offsets;
@@ -353,6 +359,33 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
     }
     rc = cudaGetLastError() == cudaSuccess ? WCB_OK : WCB_ERR_CUDA;
     return rc;
+}
+
+int wcb_rows_jvp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_materials* materials,
+                 int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
+                 const double* tangent, int64_t tangent_size, double* row_field, double* row_field_tangent,
+                 void* stream) {
+    if (scene == nullptr || desc == nullptr || materials == nullptr || tangent == nullptr || num_selected < 0)
+        return WCB_ERR_INVALID_ARGUMENT;
+    if (num_selected > 0 && (rows == nullptr || selected == nullptr || row_field_tangent == nullptr))
+        return WCB_ERR_INVALID_ARGUMENT;
+    if (freq_index < 0 || freq_index >= desc->num_freq || desc->frequency_hz == nullptr)
+        return WCB_ERR_INVALID_ARGUMENT;
+    int64_t layout[9];
+    const int rc = wcb_rows_vjp_layout(scene, desc, materials, layout);
+    if (rc != WCB_OK) return rc;
+    if (tangent_size < layout[8]) return WCB_ERR_CAPACITY;
+    if (num_selected == 0) return WCB_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    wcb::adj::AdjParams p;
+    wcb::adj::fill_params(p, scene->h, desc, materials, freq_index, rows, selected, num_selected, layout);
+    const unsigned g = unsigned((num_selected + wcb::adj::kBlock - 1) / wcb::adj::kBlock);
+    wcb::adj::k_jvp_rows<0><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent);
+    wcb::adj::k_jvp_rows<1><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent);
+    wcb::adj::k_jvp_rows<5><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent);
+    wcb::adj::launch_jvp_diffraction(p, tangent, row_field, row_field_tangent, s);
+    wcb::note_launch(4);
+    return cudaGetLastError() == cudaSuccess ? WCB_OK : WCB_ERR_CUDA;
 }
 
 }  // extern "C"

@@ -177,7 +177,7 @@ WCB_D void build_params(const AdjParams& p, const RowRec& row, ParamList& pl) {
         if (tp[3] >= 0) add_face_vertices(p, pl, tp[3]);
         const EdgeDev& ed = p.sc.edges[slot];
         add_material(p, pl, p.sc.face_material[ed.mat_face0]);
-        add_material(p, pl, p.sc.face_material[ed.mat_face1]);
+        if (ed.face_n) add_material(p, pl, p.sc.face_material[ed.mat_face1]);
     }
 }
 
@@ -194,15 +194,30 @@ struct Window {
     }
 };
 
+// Forward-mode seeds: one tangent lane whose derivative of every parameter is
+// that parameter's entry of a dense tangent vector (the layout of
+// wcb_rows_vjp_layout).  The JVP evaluates each record once with these.
 template <int N>
-WCB_D V3<Dual<N>> vertex(const AdjParams& p, const Window<N>& w, int v) {
+struct Seeds {
+    const double* t;
+    WCB_D Dual<N> param(double value, int gid) const {
+        Dual<N> d(value);
+#pragma unroll
+        for (int j = 0; j < N; ++j) d.d[j] = 0.0;
+        d.d[0] = t[gid];
+        return d;
+    }
+};
+
+template <template <int> class WT, int N>
+WCB_D V3<Dual<N>> vertex(const AdjParams& p, const WT<N>& w, int v) {
     const float* x = p.sc.vertices + 3 * v;
     return v3(w.param(x[0], gid_vertex(v, 0)), w.param(x[1], gid_vertex(v, 1)), w.param(x[2], gid_vertex(v, 2)));
 }
 
 // unit normal of (b - a) x (c - a), length floored at 1e-6 (the scene compile's rule)
-template <int N>
-WCB_D V3<Dual<N>> face_unit_normal(const AdjParams& p, const Window<N>& w, int f, V3<Dual<N>>* anchor) {
+template <template <int> class WT, int N>
+WCB_D V3<Dual<N>> face_unit_normal(const AdjParams& p, const WT<N>& w, int f, V3<Dual<N>>* anchor) {
     const V3<Dual<N>> a = vertex(p, w, p.sc.faces[3 * f]);
     const V3<Dual<N>> b = vertex(p, w, p.sc.faces[3 * f + 1]);
     const V3<Dual<N>> c = vertex(p, w, p.sc.faces[3 * f + 2]);
@@ -211,14 +226,14 @@ WCB_D V3<Dual<N>> face_unit_normal(const AdjParams& p, const Window<N>& w, int f
     return n * (Dual<N>(1.0) / s_max(length(n), 1e-6));
 }
 
-template <int N>
-WCB_D Slab<Dual<N>> slab(const AdjParams& p, const Window<N>& w, int m) {
+template <template <int> class WT, int N>
+WCB_D Slab<Dual<N>> slab(const AdjParams& p, const WT<N>& w, int m) {
     return Slab<Dual<N>>{w.param(p.eps_r[m], p.base_meps + m), w.param(p.sigma_e[m], p.base_msig + m),
                          Dual<N>(p.mu_r[m]), Dual<N>(p.gain[m]), Dual<N>(p.thickness[m])};
 }
 
-template <int N>
-WCB_D V3<Dual<N>> receiver(const AdjParams& p, const Window<N>& w, int r) {
+template <template <int> class WT, int N>
+WCB_D V3<Dual<N>> receiver(const AdjParams& p, const WT<N>& w, int r) {
     if (p.rx_kind == 1) {
         const int row = r / p.grid_cols;
         const int col = r - row * p.grid_cols;
@@ -235,8 +250,8 @@ WCB_D V3<Dual<N>> receiver(const AdjParams& p, const Window<N>& w, int r) {
 }
 
 // Edge frame from vertices, following the scene compile's construction.
-template <int N>
-WCB_D EdgeFrame<Dual<N>> edge_frame_dual(const AdjParams& p, const Window<N>& w, int slot) {
+template <template <int> class WT, int N>
+WCB_D EdgeFrame<Dual<N>> edge_frame_dual(const AdjParams& p, const WT<N>& w, int slot) {
     using D = Dual<N>;
     const int* tp = p.edge_topo + 4 * slot;
     const V3<D> va = vertex(p, w, tp[0]);
@@ -260,13 +275,14 @@ WCB_D EdgeFrame<Dual<N>> edge_frame_dual(const AdjParams& p, const Window<N>& w,
     }
     const V3<D> bis = f.n0 + n1;
     const D bl = length(bis);
-    f.bisector = value_of(bl) > 1e-6 ? bis * (D(1.0) / bl) : -f.t0;
+    f.bisector = value_of(bl) > 1e-6 ? bis * (D(1.0) / bl) : -f.t0;  // feeds only the visibility point
+    f.face_n = tp[3] >= 0;
     return f;
 }
 
 // FP64 dual re-evaluation of one record's powered path field.
-template <int N, int COMP>
-WCB_D Cx<Dual<N>> eval_record(const AdjParams& p, const RowRec& row, const Window<N>& w) {
+template <int N, int COMP, template <int> class WT>
+WCB_D Cx<Dual<N>> eval_record(const AdjParams& p, const RowRec& row, const WT<N>& w) {
     using D = Dual<N>;
     const int t = row.tx, r = row.rx;
     const V3<D> S = v3(w.param(p.tx_pos[3 * t], p.base_tx + 3 * t), w.param(p.tx_pos[3 * t + 1], p.base_tx + 3 * t + 1),
@@ -464,6 +480,31 @@ __global__ void __launch_bounds__(kBlock, 4) k_vjp_pairs(AdjParams p, const int*
 }
 
 void launch_vjp_diffraction(const AdjParams& p, const int* pair_base, long long total, cudaStream_t s);
+void fill_params(AdjParams& p, const SceneHandle* h, const wcb_solve_desc* desc, const wcb_materials* materials,
+                 int freq_index, const void* rows, const int64_t* selected, long long K, const int64_t* layout);
+
+// Forward mode: each record of component COMP evaluated once with the tangent
+// seeds; writes its FP64 path field and the field's tangent ((K,2) each).
+template <int COMP>
+__global__ void __launch_bounds__(kBlock) k_jvp_rows(AdjParams p, const double* tangent, double* field,
+                                                     double* field_tangent) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= p.count) return;
+    const RowRec row = p.rows[p.selected[i]];
+    if (row.component != COMP) return;
+    const Seeds<1> seeds{tangent};
+    const Cx<Dual<1>> pf = eval_record<1, COMP>(p, row, seeds);
+    if (field) {
+        field[2 * i] = pf.re.v;
+        field[2 * i + 1] = pf.im.v;
+    }
+    const double dre = pf.re.d[0], dim = pf.im.d[0];
+    field_tangent[2 * i] = isfinite(dre) ? dre : 0.0;
+    field_tangent[2 * i + 1] = isfinite(dim) ? dim : 0.0;
+}
+
+void launch_jvp_diffraction(const AdjParams& p, const double* tangent, double* field, double* field_tangent,
+                            cudaStream_t s);
 
 }  // namespace adj
 }  // namespace wcb

@@ -1,5 +1,5 @@
-// The diffraction records' VJP kernel (dual-number UTD), in its own
-// translation unit so it compiles in parallel with the other components.
+// The diffraction records' VJP and JVP kernels (dual-number UTD), in their own
+// translation unit so they compile in parallel with the other components.
 #include "adjoint.cuh"
 
 namespace wcb {
@@ -9,6 +9,13 @@ namespace adj {
 void launch_vjp_diffraction(const AdjParams& p, const int* pair_base, long long total, cudaStream_t s) {
     if (p.order_count <= 0 || total <= 0) return;
     k_vjp_pairs<2><<<unsigned((total + kBlock - 1) / kBlock), kBlock, 0, s>>>(p, pair_base, total);
+}
+
+// Forward mode over the diffraction records (one thread per record).
+void launch_jvp_diffraction(const AdjParams& p, const double* tangent, double* field, double* field_tangent,
+                            cudaStream_t s) {
+    if (p.count <= 0) return;
+    k_jvp_rows<2><<<unsigned((p.count + kBlock - 1) / kBlock), kBlock, 0, s>>>(p, tangent, field, field_tangent);
 }
 
 }  // namespace adj

@@ -43,6 +43,25 @@ WCB_HD void slab_fresnel(T cos_theta, const Slab<T>& m, F frequency, T wavelengt
     *r_tm = ((i_tm * (one - phase)) / (one - i_tm * i_tm * phase)) * m.gain;
 }
 
+// Interface (half-space) Fresnel coefficients gain * (r_te, r_tm): the slab law
+// above without its Fabry-Perot layer term.  The wedge faces of first-order
+// diffraction take this form at the wedge angles (the reference's design
+// notes, docs/dev/plans/07-channel-native-differentiable-solver-plan.md:57).
+template <typename T, typename F = double>
+WCB_HD void halfspace_fresnel(T cos_theta, const Slab<T>& m, F frequency, Cx<T>* r_te, Cx<T>* r_tm) {
+    const T omega = T(s_max(kTwoPi * frequency, kUtdSmallEps));
+    T ct = s_abs(cos_theta);
+    ct = s_min(s_max(ct, T(kUtdSmallEps)), T(1));
+    const T sin2 = s_max(T(1) - ct * ct, T(0));
+    const Cx<T> eta = cx(s_max(m.eps_r, T(kUtdSmallEps)), -s_max(m.sigma_e, T(0)) / (omega * T(kEps0)));
+    const T mu = s_max(m.mu_r, T(kUtdSmallEps));
+    const Cx<T> root = csqrt(eta * mu - cx(sin2, T(0)));
+    const Cx<T> mu_ct = cx(mu * ct, T(0));
+    const Cx<T> eta_ct = eta * ct;
+    *r_te = ((mu_ct - root) / (mu_ct + root)) * m.gain;
+    *r_tm = ((eta_ct - root) / (eta_ct + root)) * m.gain;
+}
+
 // One specular bounce of the transported field (the loop body of
 // _reference_fields.py:143-181).  Updates `value` and `outgoing`.
 template <typename T, typename F = double>

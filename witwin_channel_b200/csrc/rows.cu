@@ -7,8 +7,11 @@
 // the same identity (tx, rx, per-slot event type and object id) keep the
 // shortest (first on ties) and a NaN length drops the group; max_paths keeps
 // a global prefix or the first max_paths rows of each (rx, tx) pair.  Here the
-// key is packed into four 64-bit words and sorted with four stable radix
-// passes (least significant word first).
+// key is the concatenation of its fields at the widths the input needs (one
+// pass measures the largest rx, tx and object id), cut into 64-bit words and
+// sorted with one stable radix pass per word, least significant first; every
+// field keeps its full value, so any number of sources, sinks or ids sorts
+// exactly.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -26,24 +29,70 @@ namespace {
 
 constexpr int kB = 256;
 
-WCB_D unsigned long long field18(int v) { return static_cast<unsigned long long>((v + 1) & 0x3ffff); }
-
 WCB_D int row_prim(const RowRec& r) { return (r.component == 1 || r.component == 5) ? r.seq[0] : -1; }
 
-__global__ void k_row_key(long long n, const RowRec* rows, const int* order, int word, unsigned long long* keys) {
+// Canonical key fields, least significant first: edge, primitive,
+// sequence[4..0], component, depth, tx, rx.  Object ids are stored +1 (so -1
+// maps to 0).
+constexpr int kKeyFields = 11;
+
+struct KeyLayout {
+    int offset[kKeyFields];
+    int bits[kKeyFields];
+    int total;
+};
+
+WCB_D unsigned long long key_field(const RowRec& r, int f) {
+    switch (f) {
+        case 0: return static_cast<unsigned long long>(r.edge + 1);
+        case 1: return static_cast<unsigned long long>(row_prim(r) + 1);
+        case 7: return static_cast<unsigned long long>(r.component & 7);
+        case 8: return static_cast<unsigned long long>(r.depth & 7);
+        case 9: return static_cast<unsigned long long>(r.tx);
+        case 10: return static_cast<unsigned long long>(r.rx);
+        default: return static_cast<unsigned long long>(r.seq[6 - f] + 1);  // f = 2..6: seq[4]..seq[0]
+    }
+}
+
+// largest rx, tx and id + 1 (atomic max into m[0..2], cleared by the caller)
+__global__ void k_key_max(long long n, const RowRec* rows, int* m) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int rx = 0, tx = 0, id = 0;
+    if (i < n) {
+        const RowRec r = rows[i];
+        rx = max(r.rx, 0);
+        tx = max(r.tx, 0);
+        id = max(max(r.edge, row_prim(r)), 0) + 1;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) id = max(id, r.seq[k] + 1);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        rx = max(rx, __shfl_xor_sync(0xffffffffu, rx, o));
+        tx = max(tx, __shfl_xor_sync(0xffffffffu, tx, o));
+        id = max(id, __shfl_xor_sync(0xffffffffu, id, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(m, rx);
+        atomicMax(m + 1, tx);
+        atomicMax(m + 2, id);
+    }
+}
+
+// 64-bit word `word` of the concatenated key
+__global__ void k_row_key(long long n, const RowRec* rows, const int* order, KeyLayout L, int word,
+                          unsigned long long* keys) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const RowRec r = rows[order ? order[i] : i];
+    const int lo = 64 * word;
     unsigned long long k = 0;
-    if (word == 0) {
-        k = field18(r.edge);
-    } else if (word == 1) {
-        k = (field18(r.seq[3]) << 36) | (field18(r.seq[4]) << 18) | field18(row_prim(r));
-    } else if (word == 2) {
-        k = (field18(r.seq[0]) << 36) | (field18(r.seq[1]) << 18) | field18(r.seq[2]);
-    } else {
-        k = (static_cast<unsigned long long>(r.rx) << 17) | (static_cast<unsigned long long>(r.tx & 0x7ff) << 6) |
-            (static_cast<unsigned long long>(r.depth & 7) << 3) | static_cast<unsigned long long>(r.component & 7);
+#pragma unroll
+    for (int f = 0; f < kKeyFields; ++f) {
+        const int off = L.offset[f], b = L.bits[f];
+        if (off + b <= lo || off >= lo + 64) continue;
+        const unsigned long long v = key_field(r, f) & (b >= 64 ? ~0ull : ((1ull << b) - 1ull));
+        k |= off >= lo ? (v << (off - lo)) : (v >> (lo - off));
     }
     keys[i] = k;
 }
@@ -163,6 +212,31 @@ int rows_select_workspace(int64_t n, int64_t* bytes) {
     return 0;
 }
 
+namespace {
+
+int bit_width(long long v) {
+    int b = 1;
+    while (b < 63 && (v >> b) != 0) ++b;
+    return b;
+}
+
+KeyLayout key_layout(int max_rx, int max_tx, int max_id1) {
+    KeyLayout L;
+    const int id_bits = bit_width(max_id1);
+    const int widths[kKeyFields] = {id_bits, id_bits, id_bits, id_bits, id_bits, id_bits, id_bits, 3, 3,
+                                    bit_width(max_tx), bit_width(max_rx)};
+    int o = 0;
+    for (int f = 0; f < kKeyFields; ++f) {
+        L.offset[f] = o;
+        L.bits[f] = widths[f];
+        o += widths[f];
+    }
+    L.total = o;
+    return L;
+}
+
+}  // namespace
+
 int rows_select(const void* rows_v, int64_t n, int width, int64_t max_paths, int scope, int64_t* selected,
                 int64_t* num_selected, void* ws, int64_t ws_bytes, cudaStream_t stream) {
     if (n < 0 || n > INT_MAX - 1) return 1;
@@ -182,45 +256,67 @@ int rows_select(const void* rows_v, int64_t n, int width, int64_t max_paths, int
     void* tmp = b + L.tmp;
     long long* kept = reinterpret_cast<long long*>(b + L.kept);
     const int grid = int((n + kB - 1) / kB);
+    // every CUDA call and launch is checked; any failure returns WCB_ERR_CUDA (2)
+    bool ok = true;
+    auto chk = [&](cudaError_t e) { ok = ok && e == cudaSuccess; };
+    // key widths: the largest rx, tx and id + 1 (in `scan`, free until the dedup)
+    int maxima[3] = {0, 0, 0};
+    chk(cudaMemsetAsync(scan, 0, 3 * sizeof(int), stream));
+    k_key_max<<<grid, kB, 0, stream>>>(n, rows, scan);
+    chk(cudaGetLastError());
+    chk(cudaMemcpyAsync(maxima, scan, sizeof(maxima), cudaMemcpyDeviceToHost, stream));
+    chk(cudaStreamSynchronize(stream));
+    if (!ok) return 2;
+    const KeyLayout K = key_layout(maxima[0], maxima[1], maxima[2]);
     k_iota<<<grid, kB, 0, stream>>>(n, idx);
-    note_launch();
-    const int end_bits[4] = {18, 54, 54, 38};
-    for (int w = 0; w < 4; ++w) {
-        k_row_key<<<grid, kB, 0, stream>>>(n, rows, idx, w, keys);
+    chk(cudaGetLastError());
+    note_launch(2);
+    const int words = (K.total + 63) / 64;
+    for (int w = 0; w < words && ok; ++w) {
+        k_row_key<<<grid, kB, 0, stream>>>(n, rows, idx, K, w, keys);
+        chk(cudaGetLastError());
         size_t tb = L.tmp_bytes;
-        cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, idx, idx2, int(n), 0, end_bits[w], stream);
+        chk(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, idx, idx2, int(n), 0,
+                                            std::min(64, K.total - 64 * w), stream));
         std::swap(idx, idx2);
         note_launch(2);
     }
     k_group_start<<<grid, kB, 0, stream>>>(n, rows, idx, width, start);
+    chk(cudaGetLastError());
     k_winner<<<grid, kB, 0, stream>>>(n, rows, idx, start, keep);
+    chk(cudaGetLastError());
     size_t tb = L.tmp_bytes;
-    cub::DeviceScan::InclusiveSum(tmp, tb, keep, scan, int(n), stream);
+    chk(cub::DeviceScan::InclusiveSum(tmp, tb, keep, scan, int(n), stream));
     k_gather_selected<<<grid, kB, 0, stream>>>(n, idx, keep, scan, kept);
+    chk(cudaGetLastError());
     note_launch(4);
     int count = 0;
-    cudaMemcpyAsync(&count, scan + n - 1, 4, cudaMemcpyDeviceToHost, stream);
-    if (cudaStreamSynchronize(stream) != cudaSuccess) return 2;
+    chk(cudaMemcpyAsync(&count, scan + n - 1, 4, cudaMemcpyDeviceToHost, stream));
+    chk(cudaStreamSynchronize(stream));
+    if (!ok) return 2;
     long long final_count = count;
     if (max_paths >= 0 && scope == 0) {
         final_count = std::min<long long>(count, max_paths);
-        cudaMemcpyAsync(selected, kept, size_t(final_count) * 8, cudaMemcpyDeviceToDevice, stream);
+        chk(cudaMemcpyAsync(selected, kept, size_t(final_count) * 8, cudaMemcpyDeviceToDevice, stream));
     } else if (max_paths >= 0 && scope == 1 && count > 0) {
         const int g2 = int((count + kB - 1) / kB);
-        cudaMemsetAsync(keep, 0, size_t(count) * 4, stream);
+        chk(cudaMemsetAsync(keep, 0, size_t(count) * 4, stream));
         k_pair_limit<<<g2, kB, 0, stream>>>(count, rows, kept, max_paths, keep);
+        chk(cudaGetLastError());
         tb = L.tmp_bytes;
-        cub::DeviceScan::InclusiveSum(tmp, tb, keep, scan, int(count), stream);
+        chk(cub::DeviceScan::InclusiveSum(tmp, tb, keep, scan, int(count), stream));
         k_gather_selected64<<<g2, kB, 0, stream>>>(count, kept, keep, scan, reinterpret_cast<long long*>(selected));
+        chk(cudaGetLastError());
         note_launch(3);
         int c2 = 0;
-        cudaMemcpyAsync(&c2, scan + count - 1, 4, cudaMemcpyDeviceToHost, stream);
-        if (cudaStreamSynchronize(stream) != cudaSuccess) return 2;
+        chk(cudaMemcpyAsync(&c2, scan + count - 1, 4, cudaMemcpyDeviceToHost, stream));
+        chk(cudaStreamSynchronize(stream));
         final_count = c2;
     } else {
-        cudaMemcpyAsync(selected, kept, size_t(count) * 8, cudaMemcpyDeviceToDevice, stream);
+        chk(cudaMemcpyAsync(selected, kept, size_t(count) * 8, cudaMemcpyDeviceToDevice, stream));
     }
-    if (cudaStreamSynchronize(stream) != cudaSuccess) return 2;
+    chk(cudaStreamSynchronize(stream));
+    if (!ok) return 2;
     *num_selected = final_count;
     return 0;
 }

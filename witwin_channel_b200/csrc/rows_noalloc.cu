@@ -10,21 +10,26 @@
 // buffer; everything else the sort, dedup and max_paths stages need comes
 // from g_select_scratch below.
 //
-// Set-up: the first call on each device (with that device current) looks up
-// the array's device address with cudaGetSymbolAddress and caches it.  That
-// lookup may make the CUDA runtime load this library's module onto the
-// device, so make the first call on a device before any stream capture
-// begins.  Later calls only read the cached address.
+// Set-up: every call looks up the array's device address on the current
+// device with cudaGetSymbolAddress (nothing is cached, so a cudaDeviceReset
+// or a different context on the device never leaves a stale address behind).
+// The first lookup on a device may make the CUDA runtime load this library's
+// module there, so make the first call on a device before any stream capture
+// begins; later lookups are a table read.
+//
+// Synchronisation: like wcb_rows_select, the call reads its counts back to
+// the host and synchronises `stream` before it returns, so it blocks the
+// calling thread for the duration of the selection and cannot run inside a
+// stream capture.
 //
 // Sharing: every call on a device uses the same array and leaves its last
 // contents there.  Each stage writes the scratch words it later reads (the
-// one buffer that must start at zero, the per-pair keep flags, is cleared by
-// the call itself), so no state leaks from one call into the next; but two
+// buffers that must start at zero, the key-width maxima and the per-pair keep
+// flags, are cleared by the call itself), so no state leaks from one call
+// into the next; but two
 // calls that overlap in time -- on two streams, or from two host threads --
 // race on the array and corrupt each other's results.  Serialise them.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "../../include/witwin_channel_b200.h"
 #include "internal.h"
@@ -33,25 +38,16 @@ namespace wcb {
 namespace {
 
 constexpr long long kScratchBytes = WCB_ROWS_SELECT_NOALLOC_SCRATCH_BYTES;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_select_scratch[kScratchBytes];
 
-std::mutex g_setup_mutex;
-void* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of g_select_scratch on the current device (cached).
+// Device address of g_select_scratch in the current device's context.  In
+// host code the array's name is only a host-side handle; the kernels get this
+// address.
 int scratch_address(void** out) {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess) return WCB_ERR_CUDA;
-    if (dev < 0 || dev >= kMaxDevices) return WCB_ERR_NOT_SUPPORTED;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (g_scratch_addr[dev] == nullptr) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_select_scratch) != cudaSuccess || p == nullptr) return WCB_ERR_CUDA;
-        g_scratch_addr[dev] = p;
-    }
-    *out = g_scratch_addr[dev];
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_select_scratch) != cudaSuccess || p == nullptr) return WCB_ERR_CUDA;
+    *out = p;
     return WCB_OK;
 }
 

@@ -476,22 +476,26 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
         if (!sel[e]) continue;
         EdgeDev ed;
         std::memset(&ed, 0, sizeof(ed));
-        auto dir = edir[e];
-        auto t0 = norm3(cross3(n0o[e], dir));
+        // Wedge frame of the reference's ray-tracing library: the record's own
+        // direction (v0 -> v1) and t0 = normalize(n0 x dir), phi measured from t0
+        // towards n0 (native/channel/kernels/diffraction.cu:450-452).  The
+        // ordered normals make t0 point into face 0 of an interior wedge; a
+        // half-plane's t0 may point away from its sheet.
+        const auto dir = edir[e];
+        const auto t0 = norm3(cross3(n0o[e], dir));
         std::array<double, 3> to_opp = {opp0[e][0] - epos[e][0], opp0[e][1] - epos[e][1], opp0[e][2] - epos[e][2]};
-        const bool flipped = dot3(to_opp, t0) < 0.0;
-        if (flipped) {
-            dir = {-dir[0], -dir[1], -dir[2]};
-            t0 = {-t0[0], -t0[1], -t0[2]};
-        }
-        edge_topo.push_back(flipped ? recs[e].v1 : recs[e].v0);
-        edge_topo.push_back(flipped ? recs[e].v0 : recs[e].v1);
+        const bool into_face0 = dot3(to_opp, t0) >= 0.0;
+        edge_topo.push_back(recs[e].v0);
+        edge_topo.push_back(recs[e].v1);
         edge_topo.push_back(fn0[e]);
         edge_topo.push_back(fn1[e]);
+        // visibility offset: the exterior bisector; for a half-plane the in-plane
+        // direction away from the sheet
         std::array<double, 3> bis = {n0o[e][0] + n1o[e][0], n0o[e][1] + n1o[e][1], n0o[e][2] + n1o[e][2]};
         double bl = std::sqrt(dot3(bis, bis));
         if (bl > 1e-6) bis = {bis[0] / bl, bis[1] / bl, bis[2] / bl};
-        else bis = {-t0[0], -t0[1], -t0[2]};
+        else if (into_face0) bis = {-t0[0], -t0[1], -t0[2]};
+        else bis = t0;
         for (int k = 0; k < 3; ++k) {
             ed.pos[k] = epos[e][k];
             ed.dir[k] = dir[k];
@@ -506,6 +510,7 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
         ed.face1 = face1[e];
         ed.mat_face0 = mat0[e];
         ed.mat_face1 = mat1[e] >= 0 ? mat1[e] : mat0[e];
+        ed.face_n = face1[e] >= 0 ? 1 : 0;
         ed.edge_id = e;
         edges.push_back(ed);
         edge_ids.push_back(e);
@@ -552,6 +557,7 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
     // ---- BVH (host binned SAH) and triangles in leaf order
     sd.root = INT_MIN;
     sd.max_depth = 0;
+    sd.stack_entries = 8;
     if (F > 0) {
         std::vector<BvhNode> host_nodes;
         std::vector<int> slot_face;
@@ -581,6 +587,7 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
         if (sd.tri == nullptr || sd.nodes == nullptr) { scene_destroy(h); return 2; }
         sd.root = F > 1 ? 0 : ~0;
         sd.max_depth = hdepth;
+        sd.stack_entries = std::max(8, std::min(kStackDepth, hdepth + 2));
         h->num_nodes = std::max(F - 1, 0);
     }
     if (cudaStreamSynchronize(stream) != cudaSuccess) { scene_destroy(h); return 2; }

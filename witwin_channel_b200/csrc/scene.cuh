@@ -25,6 +25,7 @@ struct SceneDev {
     int num_edges;        // selected edges
     int root;             // root child reference (internal node index, or ~slot, or INT_MIN when empty)
     int max_depth;        // BVH depth (root = 0)
+    int stack_entries;    // traversal stack entries per thread (BVH depth + 2, at most kStackDepth)
     // geometry
     const float* vertices;     // (V,3)
     const int* faces;          // (F,3)

@@ -661,7 +661,11 @@ int solve_workspace_size(const SceneHandle* h, const wcb_solve_desc* d, int64_t*
 
 int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m, const wcb_outputs* out, void* ws,
           int64_t ws_bytes, cudaStream_t stream) {
-    const SceneDev& sc = h->dev;
+    // the scene record with this solve's traversal stack size: the BVH depth
+    // bound, or the caller's smaller override (a descent that would push past
+    // it drops the far subtree and sets status bit 0; no write leaves the stack)
+    SceneDev sc = h->dev;
+    if (d->stack_entries > 0) sc.stack_entries = std::min(std::max(d->stack_entries, 1), kStackDepth);
     if (d->num_tx < 0 || d->num_freq < 1 || d->max_depth < 0 || d->max_depth > kMaxDepth) return 1;
     const int rays = d->discovery_rays > 0 ? d->discovery_rays : 262144;
     const int T = d->num_tx;
@@ -702,6 +706,7 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     cudaMemsetAsync(overflow, 0, 64, stream);
     if (out->status) cudaMemsetAsync(out->status, 0, 4, stream);
     if (out->row_count) cudaMemsetAsync(out->row_count, 0, 8, stream);
+    if (out->transmission_overflow) cudaMemsetAsync(out->transmission_overflow, 0, 8, stream);
     // chain offsets (in chain-int units, per tx)
     std::vector<long long> offs(size_t(T) * kMaxDepth);
     std::vector<int> fixed_counts(size_t(T) * kMaxDepth, 0);
@@ -711,7 +716,7 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     const int B = 256;
     // traversal stacks: a descent pushes at most one entry per tree level, so
     // the measured BVH depth (+2) bounds them
-    const size_t smem = size_t(std::max(8, std::min(kStackDepth, sc.max_depth + 2))) * kBlock * 4;
+    const size_t smem = size_t(sc.stack_entries) * kBlock * 4;
     int* err = out->status;
     // The reflection candidates (discovery, chain tables) and the reflection
     // kernel run on a side stream, overlapping the edge prefilter, the LoS and
@@ -891,12 +896,15 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     p.row_capacity = out->rows ? out->row_capacity : 0;
     p.row_counter = reinterpret_cast<unsigned long long*>(out->row_count);
     p.status = out->status;
-    p.overflow_counter = overflow;
+    // transmission segments crossing more than max_depth walls: the caller's
+    // counter when given (zeroed above), else the workspace's
+    p.overflow_counter = out->transmission_overflow ? reinterpret_cast<unsigned long long*>(out->transmission_overflow)
+                                                    : overflow;
     p.ray_counter = prof.enabled ? main_ray_counter : nullptr;
     p.num_freq_total = d->num_freq;
     const long long tiles = tiles_per_tx(p) * T;
     const long long blocks = (tiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    const int sdepth = std::max(8, std::min(kStackDepth, sc.max_depth + 2));
+    const int sdepth = sc.stack_entries;
     const size_t stack_bytes = size_t(sdepth) * kCompBlock * 4;
     if (prof.enabled) cudaEventRecord(ev_main0, stream);
     ComponentEvents cev;

@@ -93,6 +93,10 @@ WCB_D bool box_hit(const Ray<G>& r, G lx, G ly, G lz, G hx, G hy, G hz, G tmax, 
     return tn <= tf;
 }
 
+// a*b - c*d without contraction into a fused multiply-add
+WCB_D float edge_fn(float a, float b, float c, float d) { return __fsub_rn(__fmul_rn(a, b), __fmul_rn(c, d)); }
+WCB_D double edge_fn(double a, double b, double c, double d) { return __dsub_rn(__dmul_rn(a, b), __dmul_rn(c, d)); }
+
 // Watertight ray/triangle test.  Returns t (ray parameter) or +inf.
 template <typename G>
 WCB_D G tri_hit(const Ray<G>& r, float4 a4, float4 b4, float4 c4) {
@@ -105,13 +109,18 @@ WCB_D G tri_hit(const Ray<G>& r, float4 a4, float4 b4, float4 c4) {
     const G Ax = comp(A0, kx) - Sx * comp(A0, kz), Ay = comp(A0, ky) - Sy * comp(A0, kz);
     const G Bx = comp(B0, kx) - Sx * comp(B0, kz), By = comp(B0, ky) - Sy * comp(B0, kz);
     const G Cx_ = comp(C0, kx) - Sx * comp(C0, kz), Cy = comp(C0, ky) - Sy * comp(C0, kz);
-    G U = Cx_ * By - Cy * Bx;
-    G V = Ax * Cy - Ay * Cx_;
-    G W = Bx * Ay - By * Ax;
+    // Edge functions with every product rounded on its own: a shared edge's
+    // function in the two adjacent triangles is then the exact negation of
+    // the other (the watertightness argument), which a fused multiply-add of
+    // one product into the subtraction would break (both could round to the
+    // same sign and the crossing would leak between the triangles).
+    G U = edge_fn(Cx_, By, Cy, Bx);
+    G V = edge_fn(Ax, Cy, Ay, Cx_);
+    G W = edge_fn(Bx, Ay, By, Ax);
     if (sizeof(G) == 4 && (U == G(0) || V == G(0) || W == G(0))) {
-        U = G(double(Cx_) * double(By) - double(Cy) * double(Bx));
-        V = G(double(Ax) * double(Cy) - double(Ay) * double(Cx_));
-        W = G(double(Bx) * double(Ay) - double(By) * double(Ax));
+        U = G(edge_fn(double(Cx_), double(By), double(Cy), double(Bx)));
+        V = G(edge_fn(double(Ax), double(Cy), double(Ay), double(Cx_)));
+        W = G(edge_fn(double(Bx), double(Ay), double(By), double(Ax)));
     }
     const G inf = sizeof(G) == 4 ? G(__int_as_float(0x7f800000)) : G(__longlong_as_double(0x7ff0000000000000LL));
     if ((U < G(0) || V < G(0) || W < G(0)) && (U > G(0) || V > G(0) || W > G(0))) return inf;
@@ -190,7 +199,7 @@ WCB_D bool traverse(const SceneDev& sc, Ray<G> r, const Ignore& ig, int* stack, 
             const bool first0 = n0 <= n1;
             const int near_c = first0 ? d.x : d.y;
             const int far_c = first0 ? d.y : d.x;
-            if (sp < kStackDepth) {
+            if (sp < sc.stack_entries) {
                 stack[sp * stride + lane] = far_c;
                 ++sp;
             } else {

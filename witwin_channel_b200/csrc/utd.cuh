@@ -179,17 +179,17 @@ WCB_HD Cx<T> kp_term(T beta, T n, T kl, int s) {
 // Selected diffraction edge (device layout, FP64 geometry).
 struct EdgeDev {
     double pos[3];     // midpoint
-    double dir[3];     // unit edge direction, oriented so t0 = n0 x dir points into face 0
-    double t0[3];      // unit face-0 tangent
+    double dir[3];     // unit edge direction of the record (v0 -> v1)
+    double t0[3];      // unit face-0 tangent normalize(n0 x dir)
     double n0[3];      // ordered outward normal of face 0
     double n1[3];      // ordered outward normal of face n
     double half_length;
     double n;          // exterior angle / pi
     double bisector[3];  // unit exterior bisector used for the visibility bias
     int face0, face1;    // reference face ids (visibility ignore set)
-    int mat_face0, mat_face1;  // faces whose slab gives R_0 and R_n
+    int mat_face0, mat_face1;  // faces whose material gives R_0 and R_n
     int edge_id;         // reference edge id
-    int pad;
+    int face_n;          // 1: a second face bounds the wedge; 0: half-plane, R_n = 0
 };
 
 template <typename T>
@@ -214,6 +214,7 @@ template <typename G>
 struct EdgeFrame {
     V3<G> c, e, t0, n0, bisector;
     G half_length, n;
+    bool face_n;  // false for a half-plane: its second face is absent (R_n = 0)
 };
 
 WCB_HD EdgeFrame<double> edge_frame(const EdgeDev& ed) {
@@ -225,6 +226,7 @@ WCB_HD EdgeFrame<double> edge_frame(const EdgeDev& ed) {
     f.bisector = v3(ed.bisector[0], ed.bisector[1], ed.bisector[2]);
     f.half_length = ed.half_length;
     f.n = ed.n;
+    f.face_n = ed.face_n != 0;
     return f;
 }
 
@@ -307,13 +309,14 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
     const T unit = s_sqrt(T(kTwoPi) / kl);
     const T delta_w = T(4) * unit;
     const T delta_b = T(kCBlend) * unit;
-    // face factors
-    const T wavelength = T(G(kC0) / frequency);
-    Cx<T> r0_te, r0_tm, rn_te, rn_tm;  // faces 0 and n, through one inlined copy
+    // face factors: interface (half-space) Fresnel at the wedge angles; a
+    // half-plane's absent second face reflects nothing
+    Cx<T> r0_te, r0_tm, rn_te = cx(T(0), T(0)), rn_tm = cx(T(0), T(0));  // faces 0 and n, one inlined copy
+    const int faces = ed.face_n ? 2 : 1;
 #pragma unroll 1
-    for (int face = 0; face < 2; ++face) {
+    for (int face = 0; face < faces; ++face) {
         Cx<T> te, tm;
-        slab_fresnel(s_sin(face == 0 ? phi_p : npi - phi), face == 0 ? m0 : mn, frequency, wavelength, &te, &tm);
+        halfspace_fresnel(s_sin(face == 0 ? phi_p : npi - phi), face == 0 ? m0 : mn, frequency, &te, &tm);
         if (face == 0) {
             r0_te = te;
             r0_tm = tm;

@@ -223,6 +223,12 @@ def _metadata(config: Config, counts: dict, path_count: int, launches: int, extr
     return meta
 
 
+def _component_counts(component_id: torch.Tensor) -> dict[str, int]:
+    """Rows per component (one device-to-host copy)."""
+    n = torch.bincount(component_id.to(torch.int64), minlength=8).cpu().tolist() if component_id.numel() else [0] * 8
+    return {name: int(n[c]) for name, c in (("los", 0), ("reflection", 1), ("diffraction", 2), ("transmission", 5))}
+
+
 def _needs_rows(config: Config) -> bool:
     return config.export_paths or config.max_paths is not None or config.ad_mode != "none"
 
@@ -239,9 +245,10 @@ def solve(scene: Any, config: Config, *, reference_frequency_hz, precision: str 
         raise TypeError("config must be a witwin_channel_b200.deterministic.Config")
     frequency = _frequency_value(reference_frequency_hz)
     _validate(scene, config)
-    if config.ad_mode == "jvp":
-        raise NotImplementedError("forward-mode AD (ad_mode='jvp') is not provided; use ad_mode='vjp'")
-    if config.ad_mode == "vjp":
+    if config.ad_mode in ("vjp", "jvp"):
+        # one differentiable fixed-topology forward serves both modes: reverse
+        # mode through backward(), forward mode through the jvp of the same
+        # autograd Function when the scene values are forward-mode dual tensors
         from .autograd import solve_vjp
 
         return solve_vjp(scene, config, reference_frequency_hz)
@@ -269,17 +276,18 @@ def solve(scene: Any, config: Config, *, reference_frequency_hz, precision: str 
         cells = engine.accumulate_rows(rows, selected, ev["path_gain"], ev["path_field"], ev["field_xyz"], ep.tx_power,
                                        T, R, config.coherent)
         dec = engine.decode_rows(rows, selected)
-        cid = dec["component_id"]
-        for name, c in (("los", 0), ("reflection", 1), ("diffraction", 2), ("transmission", 5)):
-            counts[name] = int((cid == c).sum().item())
+        counts.update(_component_counts(dec["component_id"]))
         path_count = int(selected.shape[0])
         if config.export_paths:
             paths = _path_table(dec, ev, width, compiled, config.return_field)
     else:
         cells = engine.alloc_cells(1, T, R, device, fp64=(prec == _native.PRECISION_FP64))
-        engine.run_solve(compiled, ep, mats, [frequency], components=bits, max_depth=config.max_depth,
-                         coherent=config.coherent, precision=prec, cells=cells)
+        res = engine.run_solve(compiled, ep, mats, [frequency], components=bits, max_depth=config.max_depth,
+                               coherent=config.coherent, precision=prec, cells=cells)
         path_count = -1
+    if "transmission" in config.components:
+        # tx-rx segments crossing more than max_depth walls (no transmission path)
+        extra["transmission_overflow"] = int(res["transmission_overflow"].item())
     rx = ep.rx
     path_gain = cells.path_gain[0]
     field = cells.field[0]

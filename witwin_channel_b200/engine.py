@@ -43,7 +43,8 @@ class Endpoints:
 
 
 def make_desc(ep: Endpoints, frequencies: list[float], components: int, max_depth: int, coherent: bool,
-              precision: int = _native.PRECISION_MIXED, discovery_rays: int = 0) -> tuple[_native.SolveDesc, Any]:
+              precision: int = _native.PRECISION_MIXED, discovery_rays: int = 0,
+              stack_entries: int = 0) -> tuple[_native.SolveDesc, Any]:
     d = _native.SolveDesc()
     d.num_tx = ep.num_tx
     d.tx_pos = _native.ptr(ep.tx_pos)
@@ -75,6 +76,7 @@ def make_desc(ep: Endpoints, frequencies: list[float], components: int, max_dept
     d.coherent = int(bool(coherent))
     d.precision = precision
     d.discovery_rays = discovery_rays
+    d.stack_entries = int(stack_entries)
     return d, freqs
 
 
@@ -82,7 +84,7 @@ def check_device_status(status: torch.Tensor) -> None:
     """Raise if a solve's device status word has a failure bit set (reads it: a sync)."""
     st = int(status.item())
     if st != 0:
-        raise RuntimeError(f"native solve reported device status bits {st:#x} (traversal stack overflow)")
+        raise RuntimeError(f"native solve reported device status bits {st:#x} (bit 0: traversal stack overflow)")
 
 
 def component_bits(components) -> int:
@@ -139,16 +141,22 @@ def alloc_cells(nf: int, T: int, R: int, device: torch.device, fp64: bool = Fals
 def run_solve(compiled: CompiledScene, ep: Endpoints, mats: MaterialTables, frequencies: list[float], *,
               components: int, max_depth: int, coherent: bool, precision: int = _native.PRECISION_MIXED,
               cells: CellOutputs | None = None, want_rows: bool = False, row_capacity: int | None = None,
-              discovery_rays: int = 0, check_status: bool = True, workspace: Workspace | None = None) -> dict:
+              discovery_rays: int = 0, check_status: bool = True, workspace: Workspace | None = None,
+              retry: bool = True, stack_entries: int = 0) -> dict:
+    """One ``wcb_solve``.  With ``want_rows`` a row buffer shorter than the
+    solve needs returns ``WCB_ERR_CAPACITY``; the solve then runs again with
+    the reported count (``retry``) or the error is raised.  ``stack_entries``
+    overrides the traversal stack size (0: the scene's BVH depth + 2)."""
     lib = _native.load()
     device = ep.tx_pos.device
-    desc, keep = make_desc(ep, frequencies, components, max_depth, coherent, precision, discovery_rays)
+    desc, keep = make_desc(ep, frequencies, components, max_depth, coherent, precision, discovery_rays, stack_entries)
     nbytes = ctypes.c_int64()
     _native.check(lib.wcb_solve_workspace_size(compiled.native.handle, ctypes.byref(desc), ctypes.byref(nbytes)),
                   "wcb_solve_workspace_size")
     ws = (workspace or _WORKSPACE).get(nbytes.value, device)
     status = torch.zeros(1, dtype=torch.int32, device=device)
     row_count = torch.zeros(1, dtype=torch.int64, device=device)
+    trans_overflow = torch.zeros(1, dtype=torch.int64, device=device)
     # row capacity: the caller's, else the last count seen on this scene (with
     # headroom), else 8 records per cell; a short buffer makes the solve run again
     hint = compiled.row_count_hint
@@ -166,17 +174,18 @@ def run_solve(compiled: CompiledScene, ep: Endpoints, mats: MaterialTables, freq
         out.row_capacity = capacity if want_rows else 0
         out.row_count = _native.ptr(row_count)
         out.status = _native.ptr(status)
+        out.transmission_overflow = _native.ptr(trans_overflow)
         rc = lib.wcb_solve(compiled.native.handle, ctypes.byref(desc), ctypes.byref(mats_struct := mats.as_struct()),
                            ctypes.byref(out), _native.ptr(ws), ws.numel(), _native.stream_handle(device))
         del mats_struct
-        if rc == _native.WCB_ERR_CAPACITY and want_rows:
+        if rc == _native.WCB_ERR_CAPACITY and want_rows and retry:
             capacity = int(int(row_count.item()) * 1.25) + 1024
             continue
         _native.check(rc, "wcb_solve")
         break
     if check_status:
         check_device_status(status)
-    result = {"desc": desc, "keep": keep, "status": status, "workspace": ws}
+    result = {"desc": desc, "keep": keep, "status": status, "workspace": ws, "transmission_overflow": trans_overflow}
     if want_rows:
         n = int(row_count.item())
         result["rows"] = rows[:n]

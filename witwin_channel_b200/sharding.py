@@ -5,8 +5,10 @@ are independent: each rank owns a disjoint slice of them, solves it with no
 collective on the data path, and the per-rank outputs are joined by
 concatenation.  The only collectives are the step-time reduction (max over
 ranks) and, when a caller wants the whole map on every rank, one all-gather
-of the outputs at the end.  Works with any ``torch.distributed`` backend
-(NCCL on GPUs, gloo on CPU tensors).
+of the outputs at the end.  A gradient step over a sharded job (a loss that
+is a sum over the ranks' cells) needs one exchange: the sum of the ranks'
+dense gradients, one all-reduce of one FP64 buffer.  Works with any
+``torch.distributed`` backend (NCCL on GPUs, gloo on CPU tensors).
 """
 
 from __future__ import annotations
@@ -54,3 +56,42 @@ def gather_concat(local: torch.Tensor, group=None) -> torch.Tensor:
     parts = [torch.empty_like(padded) for _ in range(world)]
     dist.all_gather(parts, padded.contiguous(), group=group)
     return torch.cat([p[:s] for p, s in zip(parts, sizes)], dim=0)
+
+
+def shard_grid(grid, rank: int, world: int):
+    """Rows ``[start, stop)`` of receiver grid ``grid`` (``shard_range`` over
+    its first axis) as a grid of their own: same axes, spacing and
+    polarisation, origin moved to row ``start`` (its points equal the full
+    grid's rows up to the FP32 rounding of the moved origin).  Returns
+    ``(sub_grid, (start, stop))``."""
+    from .scene import make_receiver_grid
+
+    start, stop = shard_range(int(grid.shape[0]), rank, world)
+    origin = grid.origin.detach().double() + grid.x_axis.detach().double() * (start * float(grid.spacing[0]))
+    sub = make_receiver_grid(origin=origin.float(), x_axis=grid.x_axis, y_axis=grid.y_axis,
+                             shape=(stop - start, int(grid.shape[1])), spacing=grid.spacing,
+                             polarization=grid.polarization)
+    return sub, (start, stop)
+
+
+def allreduce_gradients(tensors, group=None) -> None:
+    """Sum the ``.grad`` of every tensor in ``tensors`` over the ranks, in
+    place: the dense gradients (vertices, materials, frequency, transmitter
+    positions...) are packed in list order into one FP64 buffer, reduced by
+    one ``all_reduce(SUM)`` and unpacked; a missing gradient counts as zero.
+    Every rank must pass the same tensors in the same order.  With NCCL the
+    buffer lives on the current CUDA device."""
+    if not (dist.is_available() and dist.is_initialized()):
+        return
+    if not tensors:
+        return
+    grads = [t.grad if t.grad is not None else torch.zeros_like(t) for t in tensors]
+    backend = dist.get_backend(group)
+    device = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    flat = torch.cat([g.detach().reshape(-1).to(device=device, dtype=torch.float64) for g in grads])
+    dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+    offset = 0
+    for t, g in zip(tensors, grads):
+        n = g.numel()
+        t.grad = flat[offset:offset + n].reshape(t.shape).to(device=t.device, dtype=t.dtype)
+        offset += n

@@ -192,9 +192,10 @@ def batched_scenes() -> list[Scene]:
 
 
 def large_city_scene(seed: int = 4, grid_side: int = 1024) -> tuple[Scene, float]:
-    """2048 boxes on 46x46 lots, roofs subdivided 4x4 (walls split to match,
-    ~112k triangles), 25% of boxes with an interior two-layer glass sheet, 1 Tx at 25 m,
-    1024^2 grid at 1 m spacing, 28 GHz."""
+    """2048 boxes on 46x46 lots, roofs subdivided k x k with k = 4 on even and
+    5 on odd boxes (walls split to match so the mesh has no T-junctions:
+    ~134k triangles), 25% of boxes with an interior two-layer glass sheet, 1 Tx
+    at 25 m, 1024^2 grid at 1 m spacing, 28 GHz."""
     layout = city_layout(2048, seed, lots=46)
     rng = np.random.default_rng(seed + 2000)
     sheets = []
@@ -202,7 +203,7 @@ def large_city_scene(seed: int = 4, grid_side: int = 1024) -> tuple[Scene, float
         if rng.uniform() < 0.25:
             cx = 0.5 * (x0 + x1)
             sheets.append(((cx, y0 + 0.5), (cx, y1 - 0.5), 0.8 * h))
-    structures = city_scene(layout, roof_k=lambda b: 4, sheets=sheets)
+    structures = city_scene(layout, roof_k=lambda b: 4 if b % 2 == 0 else 5, sheets=sheets)
     tx = street_point(layout, np.random.default_rng(seed + 1000), 25.0)
     origin = (-(grid_side - 1) / 2.0, -(grid_side - 1) / 2.0, 1.5)
     grid = make_receiver_grid(origin=origin, x_axis=(1.0, 0.0, 0.0), y_axis=(0.0, 1.0, 0.0),
