@@ -68,6 +68,20 @@ int wcb_scene_create(const float* vertices, int64_t num_vertices, const int32_t*
                      int32_t boundary_half_plane, int32_t vertical_only, double vertical_ratio, void* stream,
                      wcb_scene** out);
 int wcb_scene_destroy(wcb_scene* scene);
+/* Moves a compiled scene's vertices in place (the reference recompiles the
+ * scene when its mesh changes: scene/compiler.py:1306-1450 behind the compile
+ * cache of deterministic.py:960-971).  `vertices` (V,3) f32 device, V as at
+ * create.  The compile's discrete decisions (coplanar groups, edge selection
+ * and wedge order, shared-boundary merges, the edge policy) are recomputed
+ * from the new vertices and compared with the compiled ones first; if any
+ * differs, nothing is changed and *topology_changed (host) is set to 1: the
+ * caller must create the scene again.  Otherwise face planes, group planes
+ * and boxes, edge frames, leaf triangles and the BVH boxes are recomputed on
+ * the device (the BVH topology is kept) and *topology_changed is 0.  Reads
+ * back two small values (one stream synchronisation); the mesh stays on the
+ * device. */
+int wcb_scene_refit(wcb_scene* scene, const float* vertices, int64_t num_vertices, int32_t* topology_changed,
+                    void* stream);
 /* counts[0..5] = faces, groups, selected edges, bvh depth, bvh nodes, representative faces */
 int wcb_scene_info(const wcb_scene* scene, int64_t* counts);
 /* Group table export: face_group (F) i32, group_rep (G) i32 (device). */
@@ -307,7 +321,9 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
  * layout[8]); each record is re-evaluated once in FP64 with one dual lane
  * seeded by it.  Writes row_field_tangent (K,2) FP64, the directional
  * derivative of each record's powered path field (real, imag), and optionally
- * row_field (K,2) FP64, the re-evaluated field.  No workspace, no host sync. */
+ * row_field (K,2) FP64, the re-evaluated field.  With tangent NULL only
+ * row_field is written (a plain FP64 evaluation, no dual lane): the records'
+ * fields the derivatives are linearised at.  No workspace, no host sync. */
 int wcb_rows_jvp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_materials* materials,
                  int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
                  const double* tangent, int64_t tangent_size, double* row_field, double* row_field_tangent,

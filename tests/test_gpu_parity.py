@@ -219,7 +219,10 @@ def test_compiled_scene_is_cached_and_invalidated():
     a = compile_scene(scene, dev)
     assert compile_scene(scene, dev) is a
     with _t.no_grad():
-        scene.structures[0].vertices.add_(0.0)  # bumps the tensor version: geometry may have changed
+        scene.structures[0].vertices.add_(0.0)  # bumps the tensor version: the vertices are re-read
+    assert compile_scene(scene, dev) is a  # ... and refitted in place (no compile decision changed)
+    st = scene.structures[0]
+    st.geometry.faces = st.faces.flip(1).clone()  # a new face tensor: compiled again
     assert compile_scene(scene, dev) is not a
 
 

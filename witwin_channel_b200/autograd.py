@@ -66,10 +66,9 @@ def _linearisation(state: _State, fi: int) -> dict:
     frequency ``fi``: the point the derivatives of |sum field|^2 are taken at.
     (The FP32 forward values would do for most losses, but a loss whose cell
     terms cancel amplifies their rounding into the gradient.)  Computed once
-    per frequency by one zero-tangent ``wcb_rows_jvp`` pass and cached."""
+    per frequency by one plain FP64 ``wcb_rows_jvp`` pass (no tangent) and cached."""
     if state.saved64[fi] is None:
-        zero = torch.zeros(max(state.param_total, 1), dtype=torch.float64, device=state.rows.device)
-        field, _ = rows_jvp(state, fi, zero)
+        field, _ = rows_jvp(state, fi, None)
         re, im = field[:, 0].contiguous(), field[:, 1].contiguous()
         gain = (re * re + im * im).contiguous()
         f_ = state.flat
@@ -168,9 +167,10 @@ def _param_total(compiled, ep, mats, frequencies, bits, config) -> int:
     return int(layout[8])
 
 
-def rows_jvp(state: _State, freq_index: int, tangent: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor]:
+def rows_jvp(state: _State, freq_index: int, tangent: torch.Tensor | None) -> tuple[torch.Tensor, torch.Tensor]:
     """Per-record FP64 path field and its directional derivative ((K,2) each)
-    for a dense FP64 tangent over the native parameter layout (``wcb_rows_jvp``)."""
+    for a dense FP64 tangent over the native parameter layout (``wcb_rows_jvp``);
+    with ``tangent`` None the fields alone (the derivative is returned as zeros)."""
     lib = _native.load()
     device = state.rows.device
     desc, keep = engine.make_desc(state.ep, state.frequencies, state.components, state.max_depth, state.coherent)
@@ -178,12 +178,13 @@ def rows_jvp(state: _State, freq_index: int, tangent: torch.Tensor) -> tuple[tor
     K = int(state.selected.shape[0])
     field = torch.zeros((max(K, 1), 2), dtype=torch.float64, device=device)
     dfield = torch.zeros((max(K, 1), 2), dtype=torch.float64, device=device)
-    tangent = tangent.to(device=device, dtype=torch.float64).contiguous()
+    if tangent is not None:
+        tangent = tangent.to(device=device, dtype=torch.float64).contiguous()
     _native.check(
         lib.wcb_rows_jvp(state.compiled.native.handle, ctypes.byref(desc), ctypes.byref(ms), int(freq_index),
                          _native.ptr(state.rows) if K else None, _native.ptr(state.selected) if K else None, K,
-                         _native.ptr(tangent), tangent.numel(), _native.ptr(field), _native.ptr(dfield),
-                         _native.stream_handle(device)),
+                         _native.ptr(tangent), 0 if tangent is None else tangent.numel(), _native.ptr(field),
+                         None if tangent is None else _native.ptr(dfield), _native.stream_handle(device)),
         "wcb_rows_jvp",
     )
     del keep
@@ -313,22 +314,20 @@ def vjp_forward(scene: Any, config, frequencies_hz) -> dict:
     K = int(selected.shape[0])
     flat = {"valid": torch.ones(K, dtype=torch.bool, device=device), "tx": dec["tx_id"], "rx": dec["rx_id"],
             "cid": dec["component_id"].contiguous()}
-    outputs32, saved64, evs = [], [], []
-    for fi in range(len(frequencies)):
-        ev = engine.evaluate_rows(compiled, ep, mats, frequencies, fi, rows, selected, width, components=bits,
-                                  max_depth=config.max_depth, coherent=config.coherent)
-        pf = ev["path_field"]
-        g32, r32, i32 = ev["path_gain"].contiguous(), pf.real.contiguous(), pf.imag.contiguous()
-        outputs32.append(_forward(flat["valid"], flat["tx"], flat["rx"], flat["cid"], g32, r32, i32, T, R,
-                                  config.coherent, 0))
-        saved64.append(None)
-        evs.append(ev)
+    evs = [engine.evaluate_rows(compiled, ep, mats, frequencies, fi, rows, selected, width, components=bits,
+                                max_depth=config.max_depth, coherent=config.coherent)
+           for fi in range(len(frequencies))]
     inputs = _differentiable_inputs(scene, compiled, freqs_t, device)
     state = _State(compiled=compiled, ep=ep, mats=mats, frequencies=frequencies, components=bits,
                    max_depth=config.max_depth, coherent=config.coherent, rows=rows, selected=selected, flat=flat,
-                   saved64=saved64, outputs32=outputs32, layer_counts=inputs["layer_counts"],
+                   saved64=[None] * len(frequencies), outputs32=[], layer_counts=inputs["layer_counts"],
                    vertex_mask=inputs["vertex_mask"], param_total=_param_total(compiled, ep, mats, frequencies,
                                                                                bits, config))
+    # the returned cell values are the FP64 records' sums (the function the
+    # derivatives are taken of), rounded to FP32
+    for fi in range(len(frequencies)):
+        s64 = _linearisation(state, fi)
+        state.outputs32.append({k: v.to(torch.float32) for k, v in s64.items()})
     out = _SolveFunction.apply(state, inputs["vertices"], inputs["eps_r"], inputs["sigma_e"], inputs["layer_eps_r"],
                                inputs["layer_sigma_e"], inputs["frequency"], inputs["tx"], inputs["rx"])
     result = dict(zip(ACCUM_FIELDS, out))

@@ -62,6 +62,22 @@ class NativeScene:
         )
         self._finalizer = weakref.finalize(self, lib.wcb_scene_destroy, handle)
 
+    def refit(self, vertices: torch.Tensor) -> bool:
+        """Move the compiled scene to ``vertices`` (same count, on this
+        device) in place.  Returns False, changing nothing, when the move
+        changes a discrete decision of the compile (a coplanar group, an edge's
+        selection or wedge order, a shared-boundary merge): the scene must then
+        be compiled again."""
+        lib = _native.load()
+        v = vertices.to(device=self.device, dtype=torch.float32).contiguous()
+        changed = _native.ctypes.c_int32(0)
+        _native.check(lib.wcb_scene_refit(self.handle, _native.ptr(v), int(v.shape[0]), _native.ctypes.byref(changed),
+                                          _native.stream_handle(self.device)), "wcb_scene_refit")
+        if changed.value:
+            return False
+        self.vertices = v
+        return True
+
     def groups(self) -> tuple[torch.Tensor, torch.Tensor]:
         lib = _native.load()
         fg = torch.empty(self.num_faces, dtype=torch.int32, device=self.device)
@@ -229,6 +245,17 @@ def _geometry_token(scene: Any) -> tuple[tuple, list]:
     return tuple(parts), refs
 
 
+def _only_vertices_moved(old: tuple, new: tuple, old_refs: list, new_refs: list) -> bool:
+    """The two geometry tokens differ only in vertex tensors (identity or
+    in-place version) of the same shapes."""
+    if len(old) != len(new) or old[-1] != new[-1] or len(old_refs) != len(new_refs):
+        return False
+    for o, n, (ov, _of, _om), (nv, _nf, _nm) in zip(old[:-1], new[:-1], old_refs, new_refs):
+        if o[2:] != n[2:] or tuple(ov.shape) != tuple(nv.shape):
+            return False
+    return True
+
+
 def compile_scene(scene: Any, device: torch.device | None = None) -> CompiledScene:
     """Compile (or fetch from the per-scene cache) the device scene."""
 
@@ -237,9 +264,18 @@ def compile_scene(scene: Any, device: torch.device | None = None) -> CompiledSce
     token, refs = _geometry_token(scene)
     scene_key = id(scene)
     cached = _CACHE.get(scene_key)
-    if cached is not None and cached[0] is not None and cached[0]() is scene and cached[1] == token \
+    if cached is not None and cached[0] is not None and cached[0]() is scene \
             and cached[2].face_material.device == device:
-        return cached[2]
+        if cached[1] == token:
+            return cached[2]
+        # only vertex values moved (same structures, faces, materials and
+        # metadata; same vertex counts): update the device scene in place
+        if _only_vertices_moved(cached[1], token, cached[3], refs):
+            V = torch.cat([st.vertices.detach().to(device=device, dtype=torch.float32).reshape(-1, 3)
+                           for st in scene.structures]) if scene.structures else None
+            if V is not None and cached[2].native.refit(V):
+                _CACHE[scene_key] = (cached[0], token, cached[2], refs)
+                return cached[2]
     verts, faces, fsurf, fstruct, fmat = [], [], [], [], []
     materials: list = []
     mat_index: dict[int, int] = {}

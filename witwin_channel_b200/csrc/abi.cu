@@ -46,6 +46,15 @@ int wcb_scene_destroy(wcb_scene* scene) {
     return WCB_OK;
 }
 
+int wcb_scene_refit(wcb_scene* scene, const float* vertices, int64_t num_vertices, int32_t* topology_changed,
+                    void* stream) {
+    if (scene == nullptr || topology_changed == nullptr || num_vertices < 0) return WCB_ERR_INVALID_ARGUMENT;
+    int changed = 0;
+    const int rc = wcb::scene_refit(scene->h, vertices, num_vertices, &changed, as_stream(stream));
+    *topology_changed = changed;
+    return rc;
+}
+
 int wcb_scene_info(const wcb_scene* scene, int64_t* counts) {
     if (scene == nullptr || counts == nullptr) return WCB_ERR_INVALID_ARGUMENT;
     const wcb::SceneDev& d = scene->h->dev;

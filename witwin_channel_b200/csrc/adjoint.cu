@@ -365,21 +365,30 @@ int wcb_rows_jvp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
                  int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
                  const double* tangent, int64_t tangent_size, double* row_field, double* row_field_tangent,
                  void* stream) {
-    if (scene == nullptr || desc == nullptr || materials == nullptr || tangent == nullptr || num_selected < 0)
+    if (scene == nullptr || desc == nullptr || materials == nullptr || num_selected < 0)
         return WCB_ERR_INVALID_ARGUMENT;
-    if (num_selected > 0 && (rows == nullptr || selected == nullptr || row_field_tangent == nullptr))
-        return WCB_ERR_INVALID_ARGUMENT;
+    if (num_selected > 0 && (rows == nullptr || selected == nullptr)) return WCB_ERR_INVALID_ARGUMENT;
+    // no tangent: the FP64 fields alone (plain evaluation, no dual lane)
+    if (tangent == nullptr ? row_field == nullptr : row_field_tangent == nullptr) return WCB_ERR_INVALID_ARGUMENT;
     if (freq_index < 0 || freq_index >= desc->num_freq || desc->frequency_hz == nullptr)
         return WCB_ERR_INVALID_ARGUMENT;
     int64_t layout[9];
     const int rc = wcb_rows_vjp_layout(scene, desc, materials, layout);
     if (rc != WCB_OK) return rc;
-    if (tangent_size < layout[8]) return WCB_ERR_CAPACITY;
+    if (tangent != nullptr && tangent_size < layout[8]) return WCB_ERR_CAPACITY;
     if (num_selected == 0) return WCB_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     wcb::adj::AdjParams p;
     wcb::adj::fill_params(p, scene->h, desc, materials, freq_index, rows, selected, num_selected, layout);
     const unsigned g = unsigned((num_selected + wcb::adj::kBlock - 1) / wcb::adj::kBlock);
+    if (tangent == nullptr) {
+        wcb::adj::k_field64_rows<0><<<g, wcb::adj::kBlock, 0, s>>>(p, row_field);
+        wcb::adj::k_field64_rows<1><<<g, wcb::adj::kBlock, 0, s>>>(p, row_field);
+        wcb::adj::k_field64_rows<5><<<g, wcb::adj::kBlock, 0, s>>>(p, row_field);
+        wcb::adj::launch_field64_diffraction(p, row_field, s);
+        wcb::note_launch(4);
+        return cudaGetLastError() == cudaSuccess ? WCB_OK : WCB_ERR_CUDA;
+    }
     wcb::adj::k_jvp_rows<0><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent);
     wcb::adj::k_jvp_rows<1><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent);
     wcb::adj::k_jvp_rows<5><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent);

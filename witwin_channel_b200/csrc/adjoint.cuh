@@ -209,6 +209,12 @@ struct Seeds {
     }
 };
 
+// Seeds of the plain FP64 evaluation (no tangent lane).
+template <int N>
+struct Plain {
+    WCB_D Dual<N> param(double value, int) const { return Dual<N>(value); }
+};
+
 template <template <int> class WT, int N>
 WCB_D V3<Dual<N>> vertex(const AdjParams& p, const WT<N>& w, int v) {
     const float* x = p.sc.vertices + 3 * v;
@@ -505,6 +511,22 @@ __global__ void __launch_bounds__(kBlock) k_jvp_rows(AdjParams p, const double* 
 
 void launch_jvp_diffraction(const AdjParams& p, const double* tangent, double* field, double* field_tangent,
                             cudaStream_t s);
+
+// The records' FP64 path fields alone (the derivative kernels' primal, no
+// tangent): the point the cell sums are linearised at.
+template <int COMP>
+__global__ void __launch_bounds__(kBlock) k_field64_rows(AdjParams p, double* field) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= p.count) return;
+    const RowRec row = p.rows[p.selected[i]];
+    if (row.component != COMP) return;
+    const Plain<0> seeds{};
+    const Cx<Dual<0>> pf = eval_record<0, COMP>(p, row, seeds);
+    field[2 * i] = pf.re.v;
+    field[2 * i + 1] = pf.im.v;
+}
+
+void launch_field64_diffraction(const AdjParams& p, double* field, cudaStream_t s);
 
 }  // namespace adj
 }  // namespace wcb

@@ -18,5 +18,11 @@ void launch_jvp_diffraction(const AdjParams& p, const double* tangent, double* f
     k_jvp_rows<2><<<unsigned((p.count + kBlock - 1) / kBlock), kBlock, 0, s>>>(p, tangent, field, field_tangent);
 }
 
+// The diffraction records' plain FP64 fields (one thread per record).
+void launch_field64_diffraction(const AdjParams& p, double* field, cudaStream_t s) {
+    if (p.count <= 0) return;
+    k_field64_rows<2><<<unsigned((p.count + kBlock - 1) / kBlock), kBlock, 0, s>>>(p, field);
+}
+
 }  // namespace adj
 }  // namespace wcb

@@ -25,6 +25,17 @@ struct Dual {
     }
 };
 
+// N = 0: no tangent lane, a plain FP64 evaluation of the same templated code
+// (the tangent loops run zero times; the one-element array is never read).
+template <>
+struct Dual<0> {
+    double v;
+    double d[1];
+
+    WCB_HD Dual() : v(0.0), d{0.0} {}
+    WCB_HD Dual(double x) : v(x), d{0.0} {}  // NOLINT: constants promote implicitly
+};
+
 template <typename T>
 struct is_dual {
     static constexpr bool value = false;

@@ -21,12 +21,31 @@ struct SceneHandle {
     std::vector<int> face_group_host;
     int num_edges_total = 0;
     int num_nodes = 0;
+    // device caches of the compile's discrete decisions (for scene_refit)
+    int* face_surface = nullptr;         // (F)
+    long long* face_keys = nullptr;      // (F,5) coplanar group keys (refit scratch)
+    int4* edge_rec = nullptr;            // (NE) v0, v1, f0, f1 of every edge record
+    unsigned char* edge_state = nullptr; // (NE) bit 0 wedge order, 1 coplanar, 2 selected before merges, 3 final
+    long long* edge_qkey = nullptr;      // (NE,6) quantised endpoints of shared-boundary candidates (refit scratch)
+    int* edge_qhead = nullptr;           // (NE) first record of a candidate's endpoint class; -1 not a candidate
+    int* key_table = nullptr;            // open-addressing table of class keys for the refit's distinctness check
+    int key_table_slots = 0;             // power of two, at least twice the classes
+    int* edge_partner = nullptr;         // (NE) merged partner of a pair head; -2 merged away; -1 none
+    int* leaf_parent = nullptr;          // (F) parent node << 1 | side (-1: none)
+    int* node_parent = nullptr;          // (F-1) parent node << 1 | side (-1: root)
+    int* bvh_counter = nullptr;          // (F-1) refit arrival counters
+    int* refit_flag = nullptr;           // (1)
+    double* diagonal_dev = nullptr;      // (1)
+    int half_plane_policy = 1;
+    int vertical_only_policy = 0;
+    double vertical_ratio = 0.7;
 };
 
 int scene_create(const float* vertices, int64_t nv, const int32_t* faces, int64_t nf, const int32_t* surface,
                  const int32_t* structure, const int32_t* material, int boundary_half_plane, int vertical_only,
                  double vertical_ratio, cudaStream_t stream, SceneHandle** out);
 void scene_destroy(SceneHandle* h);
+int scene_refit(SceneHandle* h, const float* d_vertices, int64_t nv, int* topology_changed, cudaStream_t stream);
 
 int rows_select_workspace(int64_t n, int64_t* bytes);
 int rows_select(const void* rows, int64_t n, int width, int64_t max_paths, int scope, int64_t* selected,

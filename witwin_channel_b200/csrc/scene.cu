@@ -22,11 +22,6 @@ namespace wcb {
 
 namespace {
 
-constexpr double kPlaneGroupQuant = 1.0e-4;  // propagation/geometry.py:113
-constexpr double kEdgePlaneTol = 1.34e-5;    // propagation/geometry.py:37
-constexpr double kEndpointQuant = 1.0e-4;    // scene/resources.py:296
-constexpr double kNormalCosTol = 1.0 - 1.0e-5;
-constexpr double kPlaneTolerance = 1.0e-3;   // rayd/reflection.cpp:50
 
 // ------------------------------------------------------------ BVH build
 // Binned surface-area-heuristic build on the host (Wald, "On fast
@@ -367,6 +362,10 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
     std::vector<double> elen(NE), ext(NE);
     std::vector<int> face0(NE), face1(NE), mat0(NE), mat1(NE);
     std::vector<int> fn0(NE), fn1(NE);  // faces whose unit normals are n0 and n1 (-1: n1 = -n0)
+    std::vector<unsigned char> state(NE, 0);  // refit cache: wedge order, coplanar, selected before merges, final
+    std::vector<long long> qkey(size_t(NE) * 6, 0);
+    std::vector<int> partner(NE, -1);
+    std::vector<int> qhead(NE, -1);  // refit cache: first record of a candidate's endpoint class
     auto fnormal = [&](int f) { return std::array<double, 3>{face_plane[4 * f], face_plane[4 * f + 1], face_plane[4 * f + 2]}; };
     auto opposite = [&](int f, int a, int b) {
         for (int k = 0; k < 3; ++k) {
@@ -406,6 +405,7 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
         }
         const bool wedge_ok = bnd || (interior && dot3(n0c, n1c) < 1.0);
         sel[e] = (interior || bnd) && !coplanar && L > 1e-6 && wedge_ok;
+        state[e] = (first ? 1 : 0) | (coplanar ? 2 : 0) | (sel[e] ? 4 : 0);
         boundary[e] = r.f1 < 0;
         epos[e] = {0.5 * (double(st[0]) + en[0]), 0.5 * (double(st[1]) + en[1]), 0.5 * (double(st[2]) + en[2])};
         edir[e] = d;
@@ -438,10 +438,14 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
             std::array<long long, 6> key;
             if (pa <= pb) key = {pa[0], pa[1], pa[2], pb[0], pb[1], pb[2]};
             else key = {pb[0], pb[1], pb[2], pa[0], pa[1], pa[2]};
+            for (int k = 0; k < 6; ++k) qkey[size_t(e) * 6 + k] = key[k];
             groups[key].push_back(e);
         }
         int candidates = 0;
-        for (auto& kv : groups) candidates += int(kv.second.size());
+        for (auto& kv : groups) {
+            candidates += int(kv.second.size());
+            for (int x : kv.second) qhead[x] = kv.second[0];
+        }
         if (candidates >= 2) {
             for (auto& kv : groups) {
                 auto& g = kv.second;
@@ -459,7 +463,12 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
                 mat1[a] = mat0[b];
                 ext[a] = merged;
                 boundary[a] = 0;
-                for (size_t x = 2; x < g.size(); ++x) sel[g[x]] = 0;
+                partner[a] = b;
+                partner[b] = -2;
+                for (size_t x = 2; x < g.size(); ++x) {
+                    sel[g[x]] = 0;
+                    partner[g[x]] = -2;
+                }
             }
         }
     }
@@ -473,6 +482,7 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
             double lz = std::max(std::sqrt(dot3(dv, dv)), 1e-6);
             if (!(std::fabs(dv[2]) / lz > vertical_ratio)) sel[e] = 0;
         }
+        if (sel[e]) state[e] |= 8;
         if (!sel[e]) continue;
         EdgeDev ed;
         std::memset(&ed, 0, sizeof(ed));
@@ -544,6 +554,30 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
     h->group_rep_host = group_rep;
     h->face_group_host = face_group;
     h->num_edges_total = NE;
+    // caches of the discrete decisions for scene_refit
+    {
+        std::vector<long long> fkeys(size_t(F) * 5);
+        for (int f = 0; f < F; ++f)
+            for (int k = 0; k < 5; ++k) fkeys[size_t(f) * 5 + k] = keys[f][k];
+        std::vector<int4> erec(NE);
+        for (int e = 0; e < NE; ++e) erec[e] = make_int4(recs[e].v0, recs[e].v1, recs[e].f0, recs[e].f1);
+        h->face_surface = upload(h, surface, stream);
+        h->face_keys = upload(h, fkeys, stream);
+        h->edge_rec = upload(h, erec, stream);
+        h->edge_state = upload(h, state, stream);
+        h->edge_qkey = upload(h, qkey, stream);
+        h->edge_partner = upload(h, partner, stream);
+        h->edge_qhead = upload(h, qhead, stream);
+        int slots = 1;
+        while (slots < 2 * std::max(std::max(G, NE), 1)) slots <<= 1;
+        h->key_table = upload(h, std::vector<int>(slots, -1), stream);
+        h->key_table_slots = slots;
+        h->refit_flag = upload(h, std::vector<int>(1, 0), stream);
+        h->diagonal_dev = upload(h, std::vector<double>(1, 0.0), stream);
+        h->half_plane_policy = boundary_half_plane;
+        h->vertical_only_policy = vertical_only;
+        h->vertical_ratio = vertical_ratio;
+    }
     // bounds
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int i = 0; i < V; ++i)
@@ -582,6 +616,19 @@ int scene_create(const float* d_vertices, int64_t nv, const int32_t* d_faces, in
             tri[3 * sl + 1] = make_float4(b[0], b[1], b[2], gbits);
             tri[3 * sl + 2] = make_float4(c[0], c[1], c[2], 0.0f);
         }
+        // parent links for the refit: node << 1 | side (-1 at the root)
+        std::vector<int> leaf_parent(F, -1), node_parent(std::max(F - 1, 1), -1);
+        if (F > 1)
+            for (int i = 0; i < int(host_nodes.size()); ++i) {
+                const int ch[2] = {host_nodes[i].d.x, host_nodes[i].d.y};
+                for (int side = 0; side < 2; ++side) {
+                    if (ch[side] >= 0) node_parent[ch[side]] = (i << 1) | side;
+                    else leaf_parent[~ch[side]] = (i << 1) | side;
+                }
+            }
+        h->leaf_parent = upload(h, leaf_parent, stream);
+        h->node_parent = upload(h, node_parent, stream);
+        h->bvh_counter = upload(h, std::vector<int>(std::max(F - 1, 1), 0), stream);
         sd.tri = upload(h, tri, stream);
         sd.nodes = upload(h, host_nodes, stream);
         if (sd.tri == nullptr || sd.nodes == nullptr) { scene_destroy(h); return 2; }

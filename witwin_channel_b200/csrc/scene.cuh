@@ -9,6 +9,13 @@ namespace wcb {
 
 constexpr int kStackDepth = 64;  // per-thread traversal stack entries (shared memory)
 
+// compile tolerances (shared by the host compile and the device refit)
+constexpr double kPlaneGroupQuant = 1.0e-4;  // propagation/geometry.py:113
+constexpr double kEdgePlaneTol = 1.34e-5;    // propagation/geometry.py:37
+constexpr double kEndpointQuant = 1.0e-4;    // scene/resources.py:296
+constexpr double kNormalCosTol = 1.0 - 1.0e-5;
+constexpr double kPlaneTolerance = 1.0e-3;   // rayd/reflection.cpp:50
+
 // BVH node: both child boxes plus the child references (64 bytes, four
 // 16-byte loads).  child >= 0: internal node; child < 0: leaf ~slot.
 struct __align__(16) BvhNode {
