@@ -373,7 +373,7 @@ def _fp64_plain(compiled, ep, mats, freq, bits, cfg, device, mixed_ms: float, st
             "mixed_ms_per_step": mixed_ms, "mixed_speedup": ms / mixed_ms if mixed_ms else None, "steps": steps}
 
 
-def _vjp_run(device, steps: int = 3) -> dict:
+def _vjp_run(device, steps: int = 7) -> dict:
     """The gradient workload: forward + VJP of the log10 path-gain MSE on the
     urban canyon w.r.t. concrete (eps_r, sigma_e), frequency, Tx position and
     the vertices of 8 seeded boxes (the target map comes from eps_r x1.10 and
@@ -396,19 +396,28 @@ def _vjp_run(device, steps: int = 3) -> dict:
         return loss, res
 
     step()
+    step()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
+    # per step: the device-timeline span (events) and the host wall time to the
+    # step's end (both include the host-side gaps between launches); medians
+    step_ms, wall_ms = [], []
     for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
         loss, res = step()
-    e1.record()
-    torch.cuda.synchronize()
+        e1.record()
+        torch.cuda.synchronize()
+        wall_ms.append((time.perf_counter() - t0) * 1e3)
+        step_ms.append(e0.elapsed_time(e1))
     vg = torch.cat([v.grad.reshape(-1) for v in g["leaves"]["vertices"]])
     return {
         "workload": "urban canyon 64 boxes, 256x256 grid, 28 GHz, LoS + reflection depth 3 + UTD; loss = MSE of "
                     "log10 path gain vs a target from eps_r x1.10 and 8 boxes displaced N(0, 0.5 m); gradients for "
                     "concrete eps_r and sigma_e, frequency, Tx position and the 8 boxes' 64 vertices",
-        "ms_per_step": e0.elapsed_time(e1) / steps,
+        "ms_per_step": float(sorted(step_ms)[len(step_ms) // 2]),
+        "host_wall_ms_per_step": float(sorted(wall_ms)[len(wall_ms) // 2]),
+        "steps_ms": [round(x, 3) for x in step_ms],
         "steps": steps,
         "paths": int(res.metadata["counts"]["path_count"]),
         "loss": float(loss),

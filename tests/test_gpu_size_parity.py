@@ -402,19 +402,27 @@ def test_gradient_run_sampled_cells_fd():
     strong = 0
     report = []
     for key, ours in params:
-        h = 1e-4 * max(abs(float(value(key))), 1.0)
-
         def central(step):
             ap, fp = perturb(key, step)
             am, fm = perturb(key, -step)
             return (oracle_loss(ap, fp) - oracle_loss(am, fm)) / (2 * step)
 
-        d1, d2, d4 = central(h), central(h / 2), central(h / 4)
-        r1, r2 = (4 * d2 - d1) / 3, (4 * d4 - d2) / 3
-        report.append((key, ours, r2, abs(r1 - r2)))
-        if not np.isfinite([d1, d2, d4]).all() or abs(r1 - r2) > 1e-3 * abs(r2) + 1e-12:
-            # a path of a sampled cell appears or vanishes within the step (a
-            # topology change): not a derivative check
+        # relative step 1e-4, then 1e-5 and 1e-6 where the loss is not smooth
+        # over the larger step (a centimetre move of a 100 m coordinate can
+        # carry a sampled cell's path across a shadow boundary or the UTD
+        # window cutoff)
+        smooth = False
+        for rel in (1e-4, 1e-5, 1e-6):
+            h = rel * max(abs(float(value(key))), 1.0)
+            d1, d2, d4 = central(h), central(h / 2), central(h / 4)
+            r1, r2 = (4 * d2 - d1) / 3, (4 * d4 - d2) / 3
+            if np.isfinite([d1, d2, d4]).all() and abs(r1 - r2) <= 1e-3 * abs(r2) + 1e-12:
+                smooth = True
+                break
+        report.append((key, ours, r2, abs(r1 - r2), rel))
+        if not smooth:
+            # a path of a sampled cell appears or vanishes within every step
+            # (a topology change): not a derivative check
             continue
         if abs(r2) > 0:
             strong += 1

@@ -286,10 +286,12 @@ class _SolveFunction(torch.autograd.Function):
         return tuple(torch.stack([o[k] for o in per_freq]).to(torch.float32) for k in ACCUM_FIELDS)
 
 
-def vjp_forward(scene: Any, config, frequencies_hz) -> dict:
+def vjp_forward(scene: Any, config, frequencies_hz, evaluate_rows: bool | None = None) -> dict:
     """Row-mode forward at every frequency (geometry and records frozen once)
     with autograd-connected cell outputs: ``path_gain``/``field_total_*`` (NF,T,R),
-    ``component_*`` (NF,6,T,R) in the flat (tx, rx) order, plus the records."""
+    ``component_*`` (NF,6,T,R) in the flat (tx, rx) order, plus the records.
+    ``evaluate_rows`` (default: ``config.export_paths``) adds the FP32 row
+    evaluations a path table is built from."""
     if not config.coherent and "diffraction" in config.components:
         raise NotImplementedError("ad_mode='vjp' with incoherent accumulation and diffraction is not provided")
     device = torch.device("cuda", torch.cuda.current_device())
@@ -314,9 +316,11 @@ def vjp_forward(scene: Any, config, frequencies_hz) -> dict:
     K = int(selected.shape[0])
     flat = {"valid": torch.ones(K, dtype=torch.bool, device=device), "tx": dec["tx_id"], "rx": dec["rx_id"],
             "cid": dec["component_id"].contiguous()}
+    if evaluate_rows is None:
+        evaluate_rows = bool(config.export_paths)
     evs = [engine.evaluate_rows(compiled, ep, mats, frequencies, fi, rows, selected, width, components=bits,
                                 max_depth=config.max_depth, coherent=config.coherent)
-           for fi in range(len(frequencies))]
+           for fi in range(len(frequencies))] if evaluate_rows else None
     inputs = _differentiable_inputs(scene, compiled, freqs_t, device)
     state = _State(compiled=compiled, ep=ep, mats=mats, frequencies=frequencies, components=bits,
                    max_depth=config.max_depth, coherent=config.coherent, rows=rows, selected=selected, flat=flat,

@@ -36,44 +36,71 @@ __global__ void k_vjp_count(AdjParams p, int* keys, int* idx) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= p.count) return;
     const RowRec row = p.rows[p.selected[i]];
-    ParamList pl;
-    build_params(p, row, pl);
-    p.counts[i] = pl.n;
+    if (row.component == 2) {
+        p.counts[i] = diffraction_params(p, row).count;
+    } else {
+        ParamList pl;
+        build_params(p, row, pl);
+        p.counts[i] = pl.n;
+    }
     const int rank = component_rank(row.component);
     keys[i] = rank * 8 + min(max(int(row.depth), 0), 7);
     idx[i] = int(i);
     atomicAdd(p.comp_counts + rank, 1);
 }
 
-// work items of each ordered record of one component: its parameters, or one
-// for a parameterless record whose FP64 field is wanted
-__global__ void k_vjp_work(AdjParams p, int* work) {
-    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (j >= p.order_count) return;
-    const long long i = p.order[p.order_begin + j];
-    work[j] = max(p.counts[i], p.row_field ? 1 : 0);
+// Ordered per-id sums of the id-sorted pairs (a parameter's contributions
+// form one run).  A run is cut into chunks of kChunk entries in record order;
+// one block sums a chunk (each thread a fixed strided subset, then a
+// fixed-shape block tree) and one thread then sums a run's chunk partials in
+// chunk order.  The partition depends only on the run lengths, never on
+// timing, so the gradient is deterministic bit for bit, and a parameter that
+// every record touches (a Tx coordinate, a material value) is summed by many
+// blocks instead of one.  Parameters without a run stay zero.
+constexpr int kReduceBlock = 256;
+constexpr int kChunk = 16384;
+
+__global__ void k_run_chunks(const int* run_counts, const int* num_runs, int cap, int* chunk_n) {
+    const int runs = *num_runs;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < cap; r += gridDim.x * blockDim.x)
+        chunk_n[r] = r < runs ? (run_counts[r] + kChunk - 1) / kChunk : 0;
 }
 
-// One block per run of equal ids in the id-sorted pairs (a parameter's
-// contributions): each thread sums a fixed strided subset in record order,
-// then a fixed-shape block tree; the result does not depend on timing, so
-// the gradient is deterministic.  Parameters without a run stay zero.
-constexpr int kReduceBlock = 256;
-
-__global__ void __launch_bounds__(kReduceBlock) k_vjp_reduce_runs(const unsigned* run_ids, const int* run_counts,
-                                                                   const long long* run_offsets, const int* num_runs,
-                                                                   const double* vals, double* grad) {
+__global__ void __launch_bounds__(kReduceBlock) k_reduce_chunks(const int* run_counts, const long long* run_offsets,
+                                                                const int* num_runs, const int* chunk_base,
+                                                                const int* chunk_n, int cap, const double* vals,
+                                                                double* chunk_sums) {
     typedef cub::BlockReduce<double, kReduceBlock> Reduce;
     __shared__ typename Reduce::TempStorage tmp;
     const int runs = *num_runs;
-    for (int r = blockIdx.x; r < runs; r += gridDim.x) {
-        const long long beg = run_offsets[r];
-        const int n = run_counts[r];
+    const int total = chunk_base[cap - 1] + chunk_n[cap - 1];
+    for (int c = blockIdx.x; c < total; c += gridDim.x) {
+        // the run holding chunk c: the last run whose first chunk is at or before c
+        int lo = 0, hi = runs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (chunk_base[mid] <= c) lo = mid;
+            else hi = mid - 1;
+        }
+        const int j = c - chunk_base[lo];
+        const long long beg = run_offsets[lo] + (long long)j * kChunk;
+        const int n = min(kChunk, run_counts[lo] - j * kChunk);
         double s = 0.0;
         for (int q = threadIdx.x; q < n; q += kReduceBlock) s += vals[beg + q];
-        const double total = Reduce(tmp).Sum(s);
-        if (threadIdx.x == 0) grad[run_ids[r]] = total;
+        const double sum = Reduce(tmp).Sum(s);
+        if (threadIdx.x == 0) chunk_sums[c] = sum;
         __syncthreads();
+    }
+}
+
+__global__ void k_reduce_run_chunks(const unsigned* run_ids, const int* num_runs, const int* chunk_base,
+                                    const int* chunk_n, const double* chunk_sums, double* grad) {
+    const int runs = *num_runs;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < runs; r += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        const int b = chunk_base[r];
+        for (int k = 0; k < chunk_n[r]; ++k) s += chunk_sums[b + k];
+        grad[run_ids[r]] = s;
     }
 }
 
@@ -122,7 +149,9 @@ VjpLayout vjp_layout(long long K, long long pairs) {
     cub::DeviceRunLengthEncode::Encode(nullptr, rle_b, (const unsigned*)nullptr, (unsigned*)nullptr, (int*)nullptr,
                                        (int*)nullptr, mi);
     cub::DeviceScan::ExclusiveSum(nullptr, roff_b, (int*)nullptr, (long long*)nullptr, mi);
-    L.sort_bytes = std::max(sort_b, std::max(rle_b, roff_b));
+    size_t chunk_b = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, chunk_b, (int*)nullptr, (int*)nullptr, mi);
+    L.sort_bytes = std::max(std::max(sort_b, chunk_b), std::max(rle_b, roff_b));
     L.sort_tmp = take(L.sort_bytes);
     L.total = o;
     return L;
@@ -306,23 +335,7 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
                 case 0: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 0><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
                 case 1: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 1><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
                 case 5: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 5><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
-                default: {
-                    // one thread per (record, parameter): work per record, its prefix, the total
-                    int* work = keys;
-                    int* pair_base = keys2;
-                    wcb::adj::k_vjp_work<<<g, wcb::adj::kBlock, 0, s>>>(p, work);
-                    size_t wb = L.scan_bytes;
-                    if (cub::DeviceScan::ExclusiveSum(b + L.scan_tmp, wb, work, pair_base, int(p.order_count), s) !=
-                        cudaSuccess)
-                        return WCB_ERR_CUDA;
-                    int tail[2] = {0, 0};
-                    cudaMemcpyAsync(&tail[0], pair_base + p.order_count - 1, 4, cudaMemcpyDeviceToHost, s);
-                    cudaMemcpyAsync(&tail[1], work + p.order_count - 1, 4, cudaMemcpyDeviceToHost, s);
-                    if (cudaStreamSynchronize(s) != cudaSuccess) return WCB_ERR_CUDA;
-                    wcb::adj::launch_vjp_diffraction(p, pair_base, (long long)tail[0] + tail[1], s);
-                    wcb::note_launch(2);
-                    break;
-                }
+                default: wcb::adj::launch_vjp_diffraction(p, s); break;
             }
             wcb::note_launch();
         }
@@ -352,10 +365,23 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
         if (cub::DeviceScan::ExclusiveSum(b + L.sort_tmp, tb, run_counts, run_offsets, int(std::min<long long>(pairs, P)),
                                           s) != cudaSuccess)
             return WCB_ERR_CUDA;
-        const int blocks = int(std::min<long long>(P, 4096));
-        wcb::adj::k_vjp_reduce_runs<<<blocks, wcb::adj::kReduceBlock, 0, s>>>(run_ids, run_counts, run_offsets, num_runs,
-                                                                             vals2, grad_out);
-        wcb::note_launch(3);
+        // chunk counts and bases reuse the unsorted-id and sorted-id buffers, the
+        // chunk partials the unsorted values (all free once sorted and encoded)
+        const int cap = int(std::min<long long>(pairs, P));
+        int* chunk_n = reinterpret_cast<int*>(p.out_ids);
+        int* chunk_base = reinterpret_cast<int*>(ids2);
+        double* chunk_sums = p.out_vals;
+        const int tgrid = int(std::min<long long>((cap + 255) / 256, 4096));
+        wcb::adj::k_run_chunks<<<tgrid, 256, 0, s>>>(run_counts, num_runs, cap, chunk_n);
+        tb = L.sort_bytes;
+        if (cub::DeviceScan::ExclusiveSum(b + L.sort_tmp, tb, chunk_n, chunk_base, cap, s) != cudaSuccess)
+            return WCB_ERR_CUDA;
+        wcb::adj::k_reduce_chunks<<<148 * 8, wcb::adj::kReduceBlock, 0, s>>>(run_counts, run_offsets, num_runs,
+                                                                            chunk_base, chunk_n, cap, vals2,
+                                                                            chunk_sums);
+        wcb::adj::k_reduce_run_chunks<<<tgrid, 256, 0, s>>>(run_ids, num_runs, chunk_base, chunk_n, chunk_sums,
+                                                           grad_out);
+        wcb::note_launch(6);
     }
     rc = cudaGetLastError() == cudaSuccess ? WCB_OK : WCB_ERR_CUDA;
     return rc;

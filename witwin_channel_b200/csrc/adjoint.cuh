@@ -12,45 +12,9 @@
 #include "paths.cuh"
 #include "solve.h"
 #include "utd.cuh"
+#include "utd_adjoint.cuh"
 
 namespace wcb {
-
-// ---------------------------------------------------------------- dual UTD pieces
-// KP transition F(x) with F'(x) = F(x) (1/(2x) + j) - j.
-template <int N>
-WCB_HD Cx<Dual<N>> transition(const Dual<N>& x) {
-    if (x.v <= 0.0) return cx(Dual<N>(0.0), Dual<N>(0.0));
-    const Cx<double> f = transition<double>(x.v);
-    const double inv2x = 0.5 / x.v;
-    const double dre = f.re * inv2x - f.im;
-    const double dim = f.im * inv2x + f.re - 1.0;
-    return cx(chain(f.re, dre, x), chain(f.im, dim, x));
-}
-
-// exp(-j k d) for dual geometry (the UTD phase).
-template <typename T, int N>
-WCB_HD Cx<Dual<N>> phasor_kd(const Dual<N>& k, const Dual<N>& d) {
-    return phasor_neg_kd(k, d);
-}
-
-// |(1+j)/2 - (C(x) + jS(x))| with d/dx (C + jS) = exp(j pi x^2 / 2).
-template <int N>
-WCB_HD Dual<N> fresnel_complement_abs(const Dual<N>& x) {
-    const double xv = x.v;
-    Cx<double> c;
-    if (xv >= 0.0) {
-        c = fresnel_pos<double>(xv, true).complement;
-    } else {
-        c = cx(1.0, 1.0) - fresnel_pos<double>(-xv, true).complement;
-    }
-    const double a = hypot(c.re, c.im);
-    double ph = kPi / 2 * xv * xv;
-    ph = ph - kTwoPi * floor(ph / kTwoPi);
-    double es, ec;
-    sincos(ph, &es, &ec);
-    const double g = a > 0.0 ? -(c.re * ec + c.im * es) / a : 0.0;
-    return chain(a, g, x);
-}
 
 namespace adj {
 
@@ -181,6 +145,50 @@ WCB_D void build_params(const AdjParams& p, const RowRec& row, ParamList& pl) {
     }
 }
 
+// The parameters of a diffraction record without the generic list (the same
+// set build_params gives): the distinct wanted vertices (end points, then
+// the faces' vertices), the distinct face materials, the endpoint and
+// frequency entries.
+struct DiffParamSet {
+    int nv;
+    int vid[8];
+    int m0, mn;         // differentiated material ids (-1: none); mn is only a material other than m0
+    bool same_material; // the second face exists and has face 0's material
+    int count;
+};
+
+WCB_D DiffParamSet diffraction_params(const AdjParams& p, const RowRec& row) {
+    DiffParamSet d;
+    d.nv = 0;
+    const int slot = p.edge_slot[row.edge];
+    const int* tp = p.edge_topo + 4 * slot;
+    auto addv = [&](int v) {
+        if (!vertex_wanted(p, v)) return;
+        for (int i = 0; i < d.nv; ++i)
+            if (d.vid[i] == v) return;
+        d.vid[d.nv++] = v;
+    };
+    addv(tp[0]);
+    addv(tp[1]);
+    for (int k = 0; k < 3; ++k) addv(p.sc.faces[3 * tp[2] + k]);
+    if (tp[3] >= 0)
+        for (int k = 0; k < 3; ++k) addv(p.sc.faces[3 * tp[3] + k]);
+    const EdgeDev& ed = p.sc.edges[slot];
+    d.m0 = d.mn = -1;
+    d.same_material = false;
+    if (p.want & kWantMaterials) {
+        d.m0 = p.sc.face_material[ed.mat_face0];
+        if (ed.face_n) {
+            const int m = p.sc.face_material[ed.mat_face1];
+            if (m != d.m0) d.mn = m;
+            else d.same_material = true;
+        }
+    }
+    d.count = ((p.want & kWantTx) ? 3 : 0) + (((p.want & kWantRx) && p.rx_kind == 0) ? 3 : 0) +
+              ((p.want & kWantFreq) ? 1 : 0) + 3 * d.nv + (d.m0 >= 0 ? 2 : 0) + (d.mn >= 0 ? 2 : 0);
+    return d;
+}
+
 // The ids carried as tangent lanes in this pass.
 template <int N>
 struct Window {
@@ -228,8 +236,7 @@ WCB_D V3<Dual<N>> face_unit_normal(const AdjParams& p, const WT<N>& w, int f, V3
     const V3<Dual<N>> b = vertex(p, w, p.sc.faces[3 * f + 1]);
     const V3<Dual<N>> c = vertex(p, w, p.sc.faces[3 * f + 2]);
     if (anchor) *anchor = a;
-    const V3<Dual<N>> n = cross(b - a, c - a);
-    return n * (Dual<N>(1.0) / s_max(length(n), 1e-6));
+    return unit_face_normal(a, b, c);
 }
 
 template <template <int> class WT, int N>
@@ -260,30 +267,9 @@ template <template <int> class WT, int N>
 WCB_D EdgeFrame<Dual<N>> edge_frame_dual(const AdjParams& p, const WT<N>& w, int slot) {
     using D = Dual<N>;
     const int* tp = p.edge_topo + 4 * slot;
-    const V3<D> va = vertex(p, w, tp[0]);
-    const V3<D> vb = vertex(p, w, tp[1]);
-    const V3<D> vec = vb - va;
-    const D L = s_max(length(vec), 1e-12);
-    EdgeFrame<D> f;
-    f.e = vec * (D(1.0) / L);
-    f.c = (va + vb) * D(0.5);
-    f.half_length = L * 0.5;
-    f.n0 = face_unit_normal(p, w, tp[2], (V3<D>*)nullptr);
-    const V3<D> n1 = tp[3] >= 0 ? face_unit_normal(p, w, tp[3], (V3<D>*)nullptr) : -f.n0;
-    const V3<D> t = cross(f.n0, f.e);
-    f.t0 = t * (D(1.0) / s_max(length(t), 1e-6));
-    if (tp[3] >= 0) {
-        D cosv = -dot(f.n0, n1);
-        cosv = s_min(s_max(cosv, -1.0), 1.0);
-        f.n = (D(kTwoPi) - s_acos(cosv)) / kPi;
-    } else {
-        f.n = D(2.0);
-    }
-    const V3<D> bis = f.n0 + n1;
-    const D bl = length(bis);
-    f.bisector = value_of(bl) > 1e-6 ? bis * (D(1.0) / bl) : -f.t0;  // feeds only the visibility point
-    f.face_n = tp[3] >= 0;
-    return f;
+    const V3<D> n0 = face_unit_normal(p, w, tp[2], (V3<D>*)nullptr);
+    const V3<D> n1 = tp[3] >= 0 ? face_unit_normal(p, w, tp[3], (V3<D>*)nullptr) : -n0;
+    return frame_from(vertex(p, w, tp[0]), vertex(p, w, tp[1]), n0, n1, tp[3] >= 0);
 }
 
 // FP64 dual re-evaluation of one record's powered path field.
@@ -438,54 +424,110 @@ __global__ void __launch_bounds__(kBlock) k_vjp_rows(AdjParams p) {
     }
 }
 
-// The same contributions with one thread per (record, parameter): each
-// thread carries a single tangent lane through the record's evaluation.  The
-// lanes of a dual number never mix, so every contribution is bit-identical to
-// the N-lane kernel's; the one-lane evaluation holds far fewer live values
-// per thread, which pays for the repeated value part on the heavy UTD
-// records.  `pair_base` is the exclusive prefix over the component's ordered
-// records of their work items (parameters, or one for a parameterless record
-// whose FP64 field is wanted; k_vjp_work in adjoint.cu).
-
+// Reverse mode over the diffraction records: one thread per record.  One
+// FP64 forward sweep and one reverse sweep (utd_record_vjp, then the adjoints
+// of the edge frame and of the two face normals) give the contribution of
+// every parameter of the record at once, where a dual-number evaluation
+// would repeat the UTD (and its special functions) once per parameter lane.
+// The pairs are written in the record's parameter-list order, like the
+// forward-mode kernels, so the id sort and the ordered per-id sums that
+// follow are unchanged.
 template <int COMP>
-__global__ void __launch_bounds__(kBlock, 4) k_vjp_pairs(AdjParams p, const int* pair_base, long long total) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    // the last ordered record whose work range starts at or before t
-    long long lo = 0, hi = p.order_count - 1;
-    while (lo < hi) {
-        const long long mid = (lo + hi + 1) >> 1;
-        if (pair_base[mid] <= t) lo = mid;
-        else hi = mid - 1;
-    }
-    const long long i = p.order[p.order_begin + lo];
+__global__ void __launch_bounds__(kBlock) k_vjp_diffraction(AdjParams p) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= p.order_count) return;
+    const long long i = p.order[p.order_begin + j];
     const RowRec row = p.rows[p.selected[i]];
     if (row.component != COMP) return;
-    ParamList pl;
-    build_params(p, row, pl);
-    const int q = int(t - pair_base[lo]);
-    Window<1> w;
-    w.n = q < pl.n ? 1 : 0;
-    w.id[0] = q < pl.n ? pl.id[q] : -1;
-    const Cx<Dual<1>> pf = eval_record<1, COMP>(p, row, w);
-    if (q == 0 && p.row_field) {
-        p.row_field[2 * i] = pf.re.v;
-        p.row_field[2 * i + 1] = pf.im.v;
+    const int slot = p.edge_slot[row.edge];
+    const int* tp = p.edge_topo + 4 * slot;
+    const EdgeDev& ed = p.sc.edges[slot];
+    const bool face_n = tp[3] >= 0;
+    const int t = row.tx, r = row.rx;
+    auto vtx = [&](int v) {
+        const float* x = p.sc.vertices + 3 * v;
+        return v3(double(x[0]), double(x[1]), double(x[2]));
+    };
+    int fv[2][3];
+    V3<double> fp[2][3];
+    for (int sd = 0; sd < 2; ++sd)
+        for (int k = 0; k < 3; ++k) {
+            fv[sd][k] = (sd == 0 || face_n) ? p.sc.faces[3 * tp[2 + sd] + k] : -1;
+            fp[sd][k] = fv[sd][k] >= 0 ? vtx(fv[sd][k]) : v3(0.0, 0.0, 0.0);
+        }
+    const V3<double> va = vtx(tp[0]), vb = vtx(tp[1]);
+    const V3<double> n0 = unit_face_normal(fp[0][0], fp[0][1], fp[0][2]);
+    const V3<double> n1 = face_n ? unit_face_normal(fp[1][0], fp[1][1], fp[1][2]) : -n0;
+    UtdRecordIn in;
+    in.fr = frame_from(va, vb, n0, n1, face_n);
+    in.S = v3(double(p.tx_pos[3 * t]), double(p.tx_pos[3 * t + 1]), double(p.tx_pos[3 * t + 2]));
+    const V3<Dual<0>> rq = receiver(p, Plain<0>{}, r);
+    in.R = v3(rq.x.v, rq.y.v, rq.z.v);
+    in.tx_pol = v3(double(p.tx_pol[3 * t]), double(p.tx_pol[3 * t + 1]), double(p.tx_pol[3 * t + 2]));
+    const float* rp = p.rx_pol + (long long)r * p.rx_pol_stride;
+    in.rx_pol = v3(double(rp[0]), double(rp[1]), double(rp[2]));
+    const int m0 = p.sc.face_material[ed.mat_face0];
+    const int mn = face_n ? p.sc.face_material[ed.mat_face1] : -1;
+    auto slab64 = [&](int m) {
+        return Slab<double>{double(p.eps_r[m]), double(p.sigma_e[m]), double(p.mu_r[m]), double(p.gain[m]),
+                            double(p.thickness[m])};
+    };
+    in.m0 = slab64(m0);
+    in.mn = slab64(face_n ? mn : m0);
+    in.f = p.freq;
+    const double sq = sqrt(fmax(double(p.tx_power[t]), 0.0));
+    const double gg = p.g_gain ? p.g_gain[i] : 0.0;
+    const double gr = p.g_re ? p.g_re[i] : 0.0;
+    const double gi = p.g_im ? p.g_im[i] : 0.0;
+    UtdRecordGrad g;
+    const Cx<double> pf = utd_record_vjp(in, sq, gg, gr, gi, g);
+    if (p.row_field) {
+        p.row_field[2 * i] = pf.re;
+        p.row_field[2 * i + 1] = pf.im;
     }
-    if (q < pl.n) {
-        const double gg = p.g_gain ? p.g_gain[i] : 0.0;
-        const double gr = p.g_re ? p.g_re[i] : 0.0;
-        const double gi = p.g_im ? p.g_im[i] : 0.0;
-        const double dre = pf.re.d[0], dim = pf.im.d[0];
-        const double dg = 2.0 * (pf.re.v * dre + pf.im.v * dim);
-        double c = gg * dg + gr * dre + gi * dim;
+    V3<double> vab, vbb, n0b, n1b;
+    frame_vjp(va, vb, n0, n1, face_n, g, vab, vbb, n0b, n1b);
+    V3<double> fg[2][3];
+    for (int sd = 0; sd < 2; ++sd)
+        for (int k = 0; k < 3; ++k) fg[sd][k] = v3(0.0, 0.0, 0.0);
+    face_normal_vjp(fp[0][0], fp[0][1], fp[0][2], n0b, fg[0][0], fg[0][1], fg[0][2]);
+    if (face_n) face_normal_vjp(fp[1][0], fp[1][1], fp[1][2], n1b, fg[1][0], fg[1][1], fg[1][2]);
+    // the contributions, in the order tx, rx, frequency, vertices, materials
+    const DiffParamSet ps = diffraction_params(p, row);
+    long long o = p.offsets[i];
+    auto put = [&](int id, double c) {
         if (!isfinite(c)) c = 0.0;
-        p.out_ids[p.offsets[i] + q] = unsigned(w.id[0]);
-        p.out_vals[p.offsets[i] + q] = c;
+        p.out_ids[o] = unsigned(id);
+        p.out_vals[o] = c;
+        ++o;
+    };
+    auto pick = [](V3<double> a, int comp) { return comp == 0 ? a.x : (comp == 1 ? a.y : a.z); };
+    if (p.want & kWantTx)
+        for (int k = 0; k < 3; ++k) put(p.base_tx + 3 * t + k, pick(g.S, k));
+    if ((p.want & kWantRx) && p.rx_kind == 0)
+        for (int k = 0; k < 3; ++k) put(p.base_rx + 3 * r + k, pick(g.R, k));
+    if (p.want & kWantFreq) put(p.gid_freq, g.f);
+    for (int a = 0; a < ps.nv; ++a) {
+        const int v = ps.vid[a];
+        V3<double> gv = v3(0.0, 0.0, 0.0);
+        if (v == tp[0]) gv = gv + vab;
+        if (v == tp[1]) gv = gv + vbb;
+        for (int sd = 0; sd < 2; ++sd)
+            for (int k = 0; k < 3; ++k)
+                if (fv[sd][k] == v) gv = gv + fg[sd][k];
+        for (int k = 0; k < 3; ++k) put(gid_vertex(v, k), pick(gv, k));
+    }
+    if (ps.m0 >= 0) {
+        put(p.base_meps + ps.m0, g.eps0 + (ps.same_material ? g.epsn : 0.0));
+        put(p.base_msig + ps.m0, g.sig0 + (ps.same_material ? g.sign : 0.0));
+    }
+    if (ps.mn >= 0) {
+        put(p.base_meps + ps.mn, g.epsn);
+        put(p.base_msig + ps.mn, g.sign);
     }
 }
 
-void launch_vjp_diffraction(const AdjParams& p, const int* pair_base, long long total, cudaStream_t s);
+void launch_vjp_diffraction(const AdjParams& p, cudaStream_t s);
 void fill_params(AdjParams& p, const SceneHandle* h, const wcb_solve_desc* desc, const wcb_materials* materials,
                  int freq_index, const void* rows, const int64_t* selected, long long K, const int64_t* layout);
 

@@ -5,10 +5,10 @@
 namespace wcb {
 namespace adj {
 
-// One thread per (record, parameter) over the diffraction records.
-void launch_vjp_diffraction(const AdjParams& p, const int* pair_base, long long total, cudaStream_t s) {
-    if (p.order_count <= 0 || total <= 0) return;
-    k_vjp_pairs<2><<<unsigned((total + kBlock - 1) / kBlock), kBlock, 0, s>>>(p, pair_base, total);
+// Reverse mode over the diffraction records (one thread per record).
+void launch_vjp_diffraction(const AdjParams& p, cudaStream_t s) {
+    if (p.order_count <= 0) return;
+    k_vjp_diffraction<2><<<unsigned((p.order_count + kBlock - 1) / kBlock), kBlock, 0, s>>>(p);
 }
 
 // Forward mode over the diffraction records (one thread per record).

@@ -62,6 +62,25 @@ WCB_HD void halfspace_fresnel(T cos_theta, const Slab<T>& m, F frequency, Cx<T>*
     *r_tm = ((eta_ct - root) / (eta_ct + root)) * m.gain;
 }
 
+// 1 + gain * r of halfspace_fresnel, formed without the cancellation near
+// grazing incidence (r -> -1): with a = mu cos, b = root (resp. eta cos, b),
+// 1 + g (a - b) / (a + b) = ((1 + g) a + (1 - g) b) / (a + b).
+template <typename T, typename F = double>
+WCB_HD void halfspace_fresnel_one_plus(T cos_theta, const Slab<T>& m, F frequency, Cx<T>* p_te, Cx<T>* p_tm) {
+    const T omega = T(s_max(kTwoPi * frequency, kUtdSmallEps));
+    T ct = s_abs(cos_theta);
+    ct = s_min(s_max(ct, T(kUtdSmallEps)), T(1));
+    const T sin2 = s_max(T(1) - ct * ct, T(0));
+    const Cx<T> eta = cx(s_max(m.eps_r, T(kUtdSmallEps)), -s_max(m.sigma_e, T(0)) / (omega * T(kEps0)));
+    const T mu = s_max(m.mu_r, T(kUtdSmallEps));
+    const Cx<T> root = csqrt(eta * mu - cx(sin2, T(0)));
+    const Cx<T> mu_ct = cx(mu * ct, T(0));
+    const Cx<T> eta_ct = eta * ct;
+    const T gp = T(1) + m.gain, gm = T(1) - m.gain;
+    *p_te = (mu_ct * gp + root * gm) / (mu_ct + root);
+    *p_tm = (eta_ct * gp + root * gm) / (eta_ct + root);
+}
+
 // One specular bounce of the transported field (the loop body of
 // _reference_fields.py:143-181).  Updates `value` and `outgoing`.
 template <typename T, typename F = double>

@@ -176,6 +176,75 @@ WCB_HD Cx<T> kp_term(T beta, T n, T kl, int s) {
     return transition(T(2) * kl * se * se) * (ch / sh);
 }
 
+// One KP term with the odd/even corner mend of the monotone truncation
+// (F5e/F5f): the term at beta and, inside the locality window of its corner
+// b*, its odd part through the mirrored angle 2 b* - beta; t_mono and gamma
+// weight the even and odd parts.  kl sets the window widths (4 and C_BLEND
+// times sqrt(2 pi / kl)).
+template <typename T>
+WCB_HD Cx<T> mended_term(T beta, T nn, T kl, T t_mono, T gamma, int sgn, bool incident_group) {
+    const T unit = s_sqrt(T(kTwoPi) / kl);
+    const T delta_w = T(4) * unit;
+    const T delta_b = T(kCBlend) * unit;
+    T b_star;
+    if (incident_group) {
+        b_star = value_of(s_abs(beta - T(kPi))) <= value_of(s_abs(beta + T(kPi))) ? T(kPi) : T(-kPi);
+    } else {
+        const T other = (T(2) * nn - T(1)) * T(kPi);
+        b_star = value_of(s_abs(beta - T(kPi))) <= value_of(s_abs(beta - other)) ? T(kPi) : other;
+    }
+    const T delta = beta - b_star;
+    const T rw = delta / delta_w;
+    T w = s_exp(-rw * rw);
+    if (value_of(w) <= kWindowCutoff) w = T(0);
+    // the term and, inside the locality window, its mirror through one
+    // inlined copy of kp_term; outside the window the odd part vanishes
+    Cx<T> value = cx(T(0), T(0)), mirrored = cx(T(0), T(0));
+    const int nterms = value_of(w) > 0 ? 2 : 1;
+#pragma unroll 1
+    for (int m = 0; m < nterms; ++m) {
+        const Cx<T> v = kp_term(m == 0 ? beta : T(2) * b_star - beta, nn, kl, sgn);
+        if (m == 0) value = v;
+        else mirrored = v;
+    }
+    if (nterms == 1) mirrored = value;
+    const Cx<T> odd = (value - mirrored) * (T(0.5) * w);
+    const T rb = delta / delta_b;
+    const T wb = s_exp(-rb * rb);
+    const T blend = wb + (T(1) - wb) * t_mono;
+    return (value - odd) * t_mono + odd * (gamma * blend);
+}
+
+// One end's share of the finite-edge monotone factor
+// t_mono = 1 - (|F(a_lo)| + |F(a_hi)|) / sqrt(2), F(x) = (1+j)/2 - (C(x) + jS(x)),
+// from the end's FP64 argument x.  For x >= 0 it returns |F(x)| / sqrt(2) (at
+// most 1/2, smooth in x).  For x = -u < 0 (the stationary point beyond this
+// end) it returns 1 - |F(-u)| / sqrt(2): with c = F(u),
+// |F(-u)|^2 = |(1+j) - c|^2 = 2 - 2 (Re c + Im c) + |c|^2, so the share is
+// (2 (Re c + Im c) - |c|^2) / (sqrt(2) (sqrt(2) + |F(-u)|)), a small number
+// 1 - (...) would form by cancellation.  It ripples with the phase pi u^2 / 2
+// of c = u e^{j pi u^2/2} h(u), which FP32 cannot resolve at u ~ 100 (the
+// FP32 argument alone moves it by 1e-2 rad), so that phase comes from the
+// FP64 argument; h (smooth) is the T-precision continued fraction.
+template <typename T>
+WCB_HD T fresnel_end_share(double x) {
+    const T inv_sqrt2 = T(0.70710678118654752440);
+    if (x >= 0.0) return fresnel_complement_abs(T(x)) * inv_sqrt2;
+    const double u = -x;
+    const FresnelPair<T> p = fresnel_pos(T(u), false);
+    Cx<T> c;
+    if (p.has_h) {
+        double ph = kPi / 2 * u * u;
+        ph = ph - kTwoPi * floor(ph / kTwoPi);
+        c = cexpj<T>(T(ph)) * p.h * T(u);
+    } else {
+        c = p.complement;
+    }
+    const T f = cabs(cx(T(1), T(1)) - c);
+    const T sqrt2 = T(1.41421356237309504880);
+    return (T(2) * (c.re + c.im) - cabs2(c)) / (sqrt2 * (sqrt2 + f));
+}
+
 // Selected diffraction edge (device layout, FP64 geometry).
 struct EdgeDev {
     double pos[3];     // midpoint
@@ -272,8 +341,10 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
     const T nn = T(n);
     const T npi = nn * T(kPi);
     if (value_of(phi_p) > value_of(npi)) return out;
+    bool on_face_n = false;  // receiver inside the wedge, its angle clamped onto face n
     if (value_of(phi) > value_of(npi)) {
-        phi = (value_of(phi - npi) < value_of(T(kTwoPi) - phi)) ? npi : T(0);
+        on_face_n = value_of(phi - npi) < value_of(T(kTwoPi) - phi);
+        phi = on_face_n ? npi : T(0);
     }
     out.valid = true;
     const V3<T> sh_p = cast3<T>(sp_vec * (G(1) / s_p));
@@ -293,30 +364,72 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
     const T tsT = T(t_star);
     const T tmax = T(ed.half_length), tmin = -T(ed.half_length);
     const T inv_sqrt2 = T(0.70710678118654752440);
-    // both ends through one inlined copy of the Fresnel complement
-    T hi_abs = T(0), lo_abs = T(0);
+    T t_mono;
+    if constexpr (sizeof(T) == 4) {
+        // both ends through one inlined copy, from their FP64 arguments (FP64
+        // geometry); the end the stationary point lies beyond contributes
+        // 1 - |F|/sqrt(2), so a tail factor is a difference of two small
+        // numbers instead of a small residue of O(1) ones
+        const double cb64 = fmin(fmax(value_of(dot(sp_vec, e)) / value_of(s_p), -1.0), 1.0);
+        const double sb64 = fmax(sqrt(fmax(1.0 - cb64 * cb64, 0.0)), 1e-6);
+        const double sp64 = value_of(s_p), s64 = value_of(s);
+        const double kappa64 = sb64 * sb64 / sp64 + sb64 * sb64 / s64;
+        const double sigma64 = sqrt(value_of(k) * kappa64 / kPi);
+        const double hl64 = value_of(ed.half_length), ts64 = value_of(t_star);
+        const double a_hi = sigma64 * (hl64 - ts64), a_lo = sigma64 * (hl64 + ts64);
+        T share_hi = T(0), share_lo = T(0);
 #pragma unroll 1
-    for (int e2 = 0; e2 < 2; ++e2) {
-        const T v = fresnel_complement_abs(e2 == 0 ? sigma * (tmax - tsT) : -(sigma * (tmin - tsT)));
-        if (e2 == 0) hi_abs = v;
-        else lo_abs = v;
+        for (int e2 = 0; e2 < 2; ++e2) {
+            const T v = fresnel_end_share<T>(e2 == 0 ? a_hi : a_lo);
+            if (e2 == 0) share_hi = v;
+            else share_lo = v;
+        }
+        const bool beyond_hi = a_hi < 0.0, beyond_lo = a_lo < 0.0;
+        T tm;
+        if (beyond_hi && beyond_lo) tm = share_hi + share_lo - T(1);
+        else if (beyond_hi) tm = share_hi - share_lo;
+        else if (beyond_lo) tm = share_lo - share_hi;
+        else tm = T(1) - share_hi - share_lo;
+        t_mono = s_min(s_max(tm, T(0)), T(1));
+    } else {
+        // both ends through one inlined copy of the Fresnel complement
+        T hi_abs = T(0), lo_abs = T(0);
+#pragma unroll 1
+        for (int e2 = 0; e2 < 2; ++e2) {
+            const T v = fresnel_complement_abs(e2 == 0 ? sigma * (tmax - tsT) : -(sigma * (tmin - tsT)));
+            if (e2 == 0) hi_abs = v;
+            else lo_abs = v;
+        }
+        t_mono = s_min(s_max(T(1) - inv_sqrt2 * lo_abs - inv_sqrt2 * hi_abs, T(0)), T(1));
     }
-    const T t_mono = s_min(s_max(T(1) - inv_sqrt2 * lo_abs - inv_sqrt2 * hi_abs, T(0)), T(1));
     T u;
     if (value_of(s_abs(tsT - tmax)) < value_of(s_abs(tsT - tmin))) u = sigma * (tsT - tmax);
     else u = sigma * (tmin - tsT);
     const T gamma = T(1) / (T(1) + s_exp(s_min(u / T(kGammaScale), T(80))));
-    const T unit = s_sqrt(T(kTwoPi) / kl);
-    const T delta_w = T(4) * unit;
-    const T delta_b = T(kCBlend) * unit;
     // face factors: interface (half-space) Fresnel at the wedge angles; a
     // half-plane's absent second face reflects nothing
+    // (FP32 forms 1 + R without cancellation near grazing and takes R from it)
     Cx<T> r0_te, r0_tm, rn_te = cx(T(0), T(0)), rn_tm = cx(T(0), T(0));  // faces 0 and n, one inlined copy
+    Cx<T> p0_te = cx(T(1), T(0)), p0_tm = p0_te, pn_te = p0_te, pn_tm = p0_te;  // 1 + R (FP32)
     const int faces = ed.face_n ? 2 : 1;
 #pragma unroll 1
     for (int face = 0; face < faces; ++face) {
         Cx<T> te, tm;
-        halfspace_fresnel(s_sin(face == 0 ? phi_p : npi - phi), face == 0 ? m0 : mn, frequency, &te, &tm);
+        const T sin_face = s_sin(face == 0 ? phi_p : npi - phi);
+        if constexpr (sizeof(T) == 4) {
+            halfspace_fresnel_one_plus(sin_face, face == 0 ? m0 : mn, frequency, &te, &tm);
+            if (face == 0) {
+                p0_te = te;
+                p0_tm = tm;
+            } else {
+                pn_te = te;
+                pn_tm = tm;
+            }
+            te = te - cx(T(1), T(0));
+            tm = tm - cx(T(1), T(0));
+        } else {
+            halfspace_fresnel(sin_face, face == 0 ? m0 : mn, frequency, &te, &tm);
+        }
         if (face == 0) {
             r0_te = te;
             r0_tm = tm;
@@ -327,48 +440,40 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
     }
     const T bm = phi - phi_p;
     const T bp = phi + phi_p;
-    auto mended = [&](T beta, int sgn, bool incident_group) __attribute__((always_inline)) -> Cx<T> {
-        T b_star;
-        if (incident_group) {
-            b_star = value_of(s_abs(beta - T(kPi))) <= value_of(s_abs(beta + T(kPi))) ? T(kPi) : T(-kPi);
-        } else {
-            const T other = (T(2) * nn - T(1)) * T(kPi);
-            b_star = value_of(s_abs(beta - T(kPi))) <= value_of(s_abs(beta - other)) ? T(kPi) : other;
-        }
-        const T delta = beta - b_star;
-        const T rw = delta / delta_w;
-        T w = s_exp(-rw * rw);
-        if (value_of(w) <= kWindowCutoff) w = T(0);
-        // the term and, inside the locality window, its mirror through one
-        // inlined copy of kp_term; outside the window the odd part vanishes
-        Cx<T> value = cx(T(0), T(0)), mirrored = cx(T(0), T(0));
-        const int nterms = value_of(w) > 0 ? 2 : 1;
-#pragma unroll 1
-        for (int m = 0; m < nterms; ++m) {
-            const Cx<T> v = kp_term(m == 0 ? beta : T(2) * b_star - beta, nn, kl, sgn);
-            if (m == 0) value = v;
-            else mirrored = v;
-        }
-        if (nterms == 1) mirrored = value;
-        const Cx<T> odd = (value - mirrored) * (T(0.5) * w);
-        const T rb = delta / delta_b;
-        const T wb = s_exp(-rb * rb);
-        const T blend = wb + (T(1) - wb) * t_mono;
-        return (value - odd) * t_mono + odd * (gamma * blend);
-    };
+    // FP32 with the receiver angle clamped onto face n (phi = n pi): there the
+    // KP arguments of the (beta-, +) and (beta+, -) terms, and of the (beta-, -)
+    // and (beta+, +) terms, differ by 2 n pi and their corner mends pair up,
+    // so the sums are (1 + R_0) T0 + (1 + R_n) T1.  R_n sits at grazing
+    // incidence (-1 + 1e-6) and R_0 at grazing too when the source lies near
+    // face 0's plane: the direct sums are residues FP32 cannot form by
+    // cancellation (cot near zero differs between the paired terms in the last
+    // bits).  The paired form with 1 + R formed directly has no cancellation.
+    bool merge_n = false;
+    if constexpr (sizeof(T) == 4) merge_n = on_face_n && ed.face_n && value_of(phi_p) > 0;
     // the four KP terms: (beta-, +), (beta-, -) incident; (beta+, +) weighted by
     // R_n, (beta+, -) weighted by R_0.  One loop body (not four inlined
     // copies) keeps the kernel's instruction footprint small.
     Cx<T> sum_soft = cx(T(0), T(0)), sum_hard = cx(T(0), T(0));
+    Cx<T> t0v = cx(T(0), T(0)), t1v = cx(T(0), T(0));
+    const int nterms = merge_n ? 2 : 4;
 #pragma unroll 1
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < nterms; ++q) {
         const bool incident = q < 2;
-        const Cx<T> term = mended(incident ? bm : bp, (q & 1) ? -1 : +1, incident);
+        const Cx<T> term = mended_term(incident ? bm : bp, nn, kl, t_mono, gamma, (q & 1) ? -1 : +1, incident);
+        if (merge_n) {
+            if (q == 0) t0v = term;
+            else t1v = term;
+            continue;
+        }
         const Cx<T> one = cx(T(1), T(0));
         const Cx<T> w_soft = incident ? one : (q == 2 ? rn_te : r0_te);
         const Cx<T> w_hard = incident ? one : (q == 2 ? rn_tm : r0_tm);
         sum_soft = sum_soft + w_soft * term;
         sum_hard = sum_hard + w_hard * term;
+    }
+    if (merge_n) {
+        sum_soft = p0_te * t0v + pn_te * t1v;
+        sum_hard = p0_tm * t0v + pn_tm * t1v;
     }
     // pre = -exp(-j pi/4) / (2 n sqrt(2 pi k) sin_b)
     const T pre_mag = T(1) / (T(2) * nn * s_sqrt(T(kTwoPi) * kT) * sin_b);
