@@ -301,9 +301,12 @@ int wcb_accumulate_flat_backward(const uint8_t* valid, const int32_t* tx_id, con
  * layout[8] is the total.  `want` bits: 1 Tx, 2 Rx, 4 frequency, 8 vertices,
  * 16 materials (unrequested parts are written as zeros); vertex_mask (V bytes,
  * NULL = all) limits the vertex gradient to the vertices marked nonzero.  Records are
- * re-evaluated from raw scene values in FP64 dual numbers (no stored
- * intermediates); the per-parameter sums are deterministic.  row_field
- * (optional, (K,2) FP64) receives each record's re-evaluated path field. */
+ * re-evaluated from raw scene values in FP64 (no stored intermediates): LoS,
+ * reflection and transmission records in dual numbers, diffraction records by
+ * a reverse-mode sweep; the per-parameter sums are deterministic.  row_field
+ * (optional, (K,2) FP64) receives each record's re-evaluated path field.
+ * order / comp_counts (optional, from wcb_rows_order on the same selection)
+ * replace the call's own grouping of the records. */
 int wcb_rows_vjp_layout(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_materials* materials,
                         int64_t* layout);
 int wcb_rows_vjp_workspace_size(int64_t num_selected, int32_t max_depth, int32_t max_layers, int64_t* bytes);
@@ -311,7 +314,8 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
                  int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
                  const double* grad_path_gain, const double* grad_field_real, const double* grad_field_imag,
                  int32_t want, const uint8_t* vertex_mask, double* grad_out, int64_t grad_size, double* row_field,
-                 void* workspace, int64_t workspace_bytes, void* stream);
+                 const int32_t* order, const int64_t* comp_counts, void* workspace, int64_t workspace_bytes,
+                 void* stream);
 
 /* Fixed-topology JVP of selected path records (replaces the reference's
  * forward-mode companions run inside the forward pass for ad_mode="jvp":
@@ -323,11 +327,26 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
  * derivative of each record's powered path field (real, imag), and optionally
  * row_field (K,2) FP64, the re-evaluated field.  With tangent NULL only
  * row_field is written (a plain FP64 evaluation, no dual lane): the records'
- * fields the derivatives are linearised at.  No workspace, no host sync. */
+ * fields the derivatives are linearised at.  order / comp_counts (optional,
+ * from wcb_rows_order) run each component's records in that order.  No
+ * workspace, no host sync. */
 int wcb_rows_jvp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_materials* materials,
                  int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
                  const double* tangent, int64_t tangent_size, double* row_field, double* row_field_tangent,
-                 void* stream);
+                 const int32_t* order, const int64_t* comp_counts, void* stream);
+
+/* Execution order of selected records for the derivative kernels (no
+ * reference counterpart: it only reorders their work).  order (K int32)
+ * receives the selection indices grouped by component (LoS, reflection,
+ * transmission, diffraction), then depth, diffraction records by edge,
+ * selection order kept within a group; comp_counts (host, 4 int64) the group
+ * sizes.  Warps of one edge share the wedge and most branches of the UTD.
+ * The result depends only on the records, so one order serves every
+ * frequency and pass over them.  Synchronises its stream.  Workspace:
+ * wcb_rows_order_workspace_size bytes. */
+int wcb_rows_order_workspace_size(int64_t num_selected, int64_t* bytes);
+int wcb_rows_order(const wcb_scene* scene, const void* rows, const int64_t* selected, int64_t num_selected,
+                   int32_t* order, int64_t* comp_counts, void* workspace, int64_t workspace_bytes, void* stream);
 
 /* Channel frequency response of path records (replaces PathResult.cfr,
  * path.py:646-656): per (tx, rx) cell and subcarrier k,
@@ -394,8 +413,12 @@ int wcb_los_jones(const int64_t* pair_index, int64_t num_rows, const float* sour
  * finalize kernels, values[9..11] rays of the first three, values[12..16]
  * reflection candidates per depth, values[17] prefiltered diffraction
  * edges (both for the first transmitter) and values[18] the ms of the
- * diffraction visibility kernel (part of values[7]).  `values` holds 19
- * doubles. */
+ * diffraction visibility kernel (part of values[7]).  Accumulated since the
+ * last wcb_profile_enable(1): values[19] rays of every solve (preparation and
+ * main kernels), values[20] ms of the reverse-mode diffraction VJP kernel
+ * (wcb_rows_vjp brackets it with events and synchronises its stream),
+ * values[21] the diffraction records it processed, values[22] its launches.
+ * `values` holds 23 doubles. */
 int wcb_profile_enable(int32_t enabled);
 int wcb_profile_read(double* values);
 

@@ -270,3 +270,26 @@ def test_vjp_is_deterministic_and_matches_forward():
     assert torch.equal(grads[0], grads[1])
     plain = solve(scene, Config(components={"los", "reflection"}, max_depth=2), reference_frequency_hz=3.0e9)
     torch.testing.assert_close(res.path_gain.detach(), plain.path_gain, rtol=1e-4, atol=1e-12)
+
+
+@pytest.mark.parametrize("make, comps, depth", [(two_wall, {"los", "reflection"}, 2),
+                                                (wedge, {"diffraction"}, 1),
+                                                (thin_walls, {"los", "transmission", "reflection"}, 2)])
+def test_fp64_record_search_gives_the_same_records_and_gradients(make, comps, depth):
+    """``precision="fp64"`` with ``ad_mode="vjp"`` (the plain all-FP64 form):
+    the record search runs in FP64, the values and derivatives are FP64 in
+    both forms, so the same records give the same gradients."""
+    out = []
+    for prec in ("mixed", "fp64"):
+        scene = make()
+        freq_t = torch.tensor(3.0e9, dtype=torch.float64, requires_grad=True)
+        res = solve(scene, Config(components=comps, max_depth=depth, ad_mode="vjp", export_paths=True),
+                    reference_frequency_hz=freq_t, precision=prec)
+        (res.path_gain.double().sum() * 1e6).backward()
+        g = torch.cat([st.vertices.grad.reshape(-1) for st in scene.structures] + [freq_t.grad.reshape(1)])
+        out.append((res, g))
+    (a, ga), (b, gb) = out
+    for name in ("tx_id", "rx_id", "component_id", "depth", "edge_id", "primitive_sequence"):
+        assert torch.equal(getattr(a.paths, name), getattr(b.paths, name)), name
+    torch.testing.assert_close(a.path_gain, b.path_gain, rtol=1e-6, atol=0.0)
+    torch.testing.assert_close(ga, gb, rtol=1e-9, atol=1e-12 * float(ga.abs().max()))

@@ -154,6 +154,8 @@ EXPORTED_SYMBOLS = (
     "wcb_rows_vjp_workspace_size",
     "wcb_rows_vjp",
     "wcb_rows_jvp",
+    "wcb_rows_order_workspace_size",
+    "wcb_rows_order",
     "wcb_cfr_workspace_size",
     "wcb_cfr",
     "wcb_field_free_space",
@@ -223,9 +225,13 @@ def load() -> ctypes.CDLL:
     lib.wcb_rows_vjp_workspace_size.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, _i64p]
     lib.wcb_rows_vjp.argtypes = [_vp, ctypes.POINTER(SolveDesc), ctypes.POINTER(Materials), ctypes.c_int32, _vp, _vp,
                                  ctypes.c_int64, _vp, _vp, _vp, ctypes.c_int32, _vp, _vp, ctypes.c_int64, _vp, _vp,
-                                 ctypes.c_int64, _vp]
+                                 ctypes.POINTER(ctypes.c_int64), _vp, ctypes.c_int64, _vp]
     lib.wcb_rows_jvp.argtypes = [_vp, ctypes.POINTER(SolveDesc), ctypes.POINTER(Materials), ctypes.c_int32, _vp, _vp,
-                                 ctypes.c_int64, _vp, ctypes.c_int64, _vp, _vp, _vp]
+                                 ctypes.c_int64, _vp, ctypes.c_int64, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int64),
+                                 _vp]
+    lib.wcb_rows_order_workspace_size.argtypes = [ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+    lib.wcb_rows_order.argtypes = [_vp, _vp, _vp, ctypes.c_int64, _vp, ctypes.POINTER(ctypes.c_int64), _vp,
+                                   ctypes.c_int64, _vp]
     lib.wcb_cfr_workspace_size.argtypes = [ctypes.c_int32, ctypes.c_int32, _i64p]
     lib.wcb_cfr.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                             ctypes.c_double, ctypes.c_double, _vp, ctypes.c_int32, _vp, _vp, ctypes.c_int64, _vp]
@@ -287,14 +293,16 @@ def profile_enable(enabled: bool) -> None:
 
 
 def profile_read() -> dict:
-    vals = (ctypes.c_double * 19)()
+    vals = (ctypes.c_double * 23)()
     check(load().wcb_profile_read(vals), "wcb_profile_read")
     return {"main_ms": vals[0], "prep_ms": vals[1], "rays": int(vals[2]), "main_launches": int(vals[3]),
             "prep_rays": int(vals[4]),
             "kernel_ms": {"k_los_trans": vals[5], "k_reflect": vals[6], "k_diffract": vals[7], "k_finalize": vals[8],
                           "k_diffract_vis": vals[18], "k_diffract_utd": vals[7] - vals[18]},
             "kernel_rays": {"k_los_trans": int(vals[9]), "k_reflect": int(vals[10]), "k_diffract": int(vals[11])},
-            "chains": [int(v) for v in vals[12:17]], "edges": int(vals[17])}
+            "chains": [int(v) for v in vals[12:17]], "edges": int(vals[17]),
+            "acc_rays": int(vals[19]), "acc_vjp_diffraction_ms": vals[20],
+            "acc_vjp_diffraction_records": int(vals[21]), "acc_vjp_diffraction_launches": int(vals[22])}
 
 
 def build_info() -> str:

@@ -59,6 +59,29 @@ class _State:
     layer_counts: list
     vertex_mask: torch.Tensor | None = None
     param_total: int = 0    # length of the native parameter layout
+    order: Any = None       # execution order of the records (wcb_rows_order), made on first use
+    comp_counts: Any = None  # its four group sizes (ctypes int64 array)
+
+
+def _record_order(state: _State):
+    """The records' execution order for the derivative kernels (grouped by
+    component, depth and diffraction edge), computed once per record set and
+    shared by every frequency's linearisation and VJP."""
+    if state.order is None:
+        lib = _native.load()
+        device = state.rows.device
+        K = int(state.selected.shape[0])
+        order = torch.zeros(max(K, 1), dtype=torch.int32, device=device)
+        counts = (ctypes.c_int64 * 4)()
+        nbytes = ctypes.c_int64()
+        _native.check(lib.wcb_rows_order_workspace_size(K, ctypes.byref(nbytes)), "wcb_rows_order_workspace_size")
+        ws = _ORDER_WORKSPACE.get(nbytes.value, device)
+        _native.check(lib.wcb_rows_order(state.compiled.native.handle, _native.ptr(state.rows) if K else None,
+                                         _native.ptr(state.selected) if K else None, K, _native.ptr(order), counts,
+                                         _native.ptr(ws), ws.numel(), _native.stream_handle(device)),
+                      "wcb_rows_order")
+        state.order, state.comp_counts = order, counts
+    return state.order, state.comp_counts
 
 
 def _linearisation(state: _State, fi: int) -> dict:
@@ -139,14 +162,15 @@ def rows_vjp(state: _State, freq_index: int, g_gain: torch.Tensor | None, g_re: 
     _native.check(lib.wcb_rows_vjp_workspace_size(K, int(state.max_depth), int(max_layers), ctypes.byref(nbytes)),
                   "wcb_rows_vjp_workspace_size")
     ws = _VJP_WORKSPACE.get(nbytes.value, device)
+    order, counts = _record_order(state)
     grad = torch.zeros(max(total, 1), dtype=torch.float64, device=device)
     _native.check(
         lib.wcb_rows_vjp(state.compiled.native.handle, ctypes.byref(desc), ctypes.byref(ms), int(freq_index),
                          _native.ptr(state.rows) if K else None, _native.ptr(state.selected) if K else None, K,
                          _native.ptr(g_gain), _native.ptr(g_re), _native.ptr(g_im), int(want),
                          _native.ptr(vertex_mask), _native.ptr(grad),
-                         grad.numel(), _native.ptr(row_field), _native.ptr(ws), ws.numel(),
-                         _native.stream_handle(device)),
+                         grad.numel(), _native.ptr(row_field), _native.ptr(order), counts, _native.ptr(ws),
+                         ws.numel(), _native.stream_handle(device)),
         "wcb_rows_vjp",
     )
     del keep
@@ -154,6 +178,7 @@ def rows_vjp(state: _State, freq_index: int, g_gain: torch.Tensor | None, g_re: 
 
 
 _VJP_WORKSPACE = engine.Workspace()
+_ORDER_WORKSPACE = engine.Workspace()
 
 
 def _param_total(compiled, ep, mats, frequencies, bits, config) -> int:
@@ -180,11 +205,13 @@ def rows_jvp(state: _State, freq_index: int, tangent: torch.Tensor | None) -> tu
     dfield = torch.zeros((max(K, 1), 2), dtype=torch.float64, device=device)
     if tangent is not None:
         tangent = tangent.to(device=device, dtype=torch.float64).contiguous()
+    order, counts = _record_order(state)
     _native.check(
         lib.wcb_rows_jvp(state.compiled.native.handle, ctypes.byref(desc), ctypes.byref(ms), int(freq_index),
                          _native.ptr(state.rows) if K else None, _native.ptr(state.selected) if K else None, K,
                          _native.ptr(tangent), 0 if tangent is None else tangent.numel(), _native.ptr(field),
-                         None if tangent is None else _native.ptr(dfield), _native.stream_handle(device)),
+                         None if tangent is None else _native.ptr(dfield), _native.ptr(order), counts,
+                         _native.stream_handle(device)),
         "wcb_rows_jvp",
     )
     del keep
@@ -286,12 +313,15 @@ class _SolveFunction(torch.autograd.Function):
         return tuple(torch.stack([o[k] for o in per_freq]).to(torch.float32) for k in ACCUM_FIELDS)
 
 
-def vjp_forward(scene: Any, config, frequencies_hz, evaluate_rows: bool | None = None) -> dict:
+def vjp_forward(scene: Any, config, frequencies_hz, evaluate_rows: bool | None = None,
+                precision: str = "mixed") -> dict:
     """Row-mode forward at every frequency (geometry and records frozen once)
     with autograd-connected cell outputs: ``path_gain``/``field_total_*`` (NF,T,R),
     ``component_*`` (NF,6,T,R) in the flat (tx, rx) order, plus the records.
     ``evaluate_rows`` (default: ``config.export_paths``) adds the FP32 row
-    evaluations a path table is built from."""
+    evaluations a path table is built from.  ``precision="fp64"`` runs the
+    record search (traversal, candidate tests) in FP64 as well; the values and
+    derivatives are FP64 in both forms."""
     if not config.coherent and "diffraction" in config.components:
         raise NotImplementedError("ad_mode='vjp' with incoherent accumulation and diffraction is not provided")
     device = torch.device("cuda", torch.cuda.current_device())
@@ -307,8 +337,9 @@ def vjp_forward(scene: Any, config, frequencies_hz, evaluate_rows: bool | None =
     mats = compiled.material_tables(frequencies, device)
     bits = engine.component_bits(config.components)
     T, R = ep.num_tx, ep.num_rx
+    prec = _native.PRECISION_FP64 if precision == "fp64" else _native.PRECISION_MIXED
     res = engine.run_solve(compiled, ep, mats, frequencies, components=bits, max_depth=config.max_depth,
-                           coherent=config.coherent, want_rows=True)
+                           coherent=config.coherent, want_rows=True, precision=prec)
     rows = res["rows"]
     width = max(int(config.max_depth), 0)
     selected = engine.select_rows(rows, width, config.max_paths, config.max_paths_scope)
@@ -339,7 +370,7 @@ def vjp_forward(scene: Any, config, frequencies_hz, evaluate_rows: bool | None =
     return result
 
 
-def solve_vjp(scene: Any, config, reference_frequency_hz):
+def solve_vjp(scene: Any, config, reference_frequency_hz, precision: str = "mixed"):
     """The deterministic solve with ``ad_mode="vjp"``: same outputs as the
     row-mode forward, differentiable in the scene values."""
     from .deterministic import (
@@ -356,7 +387,7 @@ def solve_vjp(scene: Any, config, reference_frequency_hz):
     launches0 = _native.launch_count()
     freq = reference_frequency_hz.reshape(1) if isinstance(reference_frequency_hz, torch.Tensor) else \
         [float(reference_frequency_hz)]
-    v = vjp_forward(scene, config, freq)
+    v = vjp_forward(scene, config, freq, precision=precision)
     device = v["power_total"].device
     pt, ftr, fti = v["power_total"][0], v["field_total_real"][0], v["field_total_imag"][0]
     cp, cfr, cfi = v["component_power"][0], v["component_field_real"][0], v["component_field_imag"][0]

@@ -199,7 +199,14 @@ int wcb_field_project_complex3(int64_t n, const float* field_vector, const float
 }
 
 int wcb_profile_enable(int32_t enabled) {
-    wcb::profile_state().enabled = enabled != 0;
+    wcb::ProfileState& st = wcb::profile_state();
+    st.enabled = enabled != 0;
+    if (st.enabled) {
+        st.acc_rays = 0;
+        st.acc_vjp_diff_ms = 0.0;
+        st.acc_vjp_diff_records = 0;
+        st.acc_vjp_diff_launches = 0;
+    }
     return WCB_OK;
 }
 
@@ -216,6 +223,10 @@ int wcb_profile_read(double* values) {
     for (int i = 0; i < 5; ++i) values[12 + i] = double(st.chains[i]);
     values[17] = double(st.edges);
     values[18] = st.diffract_vis_ms;
+    values[19] = double(st.acc_rays);
+    values[20] = st.acc_vjp_diff_ms;
+    values[21] = double(st.acc_vjp_diff_records);
+    values[22] = double(st.acc_vjp_diff_launches);
     return WCB_OK;
 }
 

@@ -32,21 +32,39 @@ namespace adj {
 
 // per record: its parameter count, its (component, depth) grouping key and
 // the per-component record counts
+// per-component record counts: one atomic per warp and component (the
+// launches use whole warps; lanes past the end vote for no component)
+WCB_D void count_component(int* comp_counts, int rank) {
+    for (int r = 0; r < 4; ++r) {
+        const unsigned b = __ballot_sync(0xffffffffu, rank == r);
+        if ((threadIdx.x & 31) == 0 && b) atomicAdd(comp_counts + r, __popc(b));
+    }
+}
+
 __global__ void k_vjp_count(AdjParams p, int* keys, int* idx) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= p.count) return;
-    const RowRec row = p.rows[p.selected[i]];
-    if (row.component == 2) {
-        p.counts[i] = diffraction_params(p, row).count;
-    } else {
-        ParamList pl;
-        build_params(p, row, pl);
-        p.counts[i] = pl.n;
+    int rank = -1;
+    if (i < p.count) {
+        const RowRec row = p.rows[p.selected[i]];
+        p.counts[i] = row.component == 2 ? diffraction_params(p, row).count : face_record_param_count(p, row);
+        keys[i] = order_key(p, row);
+        idx[i] = int(i);
+        rank = component_rank(row.component);
     }
-    const int rank = component_rank(row.component);
-    keys[i] = rank * 8 + min(max(int(row.depth), 0), 7);
-    idx[i] = int(i);
-    atomicAdd(p.comp_counts + rank, 1);
+    count_component(p.comp_counts, rank);
+}
+
+// The execution-order keys alone (wcb_rows_order)
+__global__ void k_order_keys(AdjParams p, int* keys, int* idx, int* comp_counts) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    int rank = -1;
+    if (i < p.count) {
+        const RowRec row = p.rows[p.selected[i]];
+        keys[i] = order_key(p, row);
+        idx[i] = int(i);
+        rank = component_rank(row.component);
+    }
+    count_component(comp_counts, rank);
 }
 
 // Ordered per-id sums of the id-sorted pairs (a parameter's contributions
@@ -260,7 +278,8 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
                  int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
                  const double* grad_path_gain, const double* grad_field_real, const double* grad_field_imag,
                  int32_t want, const uint8_t* vertex_mask, double* grad_out, int64_t grad_size, double* row_field,
-                 void* workspace, int64_t workspace_bytes, void* stream) {
+                 const int32_t* order, const int64_t* comp_counts_in, void* workspace, int64_t workspace_bytes,
+                 void* stream) {
     if (scene == nullptr || desc == nullptr || materials == nullptr || grad_out == nullptr || num_selected < 0)
         return WCB_ERR_INVALID_ARGUMENT;
     if (num_selected > 0 && (rows == nullptr || selected == nullptr)) return WCB_ERR_INVALID_ARGUMENT;
@@ -293,28 +312,36 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
     p.comp_counts = reinterpret_cast<int*>(b + L.comp_counts);
     int* keys = reinterpret_cast<int*>(b + L.keys);
     int* keys2 = reinterpret_cast<int*>(b + L.keys2);
-    int* order = reinterpret_cast<int*>(b + L.order);
+    int* idx = reinterpret_cast<int*>(b + L.order);
     int* order2 = reinterpret_cast<int*>(b + L.order2);
     const int grid = int((K + wcb::adj::kBlock - 1) / wcb::adj::kBlock);
     cudaMemsetAsync(p.comp_counts, 0, 16, s);
-    wcb::adj::k_vjp_count<<<grid, wcb::adj::kBlock, 0, s>>>(p, keys, order);
+    wcb::adj::k_vjp_count<<<grid, wcb::adj::kBlock, 0, s>>>(p, keys, idx);
     size_t tb = L.scan_bytes;
     if (cub::DeviceScan::ExclusiveSum(b + L.scan_tmp, tb, p.counts, offsets, int(K), s) != cudaSuccess)
         return WCB_ERR_CUDA;
-    // records grouped by (component, depth), record order kept within a group
-    tb = L.scan_bytes;
-    if (cub::DeviceRadixSort::SortPairs(b + L.scan_tmp, tb, keys, keys2, order, order2, int(K), 0, 5, s) !=
-        cudaSuccess)
-        return WCB_ERR_CUDA;
+    // records grouped by component, depth and diffraction edge (wcb_rows_order's
+    // key), record order kept within a group; or the caller's order
+    if (order == nullptr) {
+        tb = L.scan_bytes;
+        if (cub::DeviceRadixSort::SortPairs(b + L.scan_tmp, tb, keys, keys2, idx, order2, int(K), 0, 31, s) !=
+            cudaSuccess)
+            return WCB_ERR_CUDA;
+    }
     wcb::note_launch(3);
     long long last_off = 0;
     int last_cnt = 0;
     int comp_counts[4] = {0, 0, 0, 0};
     cudaMemcpyAsync(&last_off, offsets + K - 1, 8, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&last_cnt, p.counts + K - 1, 4, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(comp_counts, p.comp_counts, 16, cudaMemcpyDeviceToHost, s);
+    if (order == nullptr) cudaMemcpyAsync(comp_counts, p.comp_counts, 16, cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return WCB_ERR_CUDA;
-    p.order = order2;
+    if (order != nullptr) {
+        for (int r = 0; r < 4; ++r) comp_counts[r] = int(comp_counts_in ? comp_counts_in[r] : 0);
+        p.order = order;
+    } else {
+        p.order = order2;
+    }
     const long long pairs = last_off + last_cnt;
     if (pairs >= INT_MAX) return WCB_ERR_NOT_SUPPORTED;
     L = wcb::adj::vjp_layout(K, pairs);
@@ -335,7 +362,28 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
                 case 0: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 0><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
                 case 1: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 1><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
                 case 5: wcb::adj::k_vjp_rows<wcb::adj::kLanes, 5><<<g, wcb::adj::kBlock, 0, s>>>(p); break;
-                default: wcb::adj::launch_vjp_diffraction(p, s); break;
+                default: {
+                    wcb::ProfileState& prof = wcb::profile_state();
+                    cudaEvent_t e0 = nullptr, e1 = nullptr;
+                    if (prof.enabled) {
+                        cudaEventCreate(&e0);
+                        cudaEventCreate(&e1);
+                        cudaEventRecord(e0, s);
+                    }
+                    wcb::adj::launch_vjp_diffraction(p, s);
+                    if (prof.enabled) {
+                        float ms = 0.f;
+                        cudaEventRecord(e1, s);
+                        if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) {
+                            prof.acc_vjp_diff_ms += ms;
+                            prof.acc_vjp_diff_records += p.order_count;
+                            prof.acc_vjp_diff_launches += 1;
+                        }
+                        cudaEventDestroy(e0);
+                        cudaEventDestroy(e1);
+                    }
+                    break;
+                }
             }
             wcb::note_launch();
         }
@@ -390,7 +438,7 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
 int wcb_rows_jvp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_materials* materials,
                  int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
                  const double* tangent, int64_t tangent_size, double* row_field, double* row_field_tangent,
-                 void* stream) {
+                 const int32_t* order, const int64_t* comp_counts, void* stream) {
     if (scene == nullptr || desc == nullptr || materials == nullptr || num_selected < 0)
         return WCB_ERR_INVALID_ARGUMENT;
     if (num_selected > 0 && (rows == nullptr || selected == nullptr)) return WCB_ERR_INVALID_ARGUMENT;
@@ -406,21 +454,85 @@ int wcb_rows_jvp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     wcb::adj::AdjParams p;
     wcb::adj::fill_params(p, scene->h, desc, materials, freq_index, rows, selected, num_selected, layout);
-    const unsigned g = unsigned((num_selected + wcb::adj::kBlock - 1) / wcb::adj::kBlock);
-    if (tangent == nullptr) {
-        wcb::adj::k_field64_rows<0><<<g, wcb::adj::kBlock, 0, s>>>(p, row_field);
-        wcb::adj::k_field64_rows<1><<<g, wcb::adj::kBlock, 0, s>>>(p, row_field);
-        wcb::adj::k_field64_rows<5><<<g, wcb::adj::kBlock, 0, s>>>(p, row_field);
-        wcb::adj::launch_field64_diffraction(p, row_field, s);
-        wcb::note_launch(4);
-        return cudaGetLastError() == cudaSuccess ? WCB_OK : WCB_ERR_CUDA;
+    // one launch per component: over its dense range of the execution order
+    // (wcb_rows_order), or over every record when no order is given
+    const int cids[4] = {0, 1, 5, 2};
+    long long begin = 0;
+    p.order = order;
+    for (int r = 0; r < 4; ++r) {
+        p.order_begin = order ? begin : 0;
+        p.order_count = order ? (comp_counts ? comp_counts[r] : 0) : num_selected;
+        begin += p.order_count;
+        if (p.order_count <= 0) continue;
+        const unsigned g = unsigned((p.order_count + wcb::adj::kBlock - 1) / wcb::adj::kBlock);
+        if (tangent == nullptr) {
+            switch (cids[r]) {
+                case 0: wcb::adj::k_field64_rows<0><<<g, wcb::adj::kBlock, 0, s>>>(p, row_field); break;
+                case 1: wcb::adj::k_field64_rows<1><<<g, wcb::adj::kBlock, 0, s>>>(p, row_field); break;
+                case 5: wcb::adj::k_field64_rows<5><<<g, wcb::adj::kBlock, 0, s>>>(p, row_field); break;
+                default: wcb::adj::launch_field64_diffraction(p, row_field, s); break;
+            }
+        } else {
+            switch (cids[r]) {
+                case 0: wcb::adj::k_jvp_rows<0><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent); break;
+                case 1: wcb::adj::k_jvp_rows<1><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent); break;
+                case 5: wcb::adj::k_jvp_rows<5><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent); break;
+                default: wcb::adj::launch_jvp_diffraction(p, tangent, row_field, row_field_tangent, s); break;
+            }
+        }
+        wcb::note_launch();
     }
-    wcb::adj::k_jvp_rows<0><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent);
-    wcb::adj::k_jvp_rows<1><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent);
-    wcb::adj::k_jvp_rows<5><<<g, wcb::adj::kBlock, 0, s>>>(p, tangent, row_field, row_field_tangent);
-    wcb::adj::launch_jvp_diffraction(p, tangent, row_field, row_field_tangent, s);
-    wcb::note_launch(4);
     return cudaGetLastError() == cudaSuccess ? WCB_OK : WCB_ERR_CUDA;
+}
+
+int wcb_rows_order_workspace_size(int64_t num_selected, int64_t* bytes) {
+    if (bytes == nullptr || num_selected < 0) return WCB_ERR_INVALID_ARGUMENT;
+    const size_t k = size_t(std::max<int64_t>(num_selected, 1));
+    size_t sort_b = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_b, (int*)nullptr, (int*)nullptr, (int*)nullptr, (int*)nullptr,
+                                    int(k), 0, 31);
+    *bytes = int64_t(wcb::adj::a256(k * 4) * 3 + wcb::adj::a256(16) + wcb::adj::a256(sort_b));
+    return WCB_OK;
+}
+
+int wcb_rows_order(const wcb_scene* scene, const void* rows, const int64_t* selected, int64_t num_selected,
+                   int32_t* order, int64_t* comp_counts, void* workspace, int64_t workspace_bytes, void* stream) {
+    if (scene == nullptr || order == nullptr || comp_counts == nullptr || num_selected < 0)
+        return WCB_ERR_INVALID_ARGUMENT;
+    if (num_selected > 0 && (rows == nullptr || selected == nullptr)) return WCB_ERR_INVALID_ARGUMENT;
+    for (int r = 0; r < 4; ++r) comp_counts[r] = 0;
+    if (num_selected == 0) return WCB_OK;
+    if (num_selected >= INT_MAX) return WCB_ERR_NOT_SUPPORTED;
+    int64_t need = 0;
+    wcb_rows_order_workspace_size(num_selected, &need);
+    if (workspace == nullptr || workspace_bytes < need) return WCB_ERR_CAPACITY;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t k = size_t(num_selected);
+    char* b = static_cast<char*>(workspace);
+    int* keys = reinterpret_cast<int*>(b);
+    int* keys2 = reinterpret_cast<int*>(b + wcb::adj::a256(k * 4));
+    int* idx = reinterpret_cast<int*>(b + 2 * wcb::adj::a256(k * 4));
+    int* counts = reinterpret_cast<int*>(b + 3 * wcb::adj::a256(k * 4));
+    void* tmp = b + 3 * wcb::adj::a256(k * 4) + wcb::adj::a256(16);
+    size_t tb = size_t(need) - (3 * wcb::adj::a256(k * 4) + wcb::adj::a256(16));
+    wcb::adj::AdjParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.sc = scene->h->dev;
+    p.edge_slot = scene->h->edge_slot;
+    p.rows = static_cast<const wcb::RowRec*>(rows);
+    p.selected = reinterpret_cast<const long long*>(selected);
+    p.count = num_selected;
+    bool ok = cudaMemsetAsync(counts, 0, 16, s) == cudaSuccess;
+    wcb::adj::k_order_keys<<<unsigned((k + wcb::adj::kBlock - 1) / wcb::adj::kBlock), wcb::adj::kBlock, 0, s>>>(
+        p, keys, idx, counts);
+    ok = ok && cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, idx, order, int(k), 0, 31, s) == cudaSuccess;
+    int host[4] = {0, 0, 0, 0};
+    ok = ok && cudaMemcpyAsync(host, counts, 16, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    ok = ok && cudaStreamSynchronize(s) == cudaSuccess;
+    wcb::note_launch(2);
+    if (!ok) return WCB_ERR_CUDA;
+    for (int r = 0; r < 4; ++r) comp_counts[r] = host[r];
+    return WCB_OK;
 }
 
 }  // extern "C"

@@ -145,6 +145,42 @@ WCB_D void build_params(const AdjParams& p, const RowRec& row, ParamList& pl) {
     }
 }
 
+// Parameter count of a LoS, reflection or transmission record without the
+// generic list (the count build_params gives): endpoint and frequency
+// entries, 3 per distinct wanted vertex of its faces, and per distinct face
+// material 2 (reflection: eps_r, sigma_e) or 2 per layer (transmission).
+WCB_D int face_record_param_count(const AdjParams& p, const RowRec& row) {
+    int n = ((p.want & kWantTx) ? 3 : 0) + (((p.want & kWantRx) && p.rx_kind == 0) ? 3 : 0) +
+            ((p.want & kWantFreq) ? 1 : 0);
+    if (row.component != 1 && row.component != 5) return n;
+    int vids[3 * kMaxDepth], mids[kMaxDepth];
+    int nv = 0, nm = 0;
+    const int d = min(int(row.depth), kMaxDepth);
+    for (int k = 0; k < d; ++k) {
+        const int f = row.seq[k];
+        for (int c = 0; c < 3; ++c) {
+            const int v = p.sc.faces[3 * f + c];
+            if (!vertex_wanted(p, v)) continue;
+            bool seen = false;
+            for (int q = 0; q < nv; ++q) seen = seen || vids[q] == v;
+            if (!seen) vids[nv++] = v;
+        }
+        const int m = p.sc.face_material[f];
+        bool seen = false;
+        for (int q = 0; q < nm; ++q) seen = seen || mids[q] == m;
+        if (!seen) mids[nm++] = m;
+    }
+    n += 3 * nv;
+    if (p.want & kWantMaterials) {
+        if (row.component == 1) {
+            n += 2 * nm;
+        } else {
+            for (int q = 0; q < nm; ++q) n += 2 * min(p.layer_count[mids[q]], kMaxLayersPerMaterial);
+        }
+    }
+    return n;
+}
+
 // The parameters of a diffraction record without the generic list (the same
 // set build_params gives): the distinct wanted vertices (end points, then
 // the faces' vertices), the distinct face materials, the endpoint and
@@ -389,6 +425,16 @@ WCB_D Cx<Dual<N>> eval_record(const AdjParams& p, const RowRec& row, const WT<N>
 // rank of a component in the (component, depth) grouping
 WCB_HD int component_rank(int c) { return c == 0 ? 0 : c == 1 ? 1 : c == 5 ? 2 : 3; }
 
+// Execution-order key of a record: component rank (2 bits), depth (3 bits)
+// and, for diffraction, the edge slot (26 bits), so a warp of the derivative
+// kernels works on records of one component, and diffraction warps on one
+// edge (shared wedge, mostly shared branches).
+WCB_D int order_key(const AdjParams& p, const RowRec& row) {
+    int key = (component_rank(row.component) << 29) | (min(max(int(row.depth), 0), 7) << 26);
+    if (row.component == 2) key |= p.edge_slot[row.edge] & 0x3FFFFFF;
+    return key;
+}
+
 template <int N, int COMP>
 __global__ void __launch_bounds__(kBlock) k_vjp_rows(AdjParams p) {
     const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -414,6 +460,7 @@ __global__ void __launch_bounds__(kBlock) k_vjp_rows(AdjParams p) {
             p.row_field[2 * i + 1] = pf.im.v;
         }
         for (int j = 0; j < w.n; ++j) {
+            if (pass * N + j >= p.counts[i]) break;  // never past the record's counted slots
             const double dre = pf.re.d[j], dim = pf.im.d[j];
             const double dg = 2.0 * (pf.re.v * dre + pf.im.v * dim);
             double c = gg * dg + gr * dre + gi * dim;
@@ -495,7 +542,9 @@ __global__ void __launch_bounds__(kBlock) k_vjp_diffraction(AdjParams p) {
     // the contributions, in the order tx, rx, frequency, vertices, materials
     const DiffParamSet ps = diffraction_params(p, row);
     long long o = p.offsets[i];
+    const long long o_end = o + p.counts[i];
     auto put = [&](int id, double c) {
+        if (o >= o_end) return;  // never past the record's counted slots
         if (!isfinite(c)) c = 0.0;
         p.out_ids[o] = unsigned(id);
         p.out_vals[o] = c;
@@ -536,8 +585,9 @@ void fill_params(AdjParams& p, const SceneHandle* h, const wcb_solve_desc* desc,
 template <int COMP>
 __global__ void __launch_bounds__(kBlock) k_jvp_rows(AdjParams p, const double* tangent, double* field,
                                                      double* field_tangent) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= p.count) return;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= p.order_count) return;
+    const long long i = p.order ? p.order[p.order_begin + j] : j;
     const RowRec row = p.rows[p.selected[i]];
     if (row.component != COMP) return;
     const Seeds<1> seeds{tangent};
@@ -558,8 +608,9 @@ void launch_jvp_diffraction(const AdjParams& p, const double* tangent, double* f
 // tangent): the point the cell sums are linearised at.
 template <int COMP>
 __global__ void __launch_bounds__(kBlock) k_field64_rows(AdjParams p, double* field) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= p.count) return;
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= p.order_count) return;
+    const long long i = p.order ? p.order[p.order_begin + j] : j;
     const RowRec row = p.rows[p.selected[i]];
     if (row.component != COMP) return;
     const Plain<0> seeds{};

@@ -10,6 +10,10 @@
 
 #define WCB_HD __host__ __device__ __forceinline__
 #define WCB_D __device__ __forceinline__
+// out of line (one copy per translation unit): a helper with several call
+// sites in the special-function-heavy kernels, whose inlined copies would
+// overflow the instruction cache
+#define WCB_HD_OOL __host__ __device__ __noinline__
 
 namespace wcb {
 

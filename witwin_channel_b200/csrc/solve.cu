@@ -990,6 +990,7 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
         prof.main_ms = b;
         prof.prep_rays = (long long)nr[0];
         prof.rays = (long long)(nr[1] + nr[2] + nr[3]);
+        prof.acc_rays += prof.rays + prof.prep_rays;
         for (int i = 0; i < 3; ++i) prof.kernel_rays[i] = (long long)nr[1 + i];
         for (int i = 0; i < 4; ++i) prof.kernel_ms[i] = comp_ms[i];
         prof.diffract_vis_ms = vis_ms;

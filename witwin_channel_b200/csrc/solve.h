@@ -96,6 +96,11 @@ struct ProfileState {
     long long kernel_rays[3] = {0, 0, 0};     // los+transmission, reflection, diffraction
     long long chains[5] = {0, 0, 0, 0, 0};    // reflection candidates per depth (first transmitter)
     long long edges = 0;                      // diffraction edges kept by the prefilter (first transmitter)
+    // accumulated since profiling was last enabled (over every solve and VJP)
+    long long acc_rays = 0;                   // rays traced by all solves (preparation and per-cell kernels)
+    double acc_vjp_diff_ms = 0.0;             // reverse-mode diffraction VJP kernel time
+    long long acc_vjp_diff_records = 0;       // diffraction records it processed
+    long long acc_vjp_diff_launches = 0;
 };
 ProfileState& profile_state();
 

@@ -238,7 +238,7 @@ def solve(scene: Any, config: Config, *, reference_frequency_hz, precision: str 
 
     ``precision`` selects ``"mixed"`` (FP32 traversal and fields; FP64 image
     solve, path length and phase) or ``"fp64"`` (every stage in FP64; cell
-    mode only).
+    mode, or the differentiable forward of ``ad_mode="vjp"``/``"jvp"``).
     """
 
     if not isinstance(config, Config):
@@ -251,7 +251,7 @@ def solve(scene: Any, config: Config, *, reference_frequency_hz, precision: str 
         # autograd Function when the scene values are forward-mode dual tensors
         from .autograd import solve_vjp
 
-        return solve_vjp(scene, config, reference_frequency_hz)
+        return solve_vjp(scene, config, reference_frequency_hz, precision=precision)
     device = torch.device("cuda", torch.cuda.current_device())
     compiled = compile_scene(scene, device)
     ep = _endpoints(scene, device)
