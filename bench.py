@@ -198,6 +198,17 @@ def _batched_setup(jobs: list[tuple[int, int]]):
     return full, scenes, materials, tx_leaves
 
 
+def run_leg(args) -> None:
+    """One side leg alone (``--only-leg``), its dict printed as one JSON line:
+    the small workloads the committed ncu summaries are captured on."""
+    import torch
+
+    torch.cuda.set_device(0)
+    device = torch.device("cuda", 0)
+    leg = _canyon_run(args, device) if args.only_leg == "canyon" else _vjp_run(device)
+    print(json.dumps({"leg": args.only_leg, **leg}), flush=True)
+
+
 def run_native(args) -> None:
     import torch
     import torch.distributed as dist
@@ -536,7 +547,7 @@ def _vjp_run(device, steps: int = 7) -> dict:
     the boxes displaced by N(0, 0.5 m))."""
     import torch
 
-    from witwin_channel_b200 import Config, solve
+    from witwin_channel_b200 import Config, _native, solve
     from witwin_channel_b200.workloads import gradient_run, log_mse
 
     g = gradient_run(seed=1)
@@ -566,6 +577,11 @@ def _vjp_run(device, steps: int = 7) -> dict:
         torch.cuda.synchronize()
         wall_ms.append((time.perf_counter() - t0) * 1e3)
         step_ms.append(e0.elapsed_time(e1))
+    _native.profile_enable(True)
+    step()
+    torch.cuda.synchronize()
+    prof = _native.profile_read()
+    _native.profile_enable(False)
     vg = torch.cat([v.grad.reshape(-1) for v in g["leaves"]["vertices"]])
     return {
         "workload": "urban canyon 64 boxes, 256x256 grid, 28 GHz, LoS + reflection depth 3 + UTD; loss = MSE of "
@@ -573,6 +589,8 @@ def _vjp_run(device, steps: int = 7) -> dict:
                     "concrete eps_r and sigma_e, frequency, Tx position and the 8 boxes' 64 vertices",
         "ms_per_step": float(sorted(step_ms)[len(step_ms) // 2]),
         "host_wall_ms_per_step": float(sorted(wall_ms)[len(wall_ms) // 2]),
+        "diffraction_records_per_step": prof["acc_vjp_diffraction_records"],
+        "diffraction_vjp_kernel_ms": prof["acc_vjp_diffraction_ms"],
         "steps_ms": [round(x, 3) for x in step_ms],
         "steps": steps,
         "paths": int(res.metadata["counts"]["path_count"]),
@@ -1003,11 +1021,15 @@ def main() -> None:
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-consumer", action="store_true")
     ap.add_argument("--no-canyon", action="store_true")
+    ap.add_argument("--only-leg", choices=["canyon", "vjp"], default=None,
+                    help="run one side leg alone (profiling runs); no headline line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "native":
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.only_leg:
+        run_leg(args)
     else:
         run_native(args)
 

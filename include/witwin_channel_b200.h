@@ -205,9 +205,10 @@ int wcb_rows_select_workspace_size(int64_t num_rows, int64_t* bytes);
  * library's device image; inputs whose wcb_rows_select_workspace_size exceeds
  * it (above 597,120 records) return WCB_ERR_CAPACITY before any work.  Every
  * call looks up the array's address on the current device; the first lookup
- * on a device may load the library's module there.  The call reads its counts
- * back and synchronises `stream` before returning: it blocks the calling
- * thread and cannot run inside a stream capture.  All calls on a device share
+ * on a device may load the library's module there, so make the first call on
+ * a device before any stream capture begins.  The call reads its counts back
+ * and synchronises `stream` before returning, so it blocks the calling
+ * thread.  All calls on a device share
  * the array (each call rewrites what it reads), so calls that overlap in time
  * race: serialise them. */
 #define WCB_ROWS_SELECT_NOALLOC_SCRATCH_BYTES (32ll << 20)

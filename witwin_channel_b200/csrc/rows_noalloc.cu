@@ -19,8 +19,7 @@
 //
 // Synchronisation: like wcb_rows_select, the call reads its counts back to
 // the host and synchronises `stream` before it returns, so it blocks the
-// calling thread for the duration of the selection and cannot run inside a
-// stream capture.
+// calling thread for the duration of the selection.
 //
 // Sharing: every call on a device uses the same array and leaves its last
 // contents there.  Each stage writes the scratch words it later reads (the
