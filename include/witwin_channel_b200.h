@@ -196,6 +196,15 @@ int wcb_rows_select(const void* rows, int64_t num_rows, int32_t width, int64_t m
                     int64_t* selected, int64_t* num_selected, void* workspace, int64_t workspace_bytes, void* stream);
 int wcb_rows_select_workspace_size(int64_t num_rows, int64_t* bytes);
 
+/* Integer columns of selected records (the record-to-table unpacking of
+ * propagation/topology.py:408-466 evaluated_paths_from_block): per selected
+ * index i, tx_id, rx_id, component_id, depth, primitive_sequence (5 per row),
+ * edge_id and length of rows[selected[i]].  One pass; any output may be NULL.
+ * No host sync. */
+int wcb_rows_decode(const void* rows, const int64_t* selected, int64_t num_selected, int32_t* tx_id, int32_t* rx_id,
+                    int32_t* component_id, int32_t* depth, int32_t* primitive_sequence, int32_t* edge_id,
+                    float* length, void* stream);
+
 /* wcb_rows_select without a caller workspace and without any allocation (no
  * counterpart in the reference, whose selection allocates through torch).
  * For callers that may not allocate device memory at call time: code inside

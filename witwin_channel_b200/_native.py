@@ -156,6 +156,7 @@ EXPORTED_SYMBOLS = (
     "wcb_rows_jvp",
     "wcb_rows_order_workspace_size",
     "wcb_rows_order",
+    "wcb_rows_decode",
     "wcb_cfr_workspace_size",
     "wcb_cfr",
     "wcb_field_free_space",
@@ -230,6 +231,7 @@ def load() -> ctypes.CDLL:
                                  ctypes.c_int64, _vp, ctypes.c_int64, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int64),
                                  _vp]
     lib.wcb_rows_order_workspace_size.argtypes = [ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+    lib.wcb_rows_decode.argtypes = [_vp, _vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
     lib.wcb_rows_order.argtypes = [_vp, _vp, _vp, ctypes.c_int64, _vp, ctypes.POINTER(ctypes.c_int64), _vp,
                                    ctypes.c_int64, _vp]
     lib.wcb_cfr_workspace_size.argtypes = [ctypes.c_int32, ctypes.c_int32, _i64p]

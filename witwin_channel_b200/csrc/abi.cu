@@ -113,6 +113,13 @@ int wcb_solve(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_mate
     return WCB_OK;
 }
 
+int wcb_rows_decode(const void* rows, const int64_t* selected, int64_t num_selected, int32_t* tx_id, int32_t* rx_id,
+                    int32_t* component_id, int32_t* depth, int32_t* primitive_sequence, int32_t* edge_id,
+                    float* length, void* stream) {
+    return wcb::rows_decode(rows, selected, num_selected, tx_id, rx_id, component_id, depth, primitive_sequence,
+                            edge_id, length, as_stream(stream));
+}
+
 int wcb_rows_select_workspace_size(int64_t num_rows, int64_t* bytes) {
     if (bytes == nullptr || num_rows < 0) return WCB_ERR_INVALID_ARGUMENT;
     return wcb::rows_select_workspace(num_rows, bytes);

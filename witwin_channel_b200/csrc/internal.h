@@ -48,6 +48,8 @@ void scene_destroy(SceneHandle* h);
 int scene_refit(SceneHandle* h, const float* d_vertices, int64_t nv, int* topology_changed, cudaStream_t stream);
 
 int rows_select_workspace(int64_t n, int64_t* bytes);
+int rows_decode(const void* rows, const int64_t* selected, int64_t n, int32_t* tx, int32_t* rx, int32_t* component,
+                int32_t* depth, int32_t* seq, int32_t* edge, float* length, cudaStream_t stream);
 int rows_select(const void* rows, int64_t n, int width, int64_t max_paths, int scope, int64_t* selected,
                 int64_t* num_selected, void* ws, int64_t ws_bytes, cudaStream_t stream);
 int rows_evaluate(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m, int fi, const void* rows,

@@ -685,10 +685,13 @@ __global__ void __launch_bounds__(kSplitBlock, 2) k_diffract_utd(MainParams p, i
             const V3<double> R = v3<double>(rx, ry, rz);
             const V3<T> rx_pol = v3<T>(T(px), T(py), T(pz));
             double qx = 0, qy = 0, qz = 0, len = 0;
+            // the frequency-independent geometry once, the field per frequency
+            const EdgeFrame<double> fr = edge_frame(ed);
+            const UtdGeometry<double, T> geo = utd_geometry<double, T>(fr, S, R, tx_pol);
 #pragma unroll 1
             for (int f = 0; f < NF; ++f) {
                 const DiffractionResult<T> res =
-                    utd_field<T>(ed, S, R, tx_pol, face_slab<T>(p, f, ed.mat_face0), face_slab<T>(p, f, ed.mat_face1), p.freq[f]);
+                    utd_result(geo, fr, face_slab<T>(p, f, ed.mat_face0), face_slab<T>(p, f, ed.mat_face1), p.freq[f]);
                 qx = res.q[0]; qy = res.q[1]; qz = res.q[2];
                 len = res.length;
                 const C3<T> powered = c3_scale(res.field, cx(sqrt_p, T(0)));

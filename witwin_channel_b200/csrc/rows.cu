@@ -891,4 +891,34 @@ int los_jones(int64_t n, const int64_t* pair, const float* src, int64_t num_src,
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
+// Columns of the selected records in one pass (thread per selected record):
+// the records are read once, in selection order, and every column written
+// contiguously.  Any output pointer may be NULL.
+namespace {
+__global__ void k_rows_decode(const RowRec* rows, const int64_t* selected, long long n, int* tx, int* rx, int* comp,
+                              int* depth, int* seq, int* edge, float* len) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const RowRec r = rows[selected[i]];
+    if (tx) tx[i] = r.tx;
+    if (rx) rx[i] = r.rx;
+    if (comp) comp[i] = int(r.component);
+    if (depth) depth[i] = int(r.depth);
+    if (seq)
+        for (int k = 0; k < 5; ++k) seq[5 * i + k] = r.seq[k];
+    if (edge) edge[i] = r.edge;
+    if (len) len[i] = r.length;
+}
+}  // namespace
+
+int rows_decode(const void* rows, const int64_t* selected, int64_t n, int32_t* tx, int32_t* rx, int32_t* component,
+                int32_t* depth, int32_t* seq, int32_t* edge, float* length, cudaStream_t stream) {
+    if (n < 0 || (n > 0 && (rows == nullptr || selected == nullptr))) return 1;
+    if (n == 0) return 0;
+    k_rows_decode<<<unsigned((n + 255) / 256), 256, 0, stream>>>(static_cast<const RowRec*>(rows), selected, n, tx, rx,
+                                                                   component, depth, seq, edge, length);
+    note_launch();
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
 }  // namespace wcb

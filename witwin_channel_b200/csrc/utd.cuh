@@ -305,17 +305,32 @@ WCB_HD EdgeFrame<double> edge_frame(const EdgeDev& ed) {
 template <typename T>
 WCB_HD Cx<T> phasor_kd(double k, double d) { return phasor_neg_kd<T>(k, d); }
 
-// UTD field of one edge: geometry (stationary point, lengths, phase) in G,
-// amplitudes in T.  The face slabs give R_0 and R_n.
+// The frequency-independent part of one (source, receiver, edge) UTD
+// evaluation: the Keller stationary point, lengths, wedge angles, the
+// ray-fixed bases, the transmit polarisation on them and the spreading
+// factor.  A caller evaluating several frequencies forms it once.
 template <typename G, typename T>
-WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> R, V3<T> tx_pol, const Slab<T>& m0,
-                                         const Slab<T>& mn, G frequency, V3<G>* q_out = nullptr) {
-    DiffractionResult<T> out;
-    out.valid = false;
-    const G k = G(kTwoPi) * frequency / G(kC0);
+struct UtdGeometry {
+    bool valid;        // source outside the wedge
+    bool on_face_n;    // receiver inside the wedge, its angle clamped onto face n
+    V3<G> q;           // unclamped stationary point
+    double q_vis[3];   // clamped + biased visibility point
+    G s_p, s;          // incident and diffracted lengths (floored)
+    G t_star;          // stationary parameter along the edge
+    double kappa64;    // FP64 truncation curvature sin_b^2 (1/s' + 1/s) (FP32 end arguments)
+    T phi_p, phi, nn, npi, sin_b, sT, spT, kappa, tsT;
+    V3<T> beta_hat, phi_hat;
+    T e_beta0, e_phi0;  // transmit polarisation on the incident bases (before 1/(2 k s'))
+    T spread;
+};
+
+template <typename G, typename T>
+WCB_HD UtdGeometry<G, T> utd_geometry(const EdgeFrame<G>& ed, V3<G> S, V3<G> R, V3<T> tx_pol) {
+    UtdGeometry<G, T> g;
+    g.valid = false;
+    g.on_face_n = false;
     const V3<G> c = ed.c;
     const V3<G> e = ed.e;
-    const G n = ed.n;
     // Keller stationary point (unfolding)
     const V3<G> ds = S - c;
     const G ts = dot(ds, e);
@@ -327,28 +342,32 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
     const G rr = length(pr);
     const G t_star = value_of(rs + rr) > 0.0 ? ts + (tr - ts) * rs / (rs + rr) : ts;
     const V3<G> q = c + e * t_star;
-    if (q_out) *q_out = q;
+    g.q = q;
+    g.t_star = t_star;
     const G tc = s_min(s_max(t_star, -ed.half_length), ed.half_length);
     const V3<G> qv = c + e * tc + ed.bisector * G(kDiffractionRayBias);
-    out.q[0] = value_of(q.x); out.q[1] = value_of(q.y); out.q[2] = value_of(q.z);
-    out.q_vis[0] = value_of(qv.x); out.q_vis[1] = value_of(qv.y); out.q_vis[2] = value_of(qv.z);
+    g.q_vis[0] = value_of(qv.x); g.q_vis[1] = value_of(qv.y); g.q_vis[2] = value_of(qv.z);
     const V3<G> sp_vec = q - S;
     const V3<G> s_vec = R - q;
     const G s_p = s_max(length(sp_vec), G(kUtdMinDistance));
     const G s = s_max(length(s_vec), G(kUtdMinDistance));
-    out.length = value_of(s_p + s);
+    g.s_p = s_p;
+    g.s = s;
     // angles in the edge frame
     const T phi_p = wedge_angle(cast3<T>(ps), cast3<T>(ed.t0), cast3<T>(ed.n0));
     T phi = wedge_angle(cast3<T>(pr), cast3<T>(ed.t0), cast3<T>(ed.n0));
-    const T nn = T(n);
+    const T nn = T(ed.n);
     const T npi = nn * T(kPi);
-    if (value_of(phi_p) > value_of(npi)) return out;
-    bool on_face_n = false;  // receiver inside the wedge, its angle clamped onto face n
+    g.nn = nn;
+    g.npi = npi;
+    g.phi_p = phi_p;
+    if (value_of(phi_p) > value_of(npi)) return g;
     if (value_of(phi) > value_of(npi)) {
-        on_face_n = value_of(phi - npi) < value_of(T(kTwoPi) - phi);
-        phi = on_face_n ? npi : T(0);
+        g.on_face_n = value_of(phi - npi) < value_of(T(kTwoPi) - phi);
+        phi = g.on_face_n ? npi : T(0);
     }
-    out.valid = true;
+    g.phi = phi;
+    g.valid = true;
     const V3<T> sh_p = cast3<T>(sp_vec * (G(1) / s_p));
     const V3<T> sh = cast3<T>(s_vec * (G(1) / s));
     const V3<T> ef = cast3<T>(e);
@@ -356,14 +375,46 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
     cos_b = s_min(s_max(cos_b, T(-1)), T(1));
     const T sin_b = s_max(s_sqrt(s_max(T(1) - cos_b * cos_b, T(0))), T(1e-6));
     const T sT = T(s), spT = T(s_p);
-    const T kT = T(k);
-    const T kl = kT * sT * spT * sin_b * sin_b / (sT + spT);
-    // finite-edge truncation
+    g.sin_b = sin_b;
+    g.sT = sT;
+    g.spT = spT;
+    // finite-edge truncation curvature
     const T rho_p = spT * sin_b;
     const T rho = sT * sin_b;
-    const T kappa = rho_p * rho_p / (spT * spT * spT) + rho * rho / (sT * sT * sT);
-    const T sigma = s_sqrt(kT * kappa / T(kPi));
-    const T tsT = T(t_star);
+    g.kappa = rho_p * rho_p / (spT * spT * spT) + rho * rho / (sT * sT * sT);
+    g.tsT = T(t_star);
+    g.kappa64 = 0.0;
+    if constexpr (sizeof(T) == 4) {
+        const double cb64 = fmin(fmax(value_of(dot(sp_vec, e)) / value_of(s_p), -1.0), 1.0);
+        const double sb64 = fmax(sqrt(fmax(1.0 - cb64 * cb64, 0.0)), 1e-6);
+        g.kappa64 = sb64 * sb64 / value_of(s_p) + sb64 * sb64 / value_of(s);
+    }
+    // ray-fixed bases
+    V3<T> phi_hat_p = cross(ef, sh_p);
+    phi_hat_p = phi_hat_p * (T(1) / s_max(length(phi_hat_p), T(1e-12)));
+    const V3<T> beta_hat_p = cross(sh_p, phi_hat_p);
+    V3<T> phi_hat = cross(ef, sh);
+    phi_hat = phi_hat * (T(1) / s_max(length(phi_hat), T(1e-12)));
+    g.beta_hat = cross(sh, phi_hat);
+    g.phi_hat = phi_hat;
+    const V3<T> tx_axis = transverse(sh_p, tx_pol);
+    g.e_beta0 = dot(tx_axis, beta_hat_p);
+    g.e_phi0 = dot(tx_axis, phi_hat_p);
+    g.spread = s_sqrt(spT / (sT * (spT + sT)));
+    return g;
+}
+
+// The UTD field of a valid geometry at one frequency: unit-excitation field
+// at the receiver (phase included).  The face slabs give R_0 and R_n.
+template <typename G, typename T>
+WCB_HD C3<T> utd_field_at(const UtdGeometry<G, T>& g, const EdgeFrame<G>& ed, const Slab<T>& m0, const Slab<T>& mn,
+                          G frequency) {
+    const G k = G(kTwoPi) * frequency / G(kC0);
+    const T phi_p = g.phi_p, phi = g.phi, nn = g.nn, npi = g.npi, sin_b = g.sin_b, sT = g.sT, spT = g.spT;
+    const T kT = T(k);
+    const T kl = kT * sT * spT * sin_b * sin_b / (sT + spT);
+    const T sigma = s_sqrt(kT * g.kappa / T(kPi));
+    const T tsT = g.tsT;
     const T tmax = T(ed.half_length), tmin = -T(ed.half_length);
     const T inv_sqrt2 = T(0.70710678118654752440);
     T t_mono;
@@ -372,12 +423,8 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
         // geometry); the end the stationary point lies beyond contributes
         // 1 - |F|/sqrt(2), so a tail factor is a difference of two small
         // numbers instead of a small residue of O(1) ones
-        const double cb64 = fmin(fmax(value_of(dot(sp_vec, e)) / value_of(s_p), -1.0), 1.0);
-        const double sb64 = fmax(sqrt(fmax(1.0 - cb64 * cb64, 0.0)), 1e-6);
-        const double sp64 = value_of(s_p), s64 = value_of(s);
-        const double kappa64 = sb64 * sb64 / sp64 + sb64 * sb64 / s64;
-        const double sigma64 = sqrt(value_of(k) * kappa64 / kPi);
-        const double hl64 = value_of(ed.half_length), ts64 = value_of(t_star);
+        const double sigma64 = sqrt(value_of(k) * g.kappa64 / kPi);
+        const double hl64 = value_of(ed.half_length), ts64 = value_of(g.t_star);
         const double a_hi = sigma64 * (hl64 - ts64), a_lo = sigma64 * (hl64 + ts64);
         T share_hi = T(0), share_lo = T(0);
 #pragma unroll 1
@@ -451,7 +498,7 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
     // cancellation (cot near zero differs between the paired terms in the last
     // bits).  The paired form with 1 + R formed directly has no cancellation.
     bool merge_n = false;
-    if constexpr (sizeof(T) == 4) merge_n = on_face_n && ed.face_n && value_of(phi_p) > 0;
+    if constexpr (sizeof(T) == 4) merge_n = g.on_face_n && ed.face_n && value_of(phi_p) > 0;
     // the four KP terms: (beta-, +), (beta-, -) incident; (beta+, +) weighted by
     // R_n, (beta+, -) weighted by R_0.  One loop body (not four inlined
     // copies) keeps the kernel's instruction footprint small.
@@ -482,23 +529,37 @@ WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> 
     const Cx<T> pre = cx(-inv_sqrt2 * pre_mag, inv_sqrt2 * pre_mag);
     const Cx<T> d_soft = pre * sum_soft;
     const Cx<T> d_hard = pre * sum_hard;
-    // ray-fixed bases
-    V3<T> phi_hat_p = cross(ef, sh_p);
-    phi_hat_p = phi_hat_p * (T(1) / s_max(length(phi_hat_p), T(1e-12)));
-    const V3<T> beta_hat_p = cross(sh_p, phi_hat_p);
-    V3<T> phi_hat = cross(ef, sh);
-    phi_hat = phi_hat * (T(1) / s_max(length(phi_hat), T(1e-12)));
-    const V3<T> beta_hat = cross(sh, phi_hat);
-    const V3<T> tx_axis = transverse(sh_p, tx_pol);
     const T inc_amp = T(1) / (T(2) * kT * spT);
-    const T e_beta = dot(tx_axis, beta_hat_p) * inc_amp;
-    const T e_phi = dot(tx_axis, phi_hat_p) * inc_amp;
-    const T spread = s_sqrt(spT / (sT * (spT + sT)));
-    const Cx<T> ph = phasor_kd<T>(k, s_p + s);
-    const Cx<T> cb = -(d_soft * (e_beta * spread)) * ph;
-    const Cx<T> cf = -(d_hard * (e_phi * spread)) * ph;
-    out.field = c3_axis(beta_hat, cb) + c3_axis(phi_hat, cf);
+    const T e_beta = g.e_beta0 * inc_amp;
+    const T e_phi = g.e_phi0 * inc_amp;
+    const Cx<T> ph = phasor_kd<T>(k, g.s_p + g.s);
+    const Cx<T> cb = -(d_soft * (e_beta * g.spread)) * ph;
+    const Cx<T> cf = -(d_hard * (e_phi * g.spread)) * ph;
+    return c3_axis(g.beta_hat, cb) + c3_axis(g.phi_hat, cf);
+}
+
+// DiffractionResult of a geometry at one frequency (field zero when invalid).
+template <typename G, typename T>
+WCB_HD DiffractionResult<T> utd_result(const UtdGeometry<G, T>& g, const EdgeFrame<G>& ed, const Slab<T>& m0,
+                                       const Slab<T>& mn, G frequency, V3<G>* q_out = nullptr) {
+    DiffractionResult<T> out;
+    out.valid = g.valid;
+    if (q_out) *q_out = g.q;
+    out.q[0] = value_of(g.q.x); out.q[1] = value_of(g.q.y); out.q[2] = value_of(g.q.z);
+    for (int k = 0; k < 3; ++k) out.q_vis[k] = g.q_vis[k];
+    out.length = value_of(g.s_p + g.s);
+    if (g.valid) out.field = utd_field_at(g, ed, m0, mn, frequency);
+    else out.field = C3<T>{cx(T(0), T(0)), cx(T(0), T(0)), cx(T(0), T(0))};
     return out;
+}
+
+// UTD field of one edge: geometry (stationary point, lengths, phase) in G,
+// amplitudes in T.  The face slabs give R_0 and R_n.
+template <typename G, typename T>
+WCB_HD DiffractionResult<T> utd_field_gt(const EdgeFrame<G>& ed, V3<G> S, V3<G> R, V3<T> tx_pol, const Slab<T>& m0,
+                                         const Slab<T>& mn, G frequency, V3<G>* q_out = nullptr) {
+    const UtdGeometry<G, T> g = utd_geometry<G, T>(ed, S, R, tx_pol);
+    return utd_result(g, ed, m0, mn, frequency, q_out);
 }
 
 // The solve's form: FP64 geometry from the precomputed edge record.

@@ -270,20 +270,19 @@ def accumulate_rows(rows: torch.Tensor, selected: torch.Tensor, path_gain: torch
 
 
 def decode_rows(rows: torch.Tensor, selected: torch.Tensor) -> dict:
-    """Integer columns of the selected path records (canonical order)."""
+    """Integer columns of the selected path records (canonical order), in one
+    pass over the records (``wcb_rows_decode``)."""
 
-    r = rows[selected]
-    comp_depth = r[:, 2]
-    component = (comp_depth & 0xFFFF).to(torch.int32)
-    component = torch.where(component >= 0x8000, component - 0x10000, component)
-    depth = ((comp_depth >> 16) & 0xFFFF).to(torch.int32)
-    seq = r[:, 3:8].contiguous()
-    return {
-        "tx_id": r[:, 0].contiguous(),
-        "rx_id": r[:, 1].contiguous(),
-        "component_id": component,
-        "depth": depth,
-        "seq": seq,
-        "edge_id": r[:, 8].contiguous(),
-        "length": r[:, 9].contiguous().view(torch.float32),
-    }
+    device = rows.device
+    K = int(selected.shape[0])
+    out = {name: torch.empty(K, dtype=torch.int32, device=device)
+           for name in ("tx_id", "rx_id", "component_id", "depth", "edge_id")}
+    out["seq"] = torch.empty((K, 5), dtype=torch.int32, device=device)
+    out["length"] = torch.empty(K, dtype=torch.float32, device=device)
+    if K:
+        sel = selected.to(torch.int64).contiguous()
+        _native.check(_native.load().wcb_rows_decode(
+            _native.ptr(rows), _native.ptr(sel), K, _native.ptr(out["tx_id"]), _native.ptr(out["rx_id"]),
+            _native.ptr(out["component_id"]), _native.ptr(out["depth"]), _native.ptr(out["seq"]),
+            _native.ptr(out["edge_id"]), _native.ptr(out["length"]), _native.stream_handle(device)), "wcb_rows_decode")
+    return out
