@@ -205,7 +205,12 @@ def run_leg(args) -> None:
 
     torch.cuda.set_device(0)
     device = torch.device("cuda", 0)
-    leg = _canyon_run(args, device) if args.only_leg == "canyon" else _vjp_run(device)
+    if args.only_leg == "canyon":
+        leg = _canyon_run(args, device)
+    elif args.only_leg == "consumer":
+        leg = _consumer_run(device)
+    else:
+        leg = _vjp_run(device)
     print(json.dumps({"leg": args.only_leg, **leg}), flush=True)
 
 
@@ -650,6 +655,38 @@ def _consumer_run(device, steps: int = 3) -> dict:
 
         ev, ev_ms = timed(lambda: consumer.evaluate(compiled, request))
         table, det_ms = timed(lambda: solve(scene, cfg, reference_frequency_hz=freq).paths)
+        # fixed-topology replay of the LoS + reflection rows: at the discovery
+        # endpoints, over 8 slots of sinks moved 0..0.35 m (one replay for the
+        # block), and over 4 frequency columns; rediscovery beside it
+        lr = frozenset({"los", "reflection"})
+        req_lr = consumer.PropagationRequest(sources=sources, sinks=sinks, reference_frequency_hz=freq,
+                                             components=lr, max_depth=3, response="scalar_transport",
+                                             topology_mode="discover", ad_mode="none")
+        found, rediscover_ms = timed(lambda: consumer.evaluate(compiled, req_lr))
+        prepared = consumer.prepare_fixed_topology(found.paths.topology)
+
+        def replay_request(src, snk, topology, slots=1, offsets=None):
+            return consumer.FixedTopologyRequest(sources=src, sinks=snk, reference_frequency_hz=freq,
+                                                 topology=topology, response="scalar_transport", ad_mode="none",
+                                                 slot_count=slots, frequency_offsets_hz=offsets)
+
+        replay, replay_ms = timed(lambda: consumer.reevaluate(compiled, replay_request(sources, sinks, prepared)))
+        T = 8
+        shift = torch.linspace(0.0, 0.35, T, device=device).view(T, 1, 1) * torch.tensor([1.0, 0.6, 0.0],
+                                                                                        device=device)
+        stacked_sinks = consumer.EndpointBatch(
+            stable_ids=sinks.stable_ids.repeat(T), positions_m=(pts.unsqueeze(0) + shift).reshape(-1, 3).contiguous(),
+            polarizations=sinks.polarizations.repeat(T, 1).contiguous())
+        stacked_sources = consumer.EndpointBatch(
+            stable_ids=sources.stable_ids.repeat(T), positions_m=sources.positions_m.repeat(T, 1).contiguous(),
+            polarizations=sources.polarizations.repeat(T, 1).contiguous(), powers_w=sources.powers_w.repeat(T))
+        replicated = consumer.replicate_over_slots(prepared, T, source_count=1, sink_count=R)
+        slotted, slots_ms = timed(lambda: consumer.reevaluate(
+            compiled, replay_request(stacked_sources, stacked_sinks, replicated, slots=T)))
+        offsets = (0.0, 1.0e8, 2.0e8, 3.0e8)
+        _wide, wide_ms = timed(lambda: consumer.reevaluate(
+            compiled, replay_request(sources, sinks, prepared, offsets=offsets)))
+        K = prepared.row_count
         return {
             "workload": "urban canyon as explicit batches: 1 source x 65,536 sinks, LoS + reflection depth 3 + UTD, "
                         "scalar transport",
@@ -658,6 +695,20 @@ def _consumer_run(device, steps: int = 3) -> dict:
             "paths": ev.paths.path_count,
             "candidates": ev.diagnostics.candidate_count,
             "same_row_count_as_table": ev.paths.path_count == int(table.tx_id.shape[0]),
+            "replay": {
+                "workload": "the LoS + reflection (depth 3) rows of the canyon request, frozen and replayed",
+                "rows": K,
+                "rediscover_ms": rediscover_ms,
+                "replay_ms": replay_ms,
+                "replay_rows_per_s": K / (replay_ms * 1e-3),
+                "replay_all_valid": bool(replay.row_valid.all()),
+                "slots": T,
+                "slot_block_ms": slots_ms,
+                "slot_rows_per_s": T * K / (slots_ms * 1e-3),
+                "slot_valid_fraction": float(slotted.row_valid.float().mean()),
+                "wideband_columns": len(offsets) + 1,
+                "wideband_ms": wide_ms,
+            },
         }
     except Exception as exc:  # reported in the leg; the headline line stands
         return {"error": f"{type(exc).__name__}: {exc}"}
@@ -1021,7 +1072,7 @@ def main() -> None:
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-consumer", action="store_true")
     ap.add_argument("--no-canyon", action="store_true")
-    ap.add_argument("--only-leg", choices=["canyon", "vjp"], default=None,
+    ap.add_argument("--only-leg", choices=["canyon", "vjp", "consumer"], default=None,
                     help="run one side leg alone (profiling runs); no headline line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "native":

@@ -413,6 +413,87 @@ int wcb_los_jones(const int64_t* pair_index, int64_t num_rows, const float* sour
                   const float* sink_reference_basis, double frequency_hz, float* matrix, float* source_basis,
                   float* sink_basis, int32_t* status, void* stream);
 
+/* Fixed-topology replay of frozen line-of-sight and reflection records at new
+ * endpoint positions (replaces reevaluate and its bucket replay,
+ * witwin/channel/propagation/consumer.py:3846-4110, with prepared_row_gather
+ * :2375-2449, _los_inputs / _reflection_inputs :2734-2811, evaluate_prepared
+ * :3029-3096 and the direct-plane EPC re-solve propagation/geometry.py:214-264).
+ * One launch replays every record and every frequency column, plus one launch
+ * for the pair segmentation; no host synchronisation.
+ *
+ * Records (wcb_frozen_rows, all device, K rows): component_id 0 (LoS, depth 0)
+ * or 1 (reflection, depth 1..width); primitive_sequence (K,width) the faces of
+ * the bounces; source_index / sink_index into the endpoint batches;
+ * source_id / sink_id the stable ids the records were discovered with (NULL:
+ * no identity check); order (NULL: row order) a permutation of the rows that
+ * sets the execution order only.
+ * Endpoints (wcb_endpoint_batch, device): positions (N,3), polarizations (N,3),
+ * stable_ids (N) i64, powers (N) (sources), polarization_basis (N,2,3) (only
+ * read when out->jones is set).
+ * slot_count >= 1: pair p of row i is sink*num_sources+source for one slot and
+ * the block-diagonal layout slot*ss*ks + (sink-slot*ks)*ss + (source-slot*ss)
+ * otherwise (ss, ks the per-slot counts; the slot is the source's).
+ * materials: num_columns frequency columns (column c at frequencies[c],
+ * a device FP64 array), as wcb_materials with NF = num_columns.
+ * test_visibility: re-test each LoS record's segment and each reflection
+ * record's plane crossings, containment in its faces' coplanar groups and
+ * legs against the scene, as discovery does (FP32 segment tests); a record
+ * that fails is published with row_valid 0 and zero field, length, delay and
+ * direction.  With 0 every record is evaluated as valid.
+ *
+ * status (device int32[2], caller-zeroed): status[0] the contract bits of the
+ * reference's validation mask, 1 a source or sink index outside its batch, 2
+ * in-bounds rows not in non-decreasing pair order, 16 a stable id that differs
+ * from the batch's, 32 a slot-batched row whose sink lies outside its
+ * source's slot; status[1] engine bits, 1 traversal stack overflow, 2 a
+ * record whose component or depth this replay does not take, 4 a face id
+ * outside the scene.  A row with any bit is written as invalid zeros.
+ * Any output pointer may be NULL. */
+typedef struct {
+    int64_t num_rows;
+    int32_t width;
+    const int32_t* component_id;
+    const int32_t* depth;
+    const int32_t* primitive_sequence;
+    const int32_t* source_index;
+    const int32_t* sink_index;
+    const int64_t* source_id;
+    const int64_t* sink_id;
+    const int32_t* order;
+} wcb_frozen_rows;
+
+typedef struct {
+    int64_t count;
+    const float* positions;
+    const float* polarizations;
+    const int64_t* stable_ids;
+    const float* powers;
+    const float* polarization_basis;
+} wcb_endpoint_batch;
+
+typedef struct {
+    float* coefficient;          /* (K) complex64, column 0: receiver-projected, sqrt(power) */
+    float* coefficient_offsets;  /* (K,C-1) complex64, columns 1.. */
+    float* field;                /* (K,3) complex64, column 0: world-Cartesian, sqrt(power) */
+    float* field_offsets;        /* (K,C-1,3) complex64 */
+    float* path_length_m;        /* (K) */
+    float* delay_s;              /* (K) */
+    float* direction;            /* (K,3) arrival direction */
+    float* interaction_positions; /* (K,width,3) */
+    float* interaction_normals;  /* (K,width,3) */
+    uint8_t* row_valid;          /* (K) */
+    float* jones;                /* (K,2,2) complex64, column 0, unit excitation */
+    float* source_basis;         /* (K,2,3) */
+    float* sink_basis;           /* (K,2,3) */
+    int64_t* pair_index;         /* (K) */
+    int64_t* pair_offsets;       /* (P+1), P = slot_count * per-slot sources * per-slot sinks */
+} wcb_replay_outputs;
+
+int wcb_rows_replay(const wcb_scene* scene, const wcb_frozen_rows* rows, const wcb_endpoint_batch* sources,
+                    const wcb_endpoint_batch* sinks, int64_t slot_count, const wcb_materials* materials,
+                    const double* frequencies, int32_t num_columns, int32_t test_visibility,
+                    const wcb_replay_outputs* out, int32_t* status, void* stream);
+
 /* Measurement: when enabled, wcb_solve brackets its candidate preparation and
  * its main kernel with CUDA events on the solve stream and counts the rays
  * (segment visibility / penetration queries) the main kernel traces.

@@ -37,18 +37,29 @@ def test_capability_record_is_frozen_and_truthful():
     assert caps.contract_version == c.CONTRACT_VERSION == 6
     assert caps.components == c.COMPONENTS == frozenset({"los", "reflection", "transmission", "diffraction"})
     assert caps.responses == c.RESPONSES
-    assert caps.ad_modes == frozenset({"none"})
+    assert caps.ad_modes == c.AD_MODES == frozenset({"none", "jvp", "vjp"})
     for response in caps.responses:
         want = frozenset({"los"}) if response == "polarimetric_transport" else c.COMPONENTS
         assert caps.components_for(response) == want
-        assert caps.ad_modes_for(response) == frozenset({"none"})
+        want_ad = c.AD_MODES if response == "scalar_transport" else frozenset({"none"})
+        assert caps.ad_modes_for(response) == want_ad
     assert caps.supports_los_jones
     for component in c.COMPONENTS:
-        assert caps.ad_modes_for_component(component) == frozenset({"none"})
+        assert caps.ad_modes_for_component(component) == c.AD_MODES
+    for name in ("materials.gain", "materials.mu_r", "materials.thickness_m", "sources.powers_w"):
+        assert name in caps.primal_only_ad_inputs
+    assert not caps.supports_higher_order_ad
     assert caps.material_leaves_for("los") == ()
     assert "layer_eps_r" in caps.material_leaves_for("transmission")
     assert caps.differentiable_geometry_for("discovery") == frozenset()
-    assert not caps.supports_fixed_topology and not caps.supports_wideband_offsets
+    assert caps.differentiable_geometry_for("fixed_topology") == frozenset()
+    assert caps.supports_fixed_topology and caps.supports_wideband_offsets and caps.supports_slot_batching
+    assert caps.fixed_topology_components == frozenset({"los", "reflection"})
+    assert caps.fixed_topology_row_validity_components == frozenset({"los", "reflection"})
+    assert caps.fixed_topology_responses == c.RESPONSES
+    assert caps.wideband_responses == frozenset({"scalar_transport", "complex3_transport"})
+    assert caps.world_motions == frozenset({"frozen_world", "fixed_winner_replay"})
+    assert caps.max_slot_count is None and caps.max_frequency_offset_count is None
     with pytest.raises(Exception):
         caps.contract_version = 7  # frozen
 
@@ -120,9 +131,19 @@ def test_row_records_validate_shapes_and_dtypes():
         c.PropagationGeometry(path_length_m=torch.zeros(K), delay_s=torch.zeros(K), field_direction=torch.zeros((K, 3)),
                               interaction_positions_m=torch.zeros((K, W, 2)), interaction_normals=torch.zeros((K, W, 2)))
     scalar = c.ScalarTransport(coefficient=torch.zeros(K, dtype=torch.complex64))
-    with pytest.raises(NotImplementedError):
+    wide = c.ScalarTransport(coefficient=torch.zeros(K, dtype=torch.complex64),
+                             coefficient_offsets=torch.zeros((K, 2), dtype=torch.complex64),
+                             frequency_offsets_hz=(0.0, 1.0e6))
+    assert wide.coefficient_offsets.shape == (K, 2)
+    with pytest.raises(ValueError, match="paired"):
         c.ScalarTransport(coefficient=torch.zeros(K, dtype=torch.complex64),
-                          coefficient_offsets=torch.zeros((K, 1), dtype=torch.complex64), frequency_offsets_hz=(0.0,))
+                          coefficient_offsets=torch.zeros((K, 1), dtype=torch.complex64))
+    with pytest.raises(ValueError, match="shape"):
+        c.ScalarTransport(coefficient=torch.zeros(K, dtype=torch.complex64),
+                          coefficient_offsets=torch.zeros((K, 1), dtype=torch.complex64), frequency_offsets_hz=(0.0, 1.0))
+    with pytest.raises(ValueError, match="shape"):
+        c.Complex3Transport(field=torch.zeros((K, 3), dtype=torch.complex64), direction=torch.zeros((K, 3)),
+                            field_offsets=torch.zeros((K, 3), dtype=torch.complex64), frequency_offsets_hz=(5.0,))
     c3 = c.Complex3Transport(field=torch.zeros((K, 3), dtype=torch.complex64), direction=torch.zeros((K, 3)))
     assert c3.row_count == K
     with pytest.raises(ValueError):
@@ -166,3 +187,123 @@ def test_los_jones_input_checks_before_any_launch():
         c.consumer_los_jones(**{**kw, "pair_index": pair.int()})
     with pytest.raises(ValueError, match="CUDA"):
         c.consumer_los_jones(**kw)
+
+
+# --- fixed-topology replay: host logic (reference consumer.py:94-135, 466-512,
+# 1228-1650; tests after tests/propagation/test_fixed_topology*.py) ---------
+
+
+def test_frequency_offset_grid_checks():
+    assert c.require_frequency_offsets(None) is None
+    assert c.require_frequency_offsets((0.0, 1e6, -2e6)) == (0.0, 1e6, -2e6)
+    assert c.require_frequency_offsets((1, 2)) == (1.0, 2.0)
+    with pytest.raises(TypeError):
+        c.require_frequency_offsets(torch.tensor([0.0]))
+    with pytest.raises(TypeError):
+        c.require_frequency_offsets([0.0])
+    with pytest.raises(ValueError):
+        c.require_frequency_offsets(())
+    with pytest.raises(TypeError):
+        c.require_frequency_offsets((True,))
+    with pytest.raises(ValueError):
+        c.require_frequency_offsets((float("nan"),))
+    with pytest.raises(ValueError, match="repeat"):
+        c.require_frequency_offsets((1.0, 1.0))
+    with pytest.raises(ValueError, match="resolution"):
+        c._require_resolvable_offsets((math.ulp(28e9) / 4,), 28e9)
+    with pytest.raises(ValueError, match="closer"):
+        c._require_resolvable_offsets((1.0e6, 1.0e6 + math.ulp(28e9) / 2), 28e9)
+    with pytest.raises(ValueError, match="non-positive"):
+        c._require_resolvable_offsets((-30e9,), 28e9)
+    c._require_resolvable_offsets((0.0, 1.0e6), 28e9)
+
+
+def test_world_provenance_names_the_first_moved_domain():
+    a = c.WorldProvenance(topology_version=1, geometry_version=2, material_version=3, assignment_version=4)
+    assert a.moved_domain(c.WorldProvenance(1, 2, 3, 4)) is None
+    assert a.moved_domain(c.WorldProvenance(1, 9, 3, 4)) == "geometry_version"
+    assert a.moved_domain(c.WorldProvenance(1, 9, 3, 4), allow_geometry=True) is None
+    assert a.moved_domain(c.WorldProvenance(1, 9, 8, 4), allow_geometry=True) == "material_version"
+    assert a.moved_domain(c.WorldProvenance(7, 9, 8, 0)) == "topology_version"
+
+    class Compiled:
+        topology_version, geometry_version, material_version, assignment_version = 5, 6, 7, 8
+
+    assert c.WorldProvenance.of(Compiled()).moved_domain(c.WorldProvenance(5, 6, 7, 8)) is None
+
+
+def _frozen(component, depth, seq, source=None, sink=None) -> c.PropagationTopology:
+    K = len(component)
+    seq_t = torch.as_tensor(seq, dtype=torch.int32).reshape(K, -1 if K else 2)
+    W = int(seq_t.shape[1])
+    src = torch.tensor(source if source is not None else [0] * K, dtype=torch.int32)
+    snk = torch.tensor(sink if sink is not None else list(range(K)), dtype=torch.int32)
+    return c.PropagationTopology(**_topology(
+        K, W, component_id=torch.tensor(component, dtype=torch.int32), depth=torch.tensor(depth, dtype=torch.int32),
+        primitive_sequence=seq_t, source_index=src, sink_index=snk, source_id=src.long() + 100,
+        sink_id=snk.long() + 200))
+
+
+def test_prepare_partitions_by_component_and_depth():
+    topo = _frozen([1, 0, 1, 1, 0], [2, 0, 1, 2, 0], [[3, 4], [-1, -1], [5, -1], [6, 7], [-1, -1]])
+    prepared = c.prepare_fixed_topology(topo)
+    got = [(b.component, b.depth, b.rows.tolist()) for b in prepared.buckets]
+    assert got == [("los", 0, [1, 4]), ("reflection", 1, [2]), ("reflection", 2, [0, 3])]
+    assert prepared.execution_order.tolist() == [1, 4, 2, 0, 3]
+    assert prepared.execution_order.dtype == torch.int32
+    assert (prepared.prepare_d2h_copies, prepared.prepare_synchronizations) == (5, 5)
+    assert prepared.row_count == 5 and prepared.provenance is None
+    empty = c.prepare_fixed_topology(_frozen([], [], torch.zeros((0, 2))))
+    assert empty.buckets == () and empty.prepare_d2h_copies == 0
+
+
+@pytest.mark.parametrize("component, depth, seq, error", [
+    ([1], [2], [[3, -1]], ValueError),        # active slot holds -1
+    ([1], [1], [[3, 4]], ValueError),         # unused slot not -1
+    ([1], [3], [[3, 4]], ValueError),         # depth beyond the sequence width
+    ([0], [1], [[3, -1]], ValueError),        # a los row with an interaction
+    ([1], [0], [[-1, -1]], ValueError),       # a reflection row without one
+    ([2], [1], [[3, -1]], NotImplementedError),  # diffraction is not freezable
+    ([5], [1], [[3, -1]], NotImplementedError),  # nor transmission
+])
+def test_prepare_refuses_malformed_or_unfreezable_rows(component, depth, seq, error):
+    with pytest.raises(error):
+        c.prepare_fixed_topology(_frozen(component, depth, seq))
+    with pytest.raises(TypeError):
+        c.prepare_fixed_topology("rows")
+
+
+def test_replicate_over_slots_is_index_arithmetic():
+    topo = _frozen([1, 0, 1], [1, 0, 1], [[3], [-1], [5]], source=[0, 1, 0], sink=[0, 0, 1])
+    prepared = c.prepare_fixed_topology(topo)
+    assert c.replicate_over_slots(prepared, 1, source_count=2, sink_count=2) is prepared
+    rep = c.replicate_over_slots(prepared, 3, source_count=2, sink_count=2)
+    t = rep.topology
+    assert t.row_count == 9
+    assert t.source_index.tolist() == [0, 1, 0, 2, 3, 2, 4, 5, 4]
+    assert t.sink_index.tolist() == [0, 0, 1, 2, 2, 3, 4, 4, 5]
+    assert t.source_id.tolist() == [100, 101, 100] * 3
+    assert t.primitive_sequence.reshape(-1).tolist() == [3, -1, 5] * 3
+    assert [(b.component, b.rows.tolist()) for b in rep.buckets] == [("los", [1, 4, 7]),
+                                                                     ("reflection", [0, 2, 3, 5, 6, 8])]
+    assert rep.execution_order.tolist() == [1, 4, 7, 0, 2, 3, 5, 6, 8]
+    assert rep.prepare_d2h_copies == prepared.prepare_d2h_copies
+    with pytest.raises(ValueError):
+        c.replicate_over_slots(prepared, 0, source_count=2, sink_count=2)
+    with pytest.raises(ValueError):
+        c.replicate_over_slots(prepared, 2, source_count=0, sink_count=2)
+    with pytest.raises(TypeError):
+        c.replicate_over_slots(topo, 2, source_count=2, sink_count=2)
+
+
+def test_time_varying_request_checks():
+    topo = c.prepare_fixed_topology(_frozen([0], [0], [[-1]]))
+    kw = dict(sources=None, sinks=None, reference_frequency_hz=1e9, topology=topo, response="scalar_transport",
+              ad_mode="none")
+    with pytest.raises(TypeError, match="float64"):
+        c.TimeVaryingRequest(**{**kw, "times_s": torch.zeros(2)})
+    with pytest.raises(ValueError):
+        c.TimeVaryingRequest(**{**kw, "times_s": torch.zeros(0, dtype=torch.float64)})
+    with pytest.raises(TypeError, match="PreparedFixedTopology"):
+        c.TimeVaryingRequest(**{**kw, "topology": topo.topology, "times_s": torch.zeros(2, dtype=torch.float64)})
+    assert c.TimeVaryingRequest(**{**kw, "times_s": torch.zeros(4, dtype=torch.float64)}).slot_count == 4

@@ -127,6 +127,52 @@ class AccumulateOutputs(ctypes.Structure):
     ]
 
 
+class FrozenRows(ctypes.Structure):
+    _fields_ = [
+        ("num_rows", ctypes.c_int64),
+        ("width", ctypes.c_int32),
+        ("component_id", _vp),
+        ("depth", _vp),
+        ("primitive_sequence", _vp),
+        ("source_index", _vp),
+        ("sink_index", _vp),
+        ("source_id", _vp),
+        ("sink_id", _vp),
+        ("order", _vp),
+    ]
+
+
+class EndpointBatch(ctypes.Structure):
+    _fields_ = [
+        ("count", ctypes.c_int64),
+        ("positions", _vp),
+        ("polarizations", _vp),
+        ("stable_ids", _vp),
+        ("powers", _vp),
+        ("polarization_basis", _vp),
+    ]
+
+
+class ReplayOutputs(ctypes.Structure):
+    _fields_ = [
+        ("coefficient", _vp),
+        ("coefficient_offsets", _vp),
+        ("field", _vp),
+        ("field_offsets", _vp),
+        ("path_length_m", _vp),
+        ("delay_s", _vp),
+        ("direction", _vp),
+        ("interaction_positions", _vp),
+        ("interaction_normals", _vp),
+        ("row_valid", _vp),
+        ("jones", _vp),
+        ("source_basis", _vp),
+        ("sink_basis", _vp),
+        ("pair_index", _vp),
+        ("pair_offsets", _vp),
+    ]
+
+
 ROW_BYTES = 48
 # wcb_row as int32 words: tx, rx, (component | depth << 16), seq[5], edge, length(f32 bits), reserved[2]
 ROW_WORDS = 12
@@ -164,6 +210,7 @@ EXPORTED_SYMBOLS = (
     "wcb_field_transmission_sequence",
     "wcb_field_project_complex3",
     "wcb_los_jones",
+    "wcb_rows_replay",
     "wcb_profile_enable",
     "wcb_profile_read",
     "wcb_build_info",
@@ -244,6 +291,9 @@ def load() -> ctypes.CDLL:
     lib.wcb_field_project_complex3.argtypes = [ctypes.c_int64] + [_vp] * 5 + [_vp]
     lib.wcb_los_jones.argtypes = [_vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp, ctypes.c_int64, _vp, _vp,
                                   ctypes.c_double, _vp, _vp, _vp, _vp, _vp]
+    lib.wcb_rows_replay.argtypes = [_vp, ctypes.POINTER(FrozenRows), ctypes.POINTER(EndpointBatch),
+                                    ctypes.POINTER(EndpointBatch), ctypes.c_int64, ctypes.POINTER(Materials), _vp,
+                                    ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ReplayOutputs), _vp, _vp]
     lib.wcb_profile_enable.argtypes = [ctypes.c_int32]
     lib.wcb_profile_read.argtypes = [ctypes.POINTER(ctypes.c_double)]
     lib.wcb_build_info.argtypes = [ctypes.c_char_p, ctypes.c_int64]

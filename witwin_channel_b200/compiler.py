@@ -12,6 +12,8 @@ frequencies and material changes.
 
 from __future__ import annotations
 
+import hashlib
+import itertools
 import weakref
 from dataclasses import dataclass, field
 from typing import Any
@@ -146,6 +148,21 @@ class CompiledScene:
     num_vertices: int
     structure_vertex_offsets: list = field(default_factory=list)
     row_count_hint: int = 0  # path records of the last row-mode solve (sizes the next record buffer)
+    # World version domains (the reference's witwin.core versions that a
+    # frozen topology is checked against).  topology_version hashes the face
+    # tables and structure layout, assignment_version the face -> material /
+    # surface assignment; geometry_version is an epoch drawn from a process
+    # counter at every compile and every in-place refit, so a geometry that
+    # moved and moved back still reads as moved.  material_version is
+    # recomputed from the live material objects at each read.
+    topology_version: int = 0
+    assignment_version: int = 0
+    geometry_version: int = 0
+    source_token: tuple = ()
+
+    @property
+    def material_version(self) -> int:
+        return material_version(self.materials)
 
     # ---- material tables ------------------------------------------------
     def material_values(self, frequency: float, *, keep_graph: bool = False) -> dict[str, list]:
@@ -215,6 +232,40 @@ class CompiledScene:
         )
 
 
+_GEOMETRY_EPOCH = itertools.count(1)
+
+
+def _digest(*parts: bytes) -> int:
+    h = hashlib.blake2b(digest_size=8)
+    for part in parts:
+        h.update(part)
+    return int.from_bytes(h.digest(), "little", signed=True)
+
+
+def _value_token(value: Any) -> str:
+    """Content of a plain number, identity and in-place version of a tensor,
+    identity of anything else (a dispersion law, a callable)."""
+    if isinstance(value, torch.Tensor):
+        return f"t{id(value)}:{value._version}"
+    if isinstance(value, (bool, int, float, str)) or value is None:
+        return repr(value)
+    return f"o{id(value)}"
+
+
+def material_version(materials: list) -> int:
+    """Digest of every material value a solve reads (layer stacks, gain,
+    conductor and geometry modes)."""
+    parts = []
+    for mat in materials:
+        layers = [
+            "|".join(_value_token(getattr(layer, name, None)) for name in ("thickness_m", "eps_r", "sigma_e", "mu_r"))
+            for layer in mat.stack()
+        ]
+        parts.append(";".join(layers) + "#" + _value_token(getattr(mat, "gain", None)) + "#"
+                     + repr(getattr(mat, "conductor_model", None)) + "#" + repr(getattr(mat, "geometry_mode", None)))
+    return _digest("\n".join(parts).encode())
+
+
 def to_device(values: list, dtype: torch.dtype, device: torch.device) -> torch.Tensor:
     """One host-to-device copy of a flat list (through pinned memory, not
     waited for on the host)."""
@@ -274,6 +325,8 @@ def compile_scene(scene: Any, device: torch.device | None = None) -> CompiledSce
             V = torch.cat([st.vertices.detach().to(device=device, dtype=torch.float32).reshape(-1, 3)
                            for st in scene.structures]) if scene.structures else None
             if V is not None and cached[2].native.refit(V):
+                cached[2].geometry_version = next(_GEOMETRY_EPOCH)
+                cached[2].source_token = token
                 _CACHE[scene_key] = (cached[0], token, cached[2], refs)
                 return cached[2]
     verts, faces, fsurf, fstruct, fmat = [], [], [], [], []
@@ -300,18 +353,26 @@ def compile_scene(scene: Any, device: torch.device | None = None) -> CompiledSce
         fmat.append(torch.full((nf,), mat_index[key], dtype=torch.int32))
         offset += v.shape[0]
     if verts:
+        faces_host = torch.cat(faces).to(torch.int32)
+        topology_version = _digest(faces_host.numpy().tobytes(), torch.cat(fstruct).numpy().tobytes(),
+                                   repr(token[-1]).encode())
+        assignment_version = _digest(torch.cat(fmat).numpy().tobytes(), torch.cat(fsurf).numpy().tobytes())
         V = torch.cat(verts).to(device)
-        Fc = torch.cat(faces).to(torch.int32).to(device)
+        Fc = faces_host.to(device)
         fs = torch.cat(fsurf).to(device)
         fst = torch.cat(fstruct).to(device)
         fm = torch.cat(fmat).to(device)
     else:
+        topology_version = _digest(b"empty", repr(token[-1]).encode())
+        assignment_version = _digest(b"empty")
         V = torch.zeros((0, 3), dtype=torch.float32, device=device)
         Fc = torch.zeros((0, 3), dtype=torch.int32, device=device)
         fs = fst = fm = torch.zeros((0,), dtype=torch.int32, device=device)
     native = NativeScene(V, Fc, fs, fst, fm, _edge_policy(scene))
     compiled = CompiledScene(scene=scene, native=native, materials=materials, face_material=fm,
-                             num_vertices=int(V.shape[0]), structure_vertex_offsets=offsets)
+                             num_vertices=int(V.shape[0]), structure_vertex_offsets=offsets,
+                             topology_version=topology_version, assignment_version=assignment_version,
+                             geometry_version=next(_GEOMETRY_EPOCH), source_token=token)
     try:
         ref = weakref.ref(scene, lambda _r, k=scene_key: _CACHE.pop(k, None))
     except TypeError:  # not weak-referenceable: compile on every call

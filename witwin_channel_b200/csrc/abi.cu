@@ -160,6 +160,40 @@ int wcb_field_free_space(int64_t n, const float* source, const float* target, co
                                  path_field, path_gain, path_length, delay, direction, as_stream(stream));
 }
 
+int wcb_rows_replay(const wcb_scene* scene, const wcb_frozen_rows* rows, const wcb_endpoint_batch* sources,
+                    const wcb_endpoint_batch* sinks, int64_t slot_count, const wcb_materials* materials,
+                    const double* frequencies, int32_t num_columns, int32_t test_visibility,
+                    const wcb_replay_outputs* out, int32_t* status, void* stream) {
+    if (scene == nullptr || rows == nullptr || sources == nullptr || sinks == nullptr || materials == nullptr ||
+        out == nullptr || status == nullptr)
+        return WCB_ERR_INVALID_ARGUMENT;
+    if (rows->num_rows < 0 || rows->width < 0 || rows->width > 5 || slot_count < 1 || num_columns < 1 ||
+        sources->count < 0 || sinks->count < 0 || sources->count % slot_count != 0 || sinks->count % slot_count != 0)
+        return WCB_ERR_INVALID_ARGUMENT;
+    if (sources->count > 0 && sinks->count > INT64_MAX / sources->count) return WCB_ERR_INVALID_ARGUMENT;
+    if (rows->num_rows > 0) {
+        if (rows->component_id == nullptr || rows->depth == nullptr || rows->source_index == nullptr ||
+            rows->sink_index == nullptr || (rows->width > 0 && rows->primitive_sequence == nullptr) ||
+            sources->count == 0 || sinks->count == 0 || sources->positions == nullptr ||
+            sources->polarizations == nullptr || sinks->positions == nullptr || sinks->polarizations == nullptr ||
+            frequencies == nullptr)
+            return WCB_ERR_INVALID_ARGUMENT;
+        if ((rows->source_id != nullptr && sources->stable_ids == nullptr) ||
+            (rows->sink_id != nullptr && sinks->stable_ids == nullptr))
+            return WCB_ERR_INVALID_ARGUMENT;
+        if (out->jones != nullptr && (sources->polarization_basis == nullptr || sinks->polarization_basis == nullptr))
+            return WCB_ERR_INVALID_ARGUMENT;
+        if (materials->num_materials > 0 && (materials->eps_r == nullptr || materials->sigma_e == nullptr ||
+                                              materials->mu_r == nullptr || materials->gain == nullptr ||
+                                              materials->thickness == nullptr))
+            return WCB_ERR_INVALID_ARGUMENT;
+    }
+    if (out->pair_offsets != nullptr && rows->num_rows > 0 && out->pair_index == nullptr)
+        return WCB_ERR_INVALID_ARGUMENT;
+    return wcb::rows_replay(scene->h, rows, sources, sinks, slot_count, materials, frequencies, num_columns,
+                            test_visibility, out, status, as_stream(stream));
+}
+
 int wcb_los_jones(const int64_t* pair_index, int64_t num_rows, const float* source_positions, int64_t num_sources,
                   const float* sink_positions, int64_t num_sinks, const float* source_reference_basis,
                   const float* sink_reference_basis, double frequency_hz, float* matrix, float* source_basis,

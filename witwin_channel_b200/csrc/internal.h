@@ -59,6 +59,9 @@ int rows_accumulate(const void* rows, const int64_t* selected, int64_t n, const 
                     const wcb_outputs* out, cudaStream_t stream);
 int field_free_space(int64_t n, const float* s, const float* t, const float* pw, const float* tp, const float* rp, double f,
                      float* fv, float* c, float* pf, float* pg, float* pl, float* dl, float* dr, cudaStream_t stream);
+int rows_replay(const SceneHandle* h, const wcb_frozen_rows* rows, const wcb_endpoint_batch* src,
+                const wcb_endpoint_batch* snk, int64_t slot_count, const wcb_materials* m, const double* freqs,
+                int num_columns, int visibility, const wcb_replay_outputs* out, int* status, cudaStream_t stream);
 int los_jones(int64_t n, const int64_t* pair, const float* src, int64_t num_src, const float* snk, int64_t num_snk,
               const float* src_ref, const float* snk_ref, double f, float* matrix, float* src_basis, float* snk_basis,
               int* status, cudaStream_t stream);

@@ -20,6 +20,7 @@
 #include "em.cuh"
 #include "internal.h"
 #include "paths.cuh"
+#include "row_eval.cuh"
 #include "solve.h"
 #include "utd.cuh"
 
@@ -415,39 +416,12 @@ __global__ void k_eval_rows(EvalParams p) {
         path_gain = cabs2(path_field);
     } else if (row.component == 1) {
         const int d = row.depth;
-        double planes[4 * kMaxDepth], images[3 * kMaxDepth];
-        V3<double> pp = S;
-        for (int k = 0; k < d; ++k) {
-            const int g = sc.face_group[row.seq[k]];
-            const double* pl = sc.group_plane + 4 * g;
-            for (int q = 0; q < 4; ++q) planes[4 * k + q] = pl[q];
-            const V3<double> n = v3(pl[0], pl[1], pl[2]);
-            pp = pp - n * (2.0 * (dot(pp, n) - pl[3]));
-            images[3 * k] = pp.x; images[3 * k + 1] = pp.y; images[3 * k + 2] = pp.z;
-        }
-        if (!back_project(R, planes, images, d, hits)) {
-            for (int k = 0; k < d; ++k) hits[k] = v3(nan(""), nan(""), nan(""));
-        }
+        const ReflectionGeom g = reflection_geometry(sc, row.seq, d, S, R);
+        for (int k = 0; k < d; ++k) hits[k] = g.hits[k];
         nh = d;
-        length = wcb::length(R - pp);
-        const float wl = float(kC0 / p.freq);
-        V3<float> prev = Sf;
-        V3<float> incident = safe_normalize(cast3<float>(hits[0]) - prev, v3(0.f, 0.f, 1.f));
-        C3<float> value = c3_from_real(transverse(incident, tx_pol));
-        V3<float> outgoing = incident;
-        for (int k = 0; k < d; ++k) {
-            const V3<float> hit = cast3<float>(hits[k]);
-            incident = safe_normalize(hit - prev, outgoing);
-            const float* nf = sc.face_normal + 3 * row.seq[k];
-            normals[k] = v3(nf[0], nf[1], nf[2]);
-            reflect_bounce(value, outgoing, incident, normals[k], slab_of(p, row.seq[k]), p.freq, wl);
-            prev = hit;
-        }
-        dir = safe_normalize(Rf - prev, outgoing);
-        const float amp = 1.0f / (2.0f * float(p.k) * float(fmax(length, kUtdEps)));
-        value = c3_scale(value, phasor_neg_kd<float>(p.k, length) * amp);
-        unit_field = value;
-        coef = project_receiver(value, dir, rx_pol);
+        length = g.length;
+        reflection_field(sc, row.seq, d, g, Sf, Rf, tx_pol, rx_pol, [&](int f) { return slab_of(p, f); }, p.freq, p.k,
+                         normals, &unit_field, &coef, &dir);
         path_field = coef * sq;
         path_gain = cabs2(path_field);
     } else if (row.component == 5) {
@@ -702,21 +676,6 @@ __global__ void k_field_project(long long n, const float* fv, const float* dir, 
     const Cx<float> c = project_receiver(v, v3(dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]), v3(rpol[3 * i], rpol[3 * i + 1], rpol[3 * i + 2]));
     store_c(coef, i, c);
     if (pg) pg[i] = cabs2(c);
-}
-
-// Transverse frame of one endpoint for the propagation direction `dir`
-// (consumer_los_jones, los.cu:1964-1980): u is the first reference vector made
-// transverse and unit (falling back to the transverse part of the second, then
-// to a fixed axis); v = dir x u, turned to the side of the second vector.
-WCB_D void endpoint_frame(const float* ref, long long e, V3<float> dir, V3<float>* u, V3<float>* v) {
-    const V3<float> first = v3(ref[6 * e], ref[6 * e + 1], ref[6 * e + 2]);
-    const V3<float> second = v3(ref[6 * e + 3], ref[6 * e + 4], ref[6 * e + 5]);
-    const V3<float> fallback = stable_perp_basis(dir, second);
-    const V3<float> fu = safe_normalize(transverse(dir, first), fallback);
-    V3<float> fv = safe_normalize(cross(dir, fu), fallback);
-    if (dot(fv, second) < 0.f) fv = fv * -1.f;
-    *u = fu;
-    *v = fv;
 }
 
 WCB_D void store_frame(float* dst, long long i, V3<float> u, V3<float> v) {

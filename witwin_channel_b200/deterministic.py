@@ -157,6 +157,16 @@ def _validate(scene: Any, config: Config) -> None:
         if config.max_diffraction_order < 1:
             raise RuntimeError("deterministic diffraction requires max_diffraction_order >= 1")
     receivers = scene.receivers
+    # scalar endpoints only (reference scene/endpoints.py:173-190): arrays,
+    # directional patterns and weights belong to the path solver
+    for endpoint in (*scene.transmitters, *receivers):
+        if int(getattr(endpoint, "num_antennas", 1)) != 1:
+            raise ValueError("the deterministic solver does not support antenna arrays")
+        pattern = getattr(endpoint, "pattern", None)
+        if pattern is not None and pattern.kind != "isotropic":
+            raise ValueError("the deterministic solver does not support directional antenna patterns")
+        if getattr(endpoint, "weights", None) is not None:
+            raise ValueError("the deterministic solver does not support precoding or combining")
     has_grid = any(isinstance(r, ReceiverGrid) for r in receivers)
     if has_grid and len(receivers) > 1 and not config.export_paths:
         raise RuntimeError("mixed point/grid receivers require export_paths=True")

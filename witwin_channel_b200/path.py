@@ -12,16 +12,19 @@ the packing of evaluated rows (``from_evaluated_paths``, ``:887-975``) and
 The paths come from the same native engine as the deterministic solve (row
 mode: candidate kernels, canonical selection with a per-pair limit, row
 field evaluation in ``libwcb200.so``); the packing is index arithmetic on
-device tensors, and the CFR views run the native ``wcb_cfr`` kernel.  The
-endpoints here are single antennas (the scene types carry no antenna
-arrays), so results have ``num_rx_ant == num_tx_ant == 1`` and one time
-step; ``beamform`` applies explicit complex weights.
+device tensors, and the CFR views run the native ``wcb_cfr`` kernel.
+Antenna arrays (``path.py:1079-1486``): synthetic arrays expand the centre
+endpoints' paths by far-field steering and element patterns; explicit
+arrays trace every element as its own endpoint in the same native solve.
+Endpoint weights (precoding / combining) ride on the result for
+``beamform``.  Results have one time step.
 """
 
 from __future__ import annotations
 
 import ctypes
 import enum
+import math
 from dataclasses import dataclass, replace
 from typing import Any
 
@@ -32,6 +35,7 @@ from .compiler import compile_scene
 from .constants import PHASE_CONVENTION
 from .deterministic import AD_MODES, DEFAULT_COMPONENTS, DEPTH_CAPPED_COMPONENTS, VALID_COMPONENTS
 from .deterministic import _endpoints, _frequency_value
+from .scene import AntennaPattern, AntennaState, ReceiverGrid, orientation_matrix
 
 _LIGHT_SPEED_M_PER_S = 299_792_458.0
 _VALID_MAX_PATHS_SCOPES = frozenset({"per_pair"})
@@ -650,18 +654,304 @@ def _validate(scene: Any, config: Config) -> None:
         raise RuntimeError("witwin_channel_b200.path solver requires CUDA")
 
 
+# --- antenna arrays (reference path.py:1079-1486, scene/endpoints.py:66-125) ---
+
+_ARRAY_PHASE_CONVENTION = "exp(+j*k*element_position_dot_endpoint_direction)"
+
+
+def _unit_vector(theta: torch.Tensor, phi: torch.Tensor) -> torch.Tensor:
+    sin_theta = torch.sin(theta)
+    return torch.stack((sin_theta * torch.cos(phi), sin_theta * torch.sin(phi), torch.cos(theta)), dim=-1)
+
+
+def _rotation(endpoint: Any, device: torch.device) -> torch.Tensor:
+    orientation = getattr(endpoint, "orientation", None)
+    if orientation is None:
+        return torch.eye(3, device=device)
+    return orientation_matrix(orientation).to(device)
+
+
+def _local_direction(direction: torch.Tensor, endpoint: Any) -> torch.Tensor:
+    return direction @ _rotation(endpoint, direction.device)
+
+
+def pattern_field_response(pattern: AntennaPattern, local_direction: torch.Tensor) -> torch.Tensor:
+    """Element field response at endpoint-local directions (reference
+    ``scene/endpoints.py:66-95``): isotropic 1, vertical sqrt(1 - z^2),
+    horizontal sqrt(1 - x^2) of the unit direction, or the custom callable."""
+
+    direction = local_direction.to(torch.float32)
+    direction = direction / torch.linalg.vector_norm(direction, dim=-1, keepdim=True).clamp_min(
+        torch.finfo(torch.float32).tiny)
+    if pattern.kind == "custom":
+        response = pattern.custom(direction)
+        if response.shape != direction.shape[:-1]:
+            raise ValueError("custom pattern response must match direction batch shape")
+        return response.to(device=direction.device, dtype=torch.complex64)
+    if pattern.kind == "vertical":
+        response = torch.sqrt(torch.clamp(1.0 - direction[..., 2].square(), min=0.0))
+    elif pattern.kind == "horizontal":
+        response = torch.sqrt(torch.clamp(1.0 - direction[..., 0].square(), min=0.0))
+    else:
+        response = torch.ones(direction.shape[:-1], device=direction.device)
+    return response.to(torch.complex64)
+
+
+def steering_vector(endpoint: Any, direction: torch.Tensor, *, frequency_hz: float) -> torch.Tensor:
+    """``exp(+j k r . u)`` per element (reference ``scene/endpoints.py:98-125``)
+    under the ``exp(-j k d)`` phase convention: the element positions turned
+    by the endpoint orientation, ``u`` the unit direction.  (..., A)."""
+
+    if frequency_hz <= 0.0:
+        raise ValueError("frequency_hz must be positive")
+    device = direction.device
+    positions = endpoint.element_positions.to(device) @ _rotation(endpoint, device).T
+    unit = direction.to(torch.float32)
+    unit = unit / torch.linalg.vector_norm(unit, dim=-1, keepdim=True).clamp_min(torch.finfo(torch.float32).tiny)
+    phase = (2.0 * math.pi * float(frequency_hz) / _LIGHT_SPEED_M_PER_S) * torch.einsum("...c,ac->...a", unit,
+                                                                                         positions)
+    return torch.exp(1.0j * phase).to(torch.complex64)
+
+
+def apply_endpoint_weights(coefficients: torch.Tensor, *, tx_weights: torch.Tensor,
+                           rx_weights: torch.Tensor) -> torch.Tensor:
+    """Combine ``(rx, rx_ant, tx, tx_ant, ...)`` channels with per-endpoint
+    weights (reference ``scene/endpoints.py:143-170``): transmit weights as
+    given, receive weights conjugated; trailing dimensions kept."""
+
+    if coefficients.ndim < 4:
+        raise ValueError("coefficients must have (rx, rx_ant, tx, tx_ant, ...) dimensions")
+    expected_tx = (coefficients.shape[2], coefficients.shape[3])
+    expected_rx = (coefficients.shape[0], coefficients.shape[1])
+    if tx_weights.shape != expected_tx:
+        raise ValueError(f"tx_weights must have shape {expected_tx}")
+    if rx_weights.shape != expected_rx:
+        raise ValueError(f"rx_weights must have shape {expected_rx}")
+    tx = tx_weights.to(device=coefficients.device, dtype=torch.complex64)
+    rx = rx_weights.to(device=coefficients.device, dtype=torch.complex64)
+    tail = (1,) * (coefficients.ndim - 4)
+    weighted = coefficients * tx.reshape(1, 1, *expected_tx, *tail)
+    weighted = weighted * rx.conj().reshape(*expected_rx, 1, 1, *tail)
+    return weighted.sum(dim=3).sum(dim=1)
+
+
+def _flatten_receivers(receivers: list) -> list:
+    out: list = []
+    for receiver in receivers:
+        out.extend([receiver] * (receiver.count if isinstance(receiver, ReceiverGrid) else 1))
+    return out
+
+
+def _weight_coverage(endpoints: list, attribute: str) -> None:
+    values = [getattr(endpoint, attribute, None) for endpoint in endpoints]
+    if any(v is None for v in values) and any(v is not None for v in values):
+        raise ValueError(f"{attribute} must be configured on every endpoint or none")
+
+
+def _stack_weights(endpoints: list, attribute: str, device: torch.device) -> torch.Tensor | None:
+    values = [getattr(endpoint, attribute, None) for endpoint in endpoints]
+    if not values or all(v is None for v in values):
+        return None
+    _weight_coverage(endpoints, attribute)
+    return torch.stack(values).to(device=device, dtype=torch.complex64)
+
+
+def _antenna_counts(transmitters: list, receivers: list) -> tuple[int, int]:
+    tx_counts = {int(getattr(t, "num_antennas", 1)) for t in transmitters}
+    rx_counts = {int(getattr(r, "num_antennas", 1)) for r in receivers}
+    if len(tx_counts) > 1 or len(rx_counts) > 1:
+        raise ValueError("all endpoints on each side must use the same antenna count")
+    return next(iter(rx_counts), 1), next(iter(tx_counts), 1)
+
+
+def validate_synthetic_array_scene(transmitters: list, receivers: list) -> None:
+    """Preflight of a synthetic-array solve (reference ``path.py:1200-1212``)."""
+
+    flat = _flatten_receivers(receivers)
+    if any(not getattr(e, "synthetic_array", True) for e in (*transmitters, *flat)):
+        raise ValueError("explicit arrays require per-element topology tracing")
+    _antenna_counts(transmitters, flat)
+    _weight_coverage(transmitters, "precoding")
+    _weight_coverage(flat, "combining")
+
+
+def _endpoint_factor(endpoints: list, directions: torch.Tensor, *, frequency_hz: float,
+                     conjugate_pattern: bool) -> torch.Tensor:
+    """Steering x pattern weights of each endpoint over its own directions
+    (``directions[i]`` for ``endpoints[i]``): (endpoint, *batch, A).  Endpoints
+    sharing one object (a grid's points) are evaluated in one batch."""
+
+    groups: dict[int, list[int]] = {}
+    for index, endpoint in enumerate(endpoints):
+        groups.setdefault(id(endpoint), []).append(index)
+
+    def weights(endpoint: Any, sub: torch.Tensor) -> torch.Tensor:
+        pattern = pattern_field_response(endpoint.pattern, _local_direction(sub, endpoint))
+        if conjugate_pattern:
+            pattern = pattern.conj()
+        return steering_vector(endpoint, sub, frequency_hz=frequency_hz) * pattern.unsqueeze(-1)
+
+    if len(groups) == 1:
+        return weights(endpoints[0], directions)
+    num_ant = int(endpoints[0].num_antennas)
+    out = torch.empty((len(endpoints), *directions.shape[1:-1], num_ant), dtype=torch.complex64,
+                      device=directions.device)
+    for indices in groups.values():
+        idx = torch.tensor(indices, device=directions.device, dtype=torch.long)
+        out.index_copy_(0, idx, weights(endpoints[indices[0]], directions.index_select(0, idx)))
+    return out
+
+
+def _array_metadata(result: PathResult, semantics: str, num_rx_ant: int, num_tx_ant: int) -> dict:
+    meta = dict(result.metadata)
+    meta.update({"array_semantics": semantics, "num_rx_ant": num_rx_ant, "num_tx_ant": num_tx_ant})
+    if semantics.startswith("synthetic"):
+        meta["array_phase_convention"] = _ARRAY_PHASE_CONVENTION
+    return meta
+
+
+def pack_synthetic_arrays(result: PathResult, *, frequency_hz: float, transmitters: list,
+                          receivers: list) -> PathResult:
+    """Expand a centre-endpoint result over synthetic arrays by far-field
+    phase weighting (reference ``path.py:1215-1337``): every element shares the
+    centre's paths; each path is weighted by the transmit steering and
+    pattern at its departure direction and the receive steering and
+    conjugate pattern at its arrival (source) direction."""
+
+    if frequency_hz <= 0.0:
+        raise ValueError("frequency_hz must be positive")
+    flat = _flatten_receivers(receivers)
+    if len(transmitters) != result.num_tx or len(flat) != result.num_rx:
+        raise ValueError("endpoint counts must match the centre-reference result")
+    if result.num_tx_ant != 1 or result.num_rx_ant != 1:
+        raise ValueError("synthetic packing requires a single-antenna centre result")
+    validate_synthetic_array_scene(transmitters, receivers)
+    num_rx_ant, num_tx_ant = _antenna_counts(transmitters, flat)
+    device = result.a.device
+    tx_weights = _stack_weights(transmitters, "precoding", device)
+    rx_weights = _stack_weights(flat, "combining", device)
+    meta = _array_metadata(result, "synthetic_far_field_phase_weighting", num_rx_ant, num_tx_ant)
+    if result.num_tx == 0 or result.num_rx == 0:
+        return replace(result, metadata=meta, tx_weights=tx_weights, rx_weights=rx_weights)
+    departure = _unit_vector(result.theta_t[:, 0, :, 0], result.phi_t[:, 0, :, 0])            # (rx, tx, path, 3)
+    arrival = _unit_vector(result.theta_r[:, 0, :, 0], result.phi_r[:, 0, :, 0])
+    # (tx, rx, path, A_tx) -> (rx, tx, A_tx, path)
+    tx_factor = _endpoint_factor(transmitters, departure.transpose(0, 1), frequency_hz=frequency_hz,
+                                 conjugate_pattern=False).permute(1, 0, 3, 2)
+    # (rx, tx, path, A_rx) -> (rx, A_rx, tx, path)
+    rx_factor = _endpoint_factor(flat, arrival, frequency_hz=frequency_hz, conjugate_pattern=True).permute(0, 3, 1, 2)
+    factor = rx_factor[:, :, :, None, :] * tx_factor[:, None, :, :, :]
+
+    def expand(value: torch.Tensor) -> torch.Tensor:
+        base = value[:, 0, :, 0]
+        return base[:, None, :, None].expand(result.num_rx, num_rx_ant, result.num_tx, num_tx_ant,
+                                             *base.shape[2:]).contiguous()
+
+    return replace(
+        result, a=(expand(result.a) * factor.unsqueeze(-1)).to(torch.complex64), tau=expand(result.tau),
+        theta_t=expand(result.theta_t), phi_t=expand(result.phi_t), theta_r=expand(result.theta_r),
+        phi_r=expand(result.phi_r), valid=expand(result.valid), interaction_type=expand(result.interaction_type),
+        primitive_id=expand(result.primitive_id), material_id=expand(result.material_id),
+        position=expand(result.position), normal=expand(result.normal), num_paths=expand(result.num_paths),
+        metadata=meta, field_xyz=(expand(result.field_xyz) * factor.unsqueeze(-1)).to(torch.complex64),
+        field_direction=expand(result.field_direction), tx_weights=tx_weights, rx_weights=rx_weights)
+
+
+class _ElementEndpoints:
+    """The endpoints of an explicit-array solve: one single-element endpoint
+    per array element, at its world position, keeping the endpoint's world
+    polarization and power (reference ``path.py:1340-1387``)."""
+
+    def __init__(self, transmitters: list, receivers: list) -> None:
+        if any(isinstance(r, ReceiverGrid) for r in receivers):
+            raise ValueError("explicit arrays currently require point receivers")
+
+        def expand(endpoint: Any, role: str) -> list:
+            return [AntennaState(endpoint.id, role, p, polarization=endpoint.polarization,
+                                 power_w=getattr(endpoint, "power_w", 1.0))
+                    for p in endpoint.element_world_positions(endpoint.position)]
+
+        self.transmitters = [e for t in transmitters for e in expand(t, "tx")]
+        self.receivers = [e for r in receivers for e in expand(r, "rx")]
+
+
+def pack_explicit_arrays(result: PathResult, *, transmitters: list, receivers: list, num_rx_ant: int,
+                         num_tx_ant: int) -> PathResult:
+    """Fold per-element endpoints back into antenna dimensions and apply the
+    element patterns at each element's own departure / arrival directions
+    (reference ``path.py:1390-1454``)."""
+
+    num_rx, num_tx = len(receivers), len(transmitters)
+    if result.num_rx != num_rx * num_rx_ant or result.num_tx != num_tx * num_tx_ant:
+        raise ValueError("expanded explicit result does not match endpoint array layout")
+
+    def fold(value: torch.Tensor) -> torch.Tensor:
+        base = value[:, 0, :, 0]
+        return base.reshape(num_rx, num_rx_ant, num_tx, num_tx_ant, *base.shape[2:])
+
+    theta_t, phi_t, theta_r, phi_r = (fold(result.theta_t), fold(result.phi_t), fold(result.theta_r),
+                                      fold(result.phi_r))
+    factor = torch.ones_like(theta_t, dtype=torch.complex64)
+    departure = _unit_vector(theta_t, phi_t)
+    arrival = _unit_vector(theta_r, phi_r)
+    for tx_id, transmitter in enumerate(transmitters):
+        factor[:, :, tx_id] *= pattern_field_response(transmitter.pattern,
+                                                      _local_direction(departure[:, :, tx_id], transmitter))
+    for rx_id, receiver in enumerate(receivers):
+        factor[rx_id] *= pattern_field_response(receiver.pattern, _local_direction(arrival[rx_id], receiver)).conj()
+    device = result.a.device
+    return replace(
+        result, a=(fold(result.a) * factor.unsqueeze(-1)).contiguous(), tau=fold(result.tau), theta_t=theta_t,
+        phi_t=phi_t, theta_r=theta_r, phi_r=phi_r, valid=fold(result.valid),
+        interaction_type=fold(result.interaction_type), primitive_id=fold(result.primitive_id),
+        material_id=fold(result.material_id), position=fold(result.position), normal=fold(result.normal),
+        num_paths=fold(result.num_paths),
+        metadata=_array_metadata(result, "explicit_per_element_topology", num_rx_ant, num_tx_ant),
+        field_xyz=(fold(result.field_xyz) * factor.unsqueeze(-1)).contiguous(),
+        field_direction=fold(result.field_direction),
+        tx_weights=_stack_weights(transmitters, "precoding", device),
+        rx_weights=_stack_weights(receivers, "combining", device))
+
+
 def solve(scene: Any, config: Config, *, reference_frequency_hz) -> PathResult:
     """Canonical paths of every (rx, tx) pair packed per pair (reference
     ``path.py:1551-1721``): the native row-mode solve, selection with the
     per-pair limit, row field evaluation, then the ragged and padded
-    packing of ``from_evaluated_paths`` (``path.py:887-975``)."""
+    packing of ``from_evaluated_paths`` (``path.py:887-975``).  Antenna
+    arrays (reference ``_pipeline_solve``, ``path.py:1654-1681``): synthetic
+    arrays share the centre endpoints' paths and are expanded by far-field
+    phase weighting; if any endpoint's array is explicit, every element is
+    traced as its own endpoint."""
     if not isinstance(config, Config):
         raise TypeError("config must be a witwin_channel_b200.path.Config")
     frequency = _frequency_value(reference_frequency_hz)
+    transmitters, receivers = list(scene.transmitters), list(scene.receivers)
+    # array preflight before any device work
+    explicit = any(not getattr(e, "synthetic_array", True) for e in (*transmitters, *receivers))
+    if explicit:
+        if any(isinstance(r, ReceiverGrid) for r in receivers):
+            raise ValueError("explicit arrays currently require point receivers")
+        num_rx_ant, num_tx_ant = _antenna_counts(transmitters, receivers)
+        _weight_coverage(transmitters, "precoding")
+        _weight_coverage(receivers, "combining")
+    else:
+        validate_synthetic_array_scene(transmitters, receivers)
     _validate(scene, config)
+    if explicit:
+        elements = _ElementEndpoints(transmitters, receivers)
+        base = _solve_base(scene, config, frequency, elements)
+        return pack_explicit_arrays(base, transmitters=transmitters, receivers=receivers, num_rx_ant=num_rx_ant,
+                                    num_tx_ant=num_tx_ant)
+    base = _solve_base(scene, config, frequency, scene)
+    return pack_synthetic_arrays(base, frequency_hz=frequency, transmitters=transmitters, receivers=receivers)
+
+
+def _solve_base(scene: Any, config: Config, frequency: float, endpoints: Any) -> PathResult:
+    """One centre-endpoint solve of ``scene``'s geometry between the
+    endpoints of ``endpoints`` (``.transmitters`` / ``.receivers``)."""
     device = torch.device("cuda", torch.cuda.current_device())
     compiled = compile_scene(scene, device)
-    ep = _endpoints(scene, device)
+    ep = _endpoints(endpoints, device)
     mats = compiled.material_tables([frequency], device)
     bits = engine.component_bits(config.components)
     width = max(int(config.max_depth), 0)
@@ -703,7 +993,7 @@ def solve(scene: Any, config: Config, *, reference_frequency_hz) -> PathResult:
     nrm = torch.where(torch.isfinite(nrm), nrm, torch.zeros_like(nrm))
     # departure / arrival angles from the endpoints and the first / last event
     tx_pos = ep.tx_pos
-    rx_pos = _receiver_positions(scene, ep.rx, device)
+    rx_pos = _receiver_positions(endpoints, ep.rx, device)
     tp = tx_pos[tx_id] if K else torch.zeros((0, 3), device=device)
     rp = rx_pos[rx_id] if K else torch.zeros((0, 3), device=device)
     direct = rp - tp
@@ -756,4 +1046,6 @@ def solve(scene: Any, config: Config, *, reference_frequency_hz) -> PathResult:
     return replace(result, field_xyz=field_xyz, field_direction=field_direction)
 
 
-__all__ = ["Config", "InteractionType", "PathResult", "RaggedPathSoA", "solve"]
+__all__ = ["Config", "InteractionType", "PathResult", "RaggedPathSoA", "apply_endpoint_weights",
+           "pack_explicit_arrays", "pack_synthetic_arrays", "pattern_field_response", "solve", "steering_vector",
+           "validate_synthetic_array_scene"]

@@ -150,8 +150,108 @@ def _vec3(value: Any) -> torch.Tensor:
     return torch.tensor(tuple(float(v) for v in value), dtype=torch.float32)
 
 
-class AntennaState:
-    """A transmitter (``role="tx"``) or point receiver (``role="rx"``)."""
+_PATTERN_KINDS = ("isotropic", "vertical", "horizontal", "custom")
+
+
+class AntennaPattern:
+    """Element field pattern in the endpoint-local frame (the reference's
+    ``witwin.core.AntennaPattern``, evaluated by
+    ``witwin/channel/scene/endpoints.py:66-95``): ``isotropic`` (1),
+    ``vertical`` (sqrt(1 - z^2)), ``horizontal`` (sqrt(1 - x^2)) of the local
+    unit direction, or ``custom`` (a callable of the (..., 3) local unit
+    directions returning their complex responses)."""
+
+    def __init__(self, kind: str = "isotropic", custom: Any = None) -> None:
+        if kind not in _PATTERN_KINDS:
+            raise ValueError(f"pattern kind must be one of {_PATTERN_KINDS}")
+        if (kind == "custom") != (custom is not None):
+            raise ValueError("a custom pattern needs its callable, and only a custom pattern takes one")
+        self.kind = kind
+        self.custom = custom
+
+
+def _pattern(value: Any) -> AntennaPattern:
+    if isinstance(value, AntennaPattern):
+        return value
+    if value is None:
+        return AntennaPattern("isotropic")
+    if isinstance(value, str):
+        return AntennaPattern(value)
+    raise TypeError("pattern must be an AntennaPattern or a pattern kind string")
+
+
+def orientation_matrix(orientation: torch.Tensor) -> torch.Tensor:
+    """Local-to-world rotation of a ``(yaw, pitch, roll)`` orientation in
+    radians, intrinsic Z-Y-X (reference ``scene/endpoints.py:42-63``)."""
+
+    o = torch.as_tensor(orientation, dtype=torch.float32).reshape(-1)
+    if o.shape != (3,):
+        raise ValueError("orientation must be (yaw, pitch, roll)")
+    yaw, pitch, roll = o.unbind()
+    cy, sy = torch.cos(yaw), torch.sin(yaw)
+    cp, sp = torch.cos(pitch), torch.sin(pitch)
+    cr, sr = torch.cos(roll), torch.sin(roll)
+    return torch.stack((
+        torch.stack((cy * cp, cy * sp * sr - sy * cr, cy * sp * cr + sy * sr)),
+        torch.stack((sy * cp, sy * sp * sr + cy * cr, sy * sp * cr - cy * sr)),
+        torch.stack((-sp, cp * sr, cp * cr)),
+    )).to(torch.float32)
+
+
+class _ArrayEndpoint:
+    """Antenna-array attributes shared by point endpoints and receiver grids:
+    element positions (A, 3) in the local frame (one element at the origin
+    by default), orientation, element pattern, per-element weights
+    (precoding on a transmitter, combining on a receiver) and whether the
+    array is synthetic (one traced path set, far-field phase per element) or
+    explicit (every element traced)."""
+
+    def _init_array(self, *, orientation: Any, element_positions: Any, weights: Any, synthetic_array: bool,
+                    pattern: Any) -> None:
+        self.orientation = None if orientation is None else torch.as_tensor(orientation, dtype=torch.float32).reshape(3)
+        if element_positions is None:
+            positions = torch.zeros((1, 3), dtype=torch.float32)
+        else:
+            positions = torch.as_tensor(element_positions, dtype=torch.float32)
+            if positions.ndim != 2 or positions.shape[1] != 3 or positions.shape[0] < 1:
+                raise ValueError("element_positions must have shape (A, 3) with A >= 1")
+        self.element_positions = positions
+        if weights is not None:
+            weights = torch.as_tensor(weights).to(torch.complex64).reshape(-1)
+            if weights.shape[0] != positions.shape[0]:
+                raise ValueError("weights must hold one entry per antenna element")
+        self.weights = weights
+        self.synthetic_array = bool(synthetic_array)
+        self.pattern = _pattern(pattern)
+
+    @property
+    def num_antennas(self) -> int:
+        return int(self.element_positions.shape[0])
+
+    @property
+    def precoding(self) -> torch.Tensor | None:
+        return self.weights if getattr(self, "role", None) == "tx" else None
+
+    @property
+    def combining(self) -> torch.Tensor | None:
+        return self.weights if getattr(self, "role", None) == "rx" else None
+
+    def rotation(self) -> torch.Tensor:
+        return torch.eye(3) if self.orientation is None else orientation_matrix(self.orientation)
+
+    def element_world_positions(self, origin: torch.Tensor) -> torch.Tensor:
+        """World positions of the elements about ``origin`` (reference
+        ``scene/endpoints.py:201-205``)."""
+        return origin.reshape(1, 3).to(torch.float32) + self.element_positions @ self.rotation().T
+
+
+class AntennaState(_ArrayEndpoint):
+    """A transmitter (``role="tx"``) or point receiver (``role="rx"``), with
+    an optional antenna array (see :class:`_ArrayEndpoint`).
+
+    ``polarization`` is the world polarization: the given vector, or (0, 0, 1)
+    ((1, 0, 0) for a horizontal pattern), normalised and turned by the
+    orientation when one is given."""
 
     def __init__(
         self,
@@ -161,6 +261,11 @@ class AntennaState:
         *,
         polarization: Any = None,
         power_w: float | torch.Tensor = 1.0,
+        orientation: Any = None,
+        element_positions: Any = None,
+        weights: Any = None,
+        synthetic_array: bool = True,
+        pattern: Any = "isotropic",
         **_: Any,
     ) -> None:
         if role not in ("tx", "rx"):
@@ -168,21 +273,26 @@ class AntennaState:
         self.id = id
         self.role = role
         self.position = _vec3(position)
-        self.polarization = (
-            torch.tensor((0.0, 0.0, 1.0)) if polarization is None else _vec3(polarization)
-        )
+        self._init_array(orientation=orientation, element_positions=element_positions, weights=weights,
+                         synthetic_array=synthetic_array, pattern=pattern)
+        default = (1.0, 0.0, 0.0) if self.pattern.kind == "horizontal" else (0.0, 0.0, 1.0)
+        pol = torch.tensor(default) if polarization is None else _vec3(polarization)
+        if self.orientation is not None:
+            pol = self.rotation() @ (pol.float() / torch.linalg.vector_norm(pol.float()))
+        self.polarization = pol
         self.power_w = 1.0 if power_w is None else power_w
 
 
 ReceiverPoint = AntennaState
 
 
-class ReceiverGrid:
+class ReceiverGrid(_ArrayEndpoint):
     """A planar receiver grid.
 
     Point ``(row, col)`` sits at ``origin + x_axis*row*spacing[0] +
     y_axis*col*spacing[1]``; results come back as ``(T, shape[1], shape[0])``
     (``witwin/channel/propagation/geometry.py:71-89``; ``los.cu:391-420``).
+    Every grid point carries the grid's antenna array (synthetic only).
     """
 
     role = "rx"
@@ -197,8 +307,15 @@ class ReceiverGrid:
         spacing: Sequence[float],
         *,
         polarization: Any = None,
+        orientation: Any = None,
+        element_positions: Any = None,
+        weights: Any = None,
+        synthetic_array: bool = True,
+        pattern: Any = "isotropic",
         **_: Any,
     ) -> None:
+        self._init_array(orientation=orientation, element_positions=element_positions, weights=weights,
+                         synthetic_array=synthetic_array, pattern=pattern)
         rows, cols = (int(shape[0]), int(shape[1]))
         if rows < 0 or cols < 0:
             raise ValueError("shape entries must be non-negative")
@@ -210,9 +327,11 @@ class ReceiverGrid:
         self.y_axis = _vec3(y_axis)
         self.shape = (rows, cols)
         self.spacing = (float(spacing[0]), float(spacing[1]))
-        self.polarization = (
-            torch.tensor((0.0, 0.0, 1.0)) if polarization is None else _vec3(polarization)
-        )
+        default = (1.0, 0.0, 0.0) if self.pattern.kind == "horizontal" else (0.0, 0.0, 1.0)
+        pol = torch.tensor(default) if polarization is None else _vec3(polarization)
+        if self.orientation is not None:
+            pol = self.rotation() @ (pol.float() / torch.linalg.vector_norm(pol.float()))
+        self.polarization = pol
         self.position = self.origin
 
     @property
@@ -280,16 +399,22 @@ class Scene:
         return [e for e in self.endpoints if getattr(e, "role", None) == "rx"]
 
 
+_ARRAY_KEYS = ("orientation", "element_positions", "weights", "synthetic_array", "pattern")
+
+
 def make_transmitter(position: Any, *, polarization: Any = None, power_w: float = 1.0, **kw: Any) -> AntennaState:
-    return AntennaState(new_antenna_id(), "tx", position, polarization=polarization, power_w=power_w)
+    return AntennaState(new_antenna_id(), "tx", position, polarization=polarization, power_w=power_w,
+                        **{k: kw[k] for k in _ARRAY_KEYS if k in kw})
 
 
 def make_receiver(position: Any, *, polarization: Any = None, **kw: Any) -> AntennaState:
-    return AntennaState(new_antenna_id(), "rx", position, polarization=polarization)
+    return AntennaState(new_antenna_id(), "rx", position, polarization=polarization,
+                        **{k: kw[k] for k in _ARRAY_KEYS if k in kw})
 
 
 def make_receiver_grid(*, origin: Any, x_axis: Any, y_axis: Any, shape: Sequence[int], spacing: Sequence[float], polarization: Any = None, **kw: Any) -> ReceiverGrid:
-    return ReceiverGrid(new_antenna_id(), origin, x_axis, y_axis, shape, spacing, polarization=polarization)
+    return ReceiverGrid(new_antenna_id(), origin, x_axis, y_axis, shape, spacing, polarization=polarization,
+                        **{k: kw[k] for k in _ARRAY_KEYS if k in kw})
 
 
 def make_mesh_structure(*, vertices: Any, faces: Any, material: PhysicalMaterial, surface_id: int | None = None, name: str = "", **kw: Any) -> Structure:
@@ -297,6 +422,7 @@ def make_mesh_structure(*, vertices: Any, faces: Any, material: PhysicalMaterial
 
 
 __all__ = [
+    "AntennaPattern",
     "AntennaState",
     "MaterialLayer",
     "Mesh",
@@ -310,4 +436,5 @@ __all__ = [
     "make_receiver",
     "make_receiver_grid",
     "make_transmitter",
+    "orientation_matrix",
 ]
