@@ -317,6 +317,7 @@ def run_native(args) -> None:
     e2e_value = rays_all * e2e_steps / (e2e_ms_all / 1000.0)
     single = world == 1
     plain = None if (args.no_batched or not single) else _batched_plain(full, device)
+    forward_graph = None if (args.no_batched or not single) else _batched_forward_graph(full, device)
     canyon = None if (args.no_canyon or not single) else _canyon_run(args, device)
     vjp = None if (args.no_vjp or not single) else _vjp_run(device)
     large = None if (args.no_large or not single) else _large_run(device)
@@ -381,6 +382,7 @@ def run_native(args) -> None:
             "fp64_plain": None if plain is None else dict(
                 plain, speedup=plain["ms_per_step"] / (step_ms_all / args.steps),
                 batched_ms_per_step=step_ms_all / args.steps),
+            "forward_graph": forward_graph,
             "canyon": canyon,
             "vjp": vjp,
             "large": large,
@@ -788,6 +790,45 @@ def _large_run(device, steps: int = 2) -> dict:
     del h, res
     torch.cuda.empty_cache()
     return out
+
+
+def _batched_forward_graph(full, device, reps: int = 5) -> dict:
+    """The headline workload's batched forward (radiomaps only) issued eagerly
+    (``solve_batch``) and as a captured CUDA graph (``BatchGraph``, stream pool
+    size picked by timing); best of ``reps`` each, inputs resident."""
+    import torch
+
+    from witwin_channel_b200 import Config
+    from witwin_channel_b200.batch import BatchGraph, solve_batch
+    from witwin_channel_b200.workloads import BATCH_FREQS
+
+    try:
+        cfg = Config(components={"los", "reflection", "diffraction"}, max_depth=3, return_field=False)
+
+        def best(fn):
+            fn()
+            torch.cuda.synchronize()
+            t = float("inf")
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                fn()
+                e1.record()
+                torch.cuda.synchronize()
+                t = min(t, e0.elapsed_time(e1))
+            return t
+
+        eager_ms = best(lambda: solve_batch(full, cfg, BATCH_FREQS))
+        graph = BatchGraph(full, cfg, BATCH_FREQS, streams="auto")
+        graph_ms = best(graph.replay)
+        graph.check()
+        same = all(torch.equal(a["path_gain"], b["path_gain"])
+                   for a, b in zip(graph.replay(), solve_batch(full, cfg, BATCH_FREQS)))
+        return {"eager_ms": eager_ms, "graph_ms": graph_ms, "streams": graph.streams,
+                "tuning_ms": graph.tuning, "graph_equals_eager": same,
+                "statistic": f"best of {reps} after one untimed run"}
+    except Exception as exc:  # reported in the leg; the headline line stands
+        return {"error": f"{type(exc).__name__}: {exc}"}
 
 
 def _batched_plain(full, device, reps: int = 2) -> dict:

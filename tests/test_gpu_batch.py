@@ -62,3 +62,28 @@ def test_batch_vjp_matches_single_frequency_vjps():
         # same records, same FP64 adjoint; the cotangents pass through FP32 outputs
         assert abs(float(ft.grad) - float(g_f[fi])) <= 1e-6 * max(abs(float(ft.grad)), 1e-30) + 1e-30
     assert abs(g_eps - total_eps) <= 1e-6 * abs(total_eps)
+
+
+def test_captured_batch_graph_replays_the_eager_batch():
+    """A ``BatchGraph`` (the batched forward captured once in a CUDA graph)
+    reproduces the eager batched forward bit for bit on every replay, with a
+    fixed stream pool and with the pool size picked by timing."""
+    from witwin_channel_b200.batch import BatchGraph
+
+    scenes = [_two_tx_city(6), _two_tx_city(7), _two_tx_city(8)]
+    cfg = Config(components={"los", "reflection", "diffraction"}, max_depth=2)
+    eager = solve_batch(scenes, cfg, FREQS)
+    graph = BatchGraph(scenes, cfg, FREQS, streams=2)
+    for _ in range(2):
+        out = graph.replay()
+        graph.check()
+        for a, b in zip(out, eager):
+            assert torch.equal(a["path_gain"], b["path_gain"])
+            assert torch.equal(a["field"], b["field"])
+    tuned = BatchGraph(scenes, cfg, FREQS, streams="auto", tuning_replays=2)
+    assert set(tuned.tuning) == set(BatchGraph.STREAM_CANDIDATES)
+    assert tuned.streams == min(tuned.tuning, key=tuned.tuning.get)
+    for a, b in zip(tuned.replay(), eager):
+        assert torch.equal(a["path_gain"], b["path_gain"])
+    with pytest.raises(ValueError):
+        BatchGraph(scenes, Config(components={"los"}, ad_mode="vjp"), FREQS)

@@ -88,3 +88,114 @@ def single_transmitter_scene(scene: Any, t: int):
     txs = scene.transmitters
     return Scene(structures=scene.structures, endpoints=[txs[t]] + list(scene.receivers),
                  metadata=dict(getattr(scene, "metadata", {})))
+
+
+class BatchGraph:
+    """The batched radiomap forward of a fixed set of scenes, transmitters,
+    receivers, materials and frequencies, captured once in a CUDA graph and
+    replayed as one graph launch per step.
+
+    Everything a step reads is prepared before the capture and stays resident:
+    the compiled scenes, the endpoint and material tables, one workspace and
+    one set of cell outputs per scene.  The capture records every scene's
+    ``wcb_solve`` on a pool of ``streams`` CUDA streams (and the solve's own
+    side stream), so a replay runs them with the same overlap as the eager
+    form and no host work or synchronisation between launches.  A change of
+    any input value (a moved vertex, a new material value, another frequency)
+    needs a new ``BatchGraph``.  ``streams`` may be ``"auto"``: each candidate
+    pool size is captured and timed over a few replays, and the fastest graph
+    is kept (``tuning`` records the times).
+
+    ``replay()`` returns the per-scene outputs of :func:`solve_batch`;
+    ``check()`` reads the scenes' device status words (one synchronisation)."""
+
+    STREAM_CANDIDATES = (1, 2, 4, 8)
+
+    def __init__(self, scenes: list, config: Config, frequencies_hz, *, precision: str = "mixed",
+                 streams: int | str = 4, tuning_replays: int = 3) -> None:
+        freqs = [float(f) for f in (frequencies_hz.detach().cpu() if isinstance(frequencies_hz, torch.Tensor)
+                                    else frequencies_hz)]
+        if not 1 <= len(freqs) <= 4:
+            raise ValueError("BatchGraph takes 1 to 4 frequencies")
+        if config.ad_mode != "none":
+            raise ValueError("BatchGraph captures the forward only (ad_mode='none')")
+        for scene in scenes:
+            _validate(scene, config)
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.config = config
+        self.frequencies = freqs
+        self._prec = _native.PRECISION_FP64 if precision == "fp64" else _native.PRECISION_MIXED
+        self._bits = engine.component_bits(config.components)
+        self._items = []
+        for scene in scenes:
+            compiled = compile_scene(scene, self.device)
+            ep = _endpoints(scene, self.device)
+            mats = compiled.material_tables(freqs, self.device)
+            cells = engine.alloc_cells(len(freqs), ep.num_tx, ep.num_rx, self.device,
+                                       fp64=(self._prec == _native.PRECISION_FP64))
+            self._items.append({"compiled": compiled, "ep": ep, "mats": mats, "cells": cells,
+                                "workspace": engine.Workspace()})
+        candidates = self.STREAM_CANDIDATES if streams == "auto" else (int(streams),)
+        self.tuning: dict[int, float] = {}
+        best = None
+        for count in candidates:
+            graph, alive = self._capture(count)
+            if len(candidates) > 1:
+                self.tuning[count] = self._time(graph, tuning_replays)
+            if best is None or (len(candidates) > 1 and self.tuning[count] < self.tuning[best[0]]):
+                best = (count, graph, alive)
+        self.streams, self.graph, self._alive = best
+
+    def _launch(self, pool: list, keep: list) -> None:
+        current = torch.cuda.current_stream(self.device)
+        for i, item in enumerate(self._items):
+            s = pool[i % len(pool)]
+            s.wait_stream(current)
+            with torch.cuda.stream(s):
+                res = engine.run_solve(item["compiled"], item["ep"], item["mats"], self.frequencies,
+                                       components=self._bits, max_depth=self.config.max_depth,
+                                       coherent=self.config.coherent, precision=self._prec, cells=item["cells"],
+                                       check_status=False, workspace=item["workspace"])
+            keep.append(res)
+        for s in pool:
+            current.wait_stream(s)
+
+    def _capture(self, count: int):
+        pool = [torch.cuda.Stream(device=self.device) for _ in range(max(1, count))]
+        # an eager run first: sizes the workspaces and loads every kernel
+        warm: list = []
+        self._launch(pool, warm)
+        torch.cuda.synchronize(self.device)
+        for res in warm:
+            engine.check_device_status(res["status"])
+        graph = torch.cuda.CUDAGraph()
+        keep: list = []
+        with torch.cuda.graph(graph):
+            self._launch(pool, keep)
+        return graph, (pool, keep)
+
+    def _time(self, graph, replays: int) -> float:
+        graph.replay()
+        torch.cuda.synchronize(self.device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(max(1, replays)):
+            graph.replay()
+        e1.record()
+        torch.cuda.synchronize(self.device)
+        return e0.elapsed_time(e1) / max(1, replays)
+
+    def replay(self) -> list[dict]:
+        self.graph.replay()
+        out = []
+        for item in self._items:
+            rx = item["ep"].rx
+            res = {"path_gain": _layout_nf(item["cells"].path_gain, rx)}
+            if self.config.return_field:
+                res["field"] = _layout_nf(item["cells"].field, rx)
+            out.append(res)
+        return out
+
+    def check(self) -> None:
+        for res in self._alive[1]:
+            engine.check_device_status(res["status"])

@@ -193,6 +193,21 @@ class CompiledScene:
         out["layers"] = layers
         return out
 
+    def resident_tables(self, frequencies: list[float], device: torch.device) -> tuple["MaterialTables", torch.Tensor]:
+        """Material tables and the FP64 frequency array at ``frequencies``, kept
+        on the device for repeated calls with the same frequencies (a per-frame
+        replay of frozen rows) while the material values are unchanged."""
+        key = (tuple(float(f) for f in frequencies), str(device), self.material_version)
+        cache = self.__dict__.setdefault("_resident_tables", {})
+        hit = cache.get(key)
+        if hit is None:
+            if len(cache) >= 8:
+                cache.pop(next(iter(cache)))
+            freqs = torch.tensor([float(f) for f in frequencies], dtype=torch.float64)
+            freqs = freqs.pin_memory().to(device, non_blocking=True) if device.type == "cuda" else freqs.to(device)
+            hit = cache[key] = (self.material_tables(frequencies, device), freqs)
+        return hit
+
     def material_tables(self, frequencies: list[float], device: torch.device) -> MaterialTables:
         """Material and layer tables at ``frequencies``: every value packed into
         one float and one int buffer, each copied to the device once (pinned,

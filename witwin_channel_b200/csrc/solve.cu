@@ -557,6 +557,24 @@ static long long seq_count(long long g, int d) {
     return g;
 }
 
+// Per-transmitter chain offsets written on the device (no host staging, so a
+// solve can be captured in a CUDA graph): offs[t*kMaxDepth + k] =
+// t*per_tx + base[k].
+struct ChainBase {
+    long long v[kMaxDepth];
+};
+
+__global__ void k_chain_offsets(long long* offs, int num_tx, long long per_tx, ChainBase base) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= num_tx * kMaxDepth) return;
+    const int t = i / kMaxDepth, k = i - t * kMaxDepth;
+    offs[i] = (long long)t * per_tx + base.v[k];
+}
+
+__global__ void k_set_count(int* dst, int value) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *dst = value;
+}
+
 static ChainPlan make_plan(const SceneDev& sc, int max_depth, int rays) {
     ChainPlan pl;
     const long long G = sc.num_groups;
@@ -712,7 +730,13 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
     std::vector<int> fixed_counts(size_t(T) * kMaxDepth, 0);
     for (int t = 0; t < T; ++t)
         for (int k = 0; k < kMaxDepth; ++k) offs[t * kMaxDepth + k] = t * L.chain_ints_per_tx + pl.offset_int[k];
-    cudaMemcpyAsync(chain_offsets, offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, stream);
+    {
+        ChainBase cb;
+        for (int k = 0; k < kMaxDepth; ++k) cb.v[k] = pl.offset_int[k];
+        const int n = T * kMaxDepth;
+        k_chain_offsets<<<(n + 255) / 256, 256, 0, stream>>>(chain_offsets, T, L.chain_ints_per_tx, cb);
+        note_launch();
+    }
     const int B = 256;
     // traversal stacks: a descent pushes at most one entry per tree level, so
     // the measured BVH depth (+2) bounds them
@@ -815,8 +839,8 @@ int solve(const SceneHandle* h, const wcb_solve_desc* d, const wcb_materials* m,
                         k_chain_images<<<int((total + B - 1) / B), B, 0, side>>>(sc, txp, depth, nullptr, total, cgrp, cpl, cim, cpre);
                         note_launch(2);
                     }
-                    cudaMemcpyAsync(chain_counts + t * kMaxDepth + k, &fixed_counts[t * kMaxDepth + k], 4,
-                                    cudaMemcpyHostToDevice, side);
+                    k_set_count<<<1, 32, 0, side>>>(chain_counts + t * kMaxDepth + k, int(total));
+                    note_launch();
                 } else {
                     const long long cap = pl.cap[k];
                     k_chain_images<<<int((cap + B - 1) / B), B, 0, side>>>(sc, txp, depth, chain_counts + t * kMaxDepth + k,

@@ -1608,8 +1608,7 @@ def reevaluate(compiled_scene: CompiledScene, request: FixedTopologyRequest) -> 
     status = torch.zeros(2, dtype=torch.int32, device=device)
     launches0 = _native.launch_count()
     with torch.cuda.device(device):
-        mats = compiled.material_tables(columns, device)
-        freqs = torch.tensor(columns, dtype=torch.float64).pin_memory().to(device, non_blocking=True)
+        mats, freqs = compiled.resident_tables(columns, device)
         rows = _native.FrozenRows()
         rows.num_rows = K
         rows.width = width
