@@ -83,6 +83,17 @@ int wcb_scene_destroy(wcb_scene* scene);
 int wcb_scene_refit(wcb_scene* scene, const float* vertices, int64_t num_vertices, int32_t* topology_changed,
                     void* stream);
 /* counts[0..5] = faces, groups, selected edges, bvh depth, bvh nodes, representative faces */
+/* Rebuilds the compiled scene's BVH on the device from its current vertices
+ * (north_star (a): a linear BVH from 30-bit Morton codes of the face
+ * centroids, radix-sorted, the radix tree of Karras (HPG 2012), boxes
+ * bottom-up); no reference counterpart (the reference builds its BVH inside
+ * RayD on the host at compile, scene/compiler.py:1306-1450).  Same node
+ * layout as the compile's SAH tree, so every kernel traverses it unchanged;
+ * the discrete compile decisions (groups, edges) are untouched.  *depth
+ * (may be NULL) receives the tree depth.  A tree deeper than the traversal
+ * stack returns WCB_ERR_BVH_DEPTH and leaves the old tree in place.
+ * Synchronises `stream`; no solve on this scene may run meanwhile. */
+int wcb_scene_rebuild_bvh(wcb_scene* scene, int32_t* depth, void* stream);
 int wcb_scene_info(const wcb_scene* scene, int64_t* counts);
 /* Group table export: face_group (F) i32, group_rep (G) i32 (device). */
 int wcb_scene_groups(const wcb_scene* scene, int32_t* face_group, int32_t* group_rep, void* stream);

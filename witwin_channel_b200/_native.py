@@ -181,6 +181,7 @@ EXPORTED_SYMBOLS = (
     "wcb_scene_create",
     "wcb_scene_destroy",
     "wcb_scene_refit",
+    "wcb_scene_rebuild_bvh",
     "wcb_scene_info",
     "wcb_scene_groups",
     "wcb_scene_edges",
@@ -241,6 +242,7 @@ def load() -> ctypes.CDLL:
                                      ctypes.c_int32, ctypes.c_double, _vp, ctypes.POINTER(_vp)]
     lib.wcb_scene_destroy.argtypes = [_vp]
     lib.wcb_scene_refit.argtypes = [_vp, _vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int32), _vp]
+    lib.wcb_scene_rebuild_bvh.argtypes = [_vp, ctypes.POINTER(ctypes.c_int32), _vp]
     lib.wcb_scene_info.argtypes = [_vp, _i64p]
     lib.wcb_scene_groups.argtypes = [_vp, _vp, _vp, _vp]
     lib.wcb_scene_edges.argtypes = [_vp, _vp, _vp]

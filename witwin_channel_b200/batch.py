@@ -148,6 +148,7 @@ class BatchGraph:
 
     def _launch(self, pool: list, keep: list) -> None:
         current = torch.cuda.current_stream(self.device)
+        pool = pool[:max(1, min(len(pool), len(self._items)))]  # only streams that take work join a capture
         for i, item in enumerate(self._items):
             s = pool[i % len(pool)]
             s.wait_stream(current)

@@ -64,6 +64,15 @@ class NativeScene:
         )
         self._finalizer = weakref.finalize(self, lib.wcb_scene_destroy, handle)
 
+    def rebuild_bvh(self) -> int:
+        """Rebuild the BVH on the device from the current vertices (a linear
+        BVH from Morton codes, ``wcb_scene_rebuild_bvh``); returns its depth."""
+        lib = _native.load()
+        depth = _native.ctypes.c_int32(0)
+        _native.check(lib.wcb_scene_rebuild_bvh(self.handle, _native.ctypes.byref(depth),
+                                                _native.stream_handle(self.device)), "wcb_scene_rebuild_bvh")
+        return int(depth.value)
+
     def refit(self, vertices: torch.Tensor) -> bool:
         """Move the compiled scene to ``vertices`` (same count, on this
         device) in place.  Returns False, changing nothing, when the move

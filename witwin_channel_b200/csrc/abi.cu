@@ -160,6 +160,15 @@ int wcb_field_free_space(int64_t n, const float* source, const float* target, co
                                  path_field, path_gain, path_length, delay, direction, as_stream(stream));
 }
 
+int wcb_scene_rebuild_bvh(wcb_scene* scene, int32_t* depth, void* stream) {
+    if (scene == nullptr) return WCB_ERR_INVALID_ARGUMENT;
+    int d = 0;
+    const int rc = wcb::scene_rebuild_bvh(scene->h, &d, as_stream(stream));
+    if (depth) *depth = d;
+    if (rc == 4) return WCB_ERR_BVH_DEPTH;
+    return rc == 0 ? WCB_OK : (rc == 1 ? WCB_ERR_INVALID_ARGUMENT : WCB_ERR_CUDA);
+}
+
 int wcb_rows_replay(const wcb_scene* scene, const wcb_frozen_rows* rows, const wcb_endpoint_batch* sources,
                     const wcb_endpoint_batch* sinks, int64_t slot_count, const wcb_materials* materials,
                     const double* frequencies, int32_t num_columns, int32_t test_visibility,

@@ -59,6 +59,8 @@ int rows_accumulate(const void* rows, const int64_t* selected, int64_t n, const 
                     const wcb_outputs* out, cudaStream_t stream);
 int field_free_space(int64_t n, const float* s, const float* t, const float* pw, const float* tp, const float* rp, double f,
                      float* fv, float* c, float* pf, float* pg, float* pl, float* dl, float* dr, cudaStream_t stream);
+int refit_boxes(SceneHandle* h, cudaStream_t stream);
+int scene_rebuild_bvh(SceneHandle* h, int* depth_out, cudaStream_t stream);
 int rows_replay(const SceneHandle* h, const wcb_frozen_rows* rows, const wcb_endpoint_batch* src,
                 const wcb_endpoint_batch* snk, int64_t slot_count, const wcb_materials* m, const double* freqs,
                 int num_columns, int visibility, const wcb_replay_outputs* out, int* status, cudaStream_t stream);

@@ -492,6 +492,19 @@ __global__ void k_diagonal(const float* v, int V, double* diagonal) {
 
 }  // namespace refit
 
+// Boxes of the compiled scene's BVH from its current leaf triangles and parent
+// links (bvh_counter zeroed by the caller), bottom-up.
+int refit_boxes(SceneHandle* h, cudaStream_t stream) {
+    using namespace refit;
+    const SceneDev& sd = h->dev;
+    const int F = sd.num_faces;
+    if (F < 2) return 0;
+    k_bvh<<<(F + kB - 1) / kB, kB, 0, stream>>>(sd.vertices, sd.faces, sd.tri, F, h->leaf_parent, h->node_parent,
+                                                const_cast<BvhNode*>(sd.nodes), h->bvh_counter);
+    note_launch();
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
 int scene_refit(SceneHandle* h, const float* d_vertices, int64_t nv, int* topology_changed, cudaStream_t stream) {
     using namespace refit;
     if (h == nullptr || topology_changed == nullptr || (nv > 0 && d_vertices == nullptr)) return 1;
