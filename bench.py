@@ -209,6 +209,8 @@ def run_leg(args) -> None:
         leg = _canyon_run(args, device)
     elif args.only_leg == "consumer":
         leg = _consumer_run(device)
+    elif args.only_leg == "large":
+        leg = _large_run(device)
     else:
         leg = _vjp_run(device)
     print(json.dumps({"leg": args.only_leg, **leg}), flush=True)
@@ -1131,7 +1133,7 @@ def main() -> None:
     ap.add_argument("--no-large", action="store_true")
     ap.add_argument("--no-consumer", action="store_true")
     ap.add_argument("--no-canyon", action="store_true")
-    ap.add_argument("--only-leg", choices=["canyon", "vjp", "consumer"], default=None,
+    ap.add_argument("--only-leg", choices=["canyon", "vjp", "consumer", "large"], default=None,
                     help="run one side leg alone (profiling runs); no headline line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "native":

@@ -349,8 +349,10 @@ int wcb_rows_vjp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
  * row_field (K,2) FP64, the re-evaluated field.  With tangent NULL only
  * row_field is written (a plain FP64 evaluation, no dual lane): the records'
  * fields the derivatives are linearised at.  order / comp_counts (optional,
- * from wcb_rows_order) run each component's records in that order.  No
- * workspace, no host sync. */
+ * from wcb_rows_order) run each component's records in that order.
+ * freq_index -1 (tangent NULL): the fields at every frequency of the desc,
+ * row_field (NF,K,2); diffraction records form their frequency-independent
+ * UTD geometry once for up to 4 frequencies.  No workspace, no host sync. */
 int wcb_rows_jvp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_materials* materials,
                  int32_t freq_index, const void* rows, const int64_t* selected, int64_t num_selected,
                  const double* tangent, int64_t tangent_size, double* row_field, double* row_field_tangent,

@@ -87,3 +87,21 @@ def test_captured_batch_graph_replays_the_eager_batch():
         assert torch.equal(a["path_gain"], b["path_gain"])
     with pytest.raises(ValueError):
         BatchGraph(scenes, Config(components={"los"}, ad_mode="vjp"), FREQS)
+
+
+def test_all_frequency_linearisation_equals_per_frequency_fields():
+    """``wcb_rows_jvp`` with ``freq_index=-1`` (every frequency in one pass,
+    diffraction geometry shared) gives each frequency's FP64 record fields."""
+    from witwin_channel_b200 import autograd as ad
+
+    scene = _two_tx_city(9)
+    cfg = Config(components={"los", "reflection", "diffraction"}, max_depth=2, ad_mode="vjp")
+    freqs = torch.tensor((3.5e9, 6.0e9, 28.0e9, 39.0e9), dtype=torch.float64, requires_grad=True)
+    v = ad.vjp_forward(scene, cfg, freqs)
+    assert v["count"] > 0
+    state = v["power_total"].grad_fn.state  # the autograd node keeps the frozen records
+    both = ad.rows_field64_all(state)
+    assert tuple(both.shape) == (4, v["count"], 2)
+    for fi in range(4):
+        one, _ = ad.rows_jvp(state, fi, None)
+        torch.testing.assert_close(both[fi], one, rtol=1e-12, atol=1e-30)

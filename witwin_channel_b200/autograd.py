@@ -91,13 +91,41 @@ def _linearisation(state: _State, fi: int) -> dict:
     terms cancel amplifies their rounding into the gradient.)  Computed once
     per frequency by one plain FP64 ``wcb_rows_jvp`` pass (no tangent) and cached."""
     if state.saved64[fi] is None:
-        field, _ = rows_jvp(state, fi, None)
-        re, im = field[:, 0].contiguous(), field[:, 1].contiguous()
-        gain = (re * re + im * im).contiguous()
+        # every frequency in one pass (diffraction records share their UTD
+        # geometry across the frequencies), each accumulated in FP64
+        fields = rows_field64_all(state) if len(state.frequencies) > 1 else rows_jvp(state, fi, None)[0][None]
         f_ = state.flat
-        state.saved64[fi] = _forward(f_["valid"], f_["tx"], f_["rx"], f_["cid"], gain, re, im, state.ep.num_tx,
-                                     state.ep.num_rx, state.coherent, 0)
+        for fj in range(len(state.frequencies)):
+            if state.saved64[fj] is not None:
+                continue
+            field = fields[fj]
+            re, im = field[:, 0].contiguous(), field[:, 1].contiguous()
+            gain = (re * re + im * im).contiguous()
+            state.saved64[fj] = _forward(f_["valid"], f_["tx"], f_["rx"], f_["cid"], gain, re, im, state.ep.num_tx,
+                                         state.ep.num_rx, state.coherent, 0)
     return state.saved64[fi]
+
+
+def rows_field64_all(state: _State) -> torch.Tensor:
+    """The records' FP64 path fields at every solve frequency, (NF, K, 2), in
+    one ``wcb_rows_jvp`` call (``freq_index=-1``)."""
+    lib = _native.load()
+    device = state.rows.device
+    desc, keep = engine.make_desc(state.ep, state.frequencies, state.components, state.max_depth, state.coherent)
+    ms = state.mats.as_struct()
+    K = int(state.selected.shape[0])
+    NF = len(state.frequencies)
+    field = torch.zeros((NF, max(K, 1), 2), dtype=torch.float64, device=device)
+    order, counts = _record_order(state)
+    _native.check(
+        lib.wcb_rows_jvp(state.compiled.native.handle, ctypes.byref(desc), ctypes.byref(ms), -1,
+                         _native.ptr(state.rows) if K else None, _native.ptr(state.selected) if K else None, K,
+                         None, 0, _native.ptr(field), None, _native.ptr(order), counts,
+                         _native.stream_handle(device)),
+        "wcb_rows_jvp",
+    )
+    del keep
+    return field[:, :K]
 
 
 def _as_f64(x, device) -> torch.Tensor:

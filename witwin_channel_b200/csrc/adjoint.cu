@@ -444,8 +444,55 @@ int wcb_rows_jvp(const wcb_scene* scene, const wcb_solve_desc* desc, const wcb_m
     if (num_selected > 0 && (rows == nullptr || selected == nullptr)) return WCB_ERR_INVALID_ARGUMENT;
     // no tangent: the FP64 fields alone (plain evaluation, no dual lane)
     if (tangent == nullptr ? row_field == nullptr : row_field_tangent == nullptr) return WCB_ERR_INVALID_ARGUMENT;
-    if (freq_index < 0 || freq_index >= desc->num_freq || desc->frequency_hz == nullptr)
-        return WCB_ERR_INVALID_ARGUMENT;
+    if (desc->frequency_hz == nullptr || desc->num_freq < 1) return WCB_ERR_INVALID_ARGUMENT;
+    if (freq_index == -1) {
+        // every frequency of the desc, fields only: row_field (NF, K, 2);
+        // diffraction records form their UTD geometry once for all of them
+        if (tangent != nullptr) return WCB_ERR_INVALID_ARGUMENT;
+        int64_t layout_all[9];
+        const int rc_all = wcb_rows_vjp_layout(scene, desc, materials, layout_all);
+        if (rc_all != WCB_OK) return rc_all;
+        if (num_selected == 0) return WCB_OK;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const int NF = desc->num_freq;
+        const int cids[4] = {0, 1, 5, 2};
+        long long begin = 0;
+        for (int r = 0; r < 4; ++r) {
+            const long long count = order ? (comp_counts ? comp_counts[r] : 0) : num_selected;
+            const long long at = order ? begin : 0;
+            begin += count;
+            if (count <= 0) continue;
+            const unsigned g = unsigned((count + wcb::adj::kBlock - 1) / wcb::adj::kBlock);
+            wcb::adj::AdjParams p;
+            if (cids[r] == 2 && NF <= 4) {
+                wcb::adj::fill_params(p, scene->h, desc, materials, 0, rows, selected, num_selected, layout_all);
+                p.order = order;
+                p.order_begin = at;
+                p.order_count = count;
+                wcb::adj::FreqSet fs{};
+                for (int c = 0; c < NF; ++c) fs.f[c] = desc->frequency_hz[c];
+                wcb::adj::launch_field64_diffraction_multi(p, NF, fs, row_field, s);
+                wcb::note_launch();
+                continue;
+            }
+            for (int c = 0; c < NF; ++c) {
+                wcb::adj::fill_params(p, scene->h, desc, materials, c, rows, selected, num_selected, layout_all);
+                p.order = order;
+                p.order_begin = at;
+                p.order_count = count;
+                double* out = row_field + 2 * num_selected * (long long)c;
+                switch (cids[r]) {
+                    case 0: wcb::adj::k_field64_rows<0><<<g, wcb::adj::kBlock, 0, s>>>(p, out); break;
+                    case 1: wcb::adj::k_field64_rows<1><<<g, wcb::adj::kBlock, 0, s>>>(p, out); break;
+                    case 5: wcb::adj::k_field64_rows<5><<<g, wcb::adj::kBlock, 0, s>>>(p, out); break;
+                    default: wcb::adj::launch_field64_diffraction(p, out, s); break;
+                }
+                wcb::note_launch();
+            }
+        }
+        return cudaGetLastError() == cudaSuccess ? WCB_OK : WCB_ERR_CUDA;
+    }
+    if (freq_index < 0 || freq_index >= desc->num_freq) return WCB_ERR_INVALID_ARGUMENT;
     int64_t layout[9];
     const int rc = wcb_rows_vjp_layout(scene, desc, materials, layout);
     if (rc != WCB_OK) return rc;

@@ -619,7 +619,14 @@ __global__ void __launch_bounds__(kBlock) k_field64_rows(AdjParams p, double* fi
     field[2 * i + 1] = pf.im.v;
 }
 
+// The frequencies of a multi-frequency plain evaluation (at most 4, the
+// solve's own limit per call).
+struct FreqSet {
+    double f[4];
+};
+
 void launch_field64_diffraction(const AdjParams& p, double* field, cudaStream_t s);
+void launch_field64_diffraction_multi(const AdjParams& p, int nf, const FreqSet& fs, double* field, cudaStream_t s);
 
 }  // namespace adj
 }  // namespace wcb
