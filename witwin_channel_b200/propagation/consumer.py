@@ -20,7 +20,7 @@ is index arithmetic on device tensors.
 What this engine advertises is what it does: components LoS, reflection,
 transmission and diffraction; the scalar and complex3 responses, and the
 polarimetric (LoS Jones) response through the native ``wcb_los_jones``
-(``consumer_los_jones``, ``:2037-2093``); AD mode "none".
+(``consumer_los_jones``, ``:2037-2093``).
 
 Fixed-topology replay (``prepare_fixed_topology``, ``replicate_over_slots``,
 ``reevaluate``, ``rediscovery_required``, ``evaluate_time_varying``;
@@ -28,8 +28,14 @@ reference ``:1228-1784, 3523-4342``) re-evaluates frozen LoS and reflection
 rows at new endpoint positions through one native ``wcb_rows_replay``
 launch: every row and every wideband frequency column in one pass, the
 contract validation folded into the same launch, one 8-byte status read per
-call.  AD modes other than "none" are not advertised, and requests for them
-fail before any native work.
+call.
+
+AD: ``ad_mode`` "vjp" and "jvp" differentiate the scalar coefficient on both
+routes (source and sink positions, vertices, eps_r / sigma_e and a tensor
+frequency) through the native fixed-topology VJP / JVP of the rows' records;
+the other responses, the wideband columns and the geometry outputs are
+primal-only, and requests that need them differentiated fail before any
+native work.
 """
 
 from __future__ import annotations
