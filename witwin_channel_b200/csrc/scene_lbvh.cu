@@ -63,22 +63,13 @@ WCB_D unsigned spread10(unsigned x) {
     return x;
 }
 
-// key = large << 62 | 30-bit Morton code of the normalised centroid << 32 |
-// face index (unique keys, so the tree is fully determined).  A face whose
-// box spans more than 1/16 of the centroid bounds on some axis is "large":
-// the top split then separates the large faces (a ground plane, long walls)
-// from the rest, whose subtree keeps tight boxes instead of inheriting theirs.
+// key = 30-bit Morton code of the normalised centroid << 32 | face index
+// (unique keys, so the tree is fully determined)
 __global__ void k_morton(const float* v, const int* faces, int F, const float* bounds, unsigned long long* keys,
                          int* vals) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= F) return;
     unsigned q[3];
-    bool large = false;
-    for (int k = 0; k < 3; ++k) {
-        const float a = v[3 * faces[3 * f] + k], b = v[3 * faces[3 * f + 1] + k], c = v[3 * faces[3 * f + 2] + k];
-        const float span = fmaxf(fmaxf(a, b), c) - fminf(fminf(a, b), c);
-        if (span > 0.0625f * (bounds[3 + k] - bounds[k])) large = true;
-    }
     for (int k = 0; k < 3; ++k) {
         const float c = (v[3 * faces[3 * f] + k] + v[3 * faces[3 * f + 1] + k] + v[3 * faces[3 * f + 2] + k]) *
                         (1.0f / 3.0f);
@@ -87,8 +78,7 @@ __global__ void k_morton(const float* v, const int* faces, int F, const float* b
         q[k] = unsigned(fminf(fmaxf(u * 1024.0f, 0.0f), 1023.0f));
     }
     const unsigned code = (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
-    keys[f] = (static_cast<unsigned long long>(large) << 62) | (static_cast<unsigned long long>(code) << 32) |
-              static_cast<unsigned>(f);
+    keys[f] = (static_cast<unsigned long long>(code) << 32) | static_cast<unsigned>(f);
     vals[f] = f;
 }
 
