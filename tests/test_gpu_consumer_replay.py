@@ -12,6 +12,8 @@ Checked:
   publishes as valid is a row discovery finds at the new endpoints, with the
   same numbers, every invalid row is one discovery no longer finds, and a row
   whose segment is now blocked is published as exact zeros;
+* at a moved grid, the replayed rows against the FP64 oracle's discovery
+  there (0.01 dB, 1e-3 rad);
 * wideband columns equal one replay per absolute frequency, bit for bit, and a
   zero offset reproduces the reference column;
 * slot batching and the time-varying route equal one replay per slot;
@@ -367,3 +369,63 @@ def test_stale_world_is_refused_and_fixed_winner_replay_follows_refit():
     assert c.rediscovery_required(recompiled, prepared) == "material_version"
     with pytest.raises(ValueError, match="material_version"):
         _replay(recompiled, sources, sinks, freq, prepared, world_motion="fixed_winner_replay")
+
+
+def test_moved_sink_replay_matches_the_oracle():
+    """Replay at moved sinks against the FP64 oracle's own discovery at the
+    moved grid: every valid replayed row is an oracle row (same pair,
+    component and coplanar groups) with its gain within 0.01 dB and phase
+    within 1e-3 rad; every oracle row of a frozen key is replayed as valid."""
+    from oracle import solve as osolve
+    from witwin_channel_b200.scene import make_receiver_grid
+
+    scene, freq = scenes.small_city()
+    compiled = compile_scene(scene, DEV)
+    sources, sinks = _city_batches(scene)
+    found = _discover(compiled, sources, sinks, freq, depth=2)
+    prepared = c.prepare_fixed_topology(found.paths.topology)
+    shift = (1.3, -0.9, 0.4)
+    g = scene.receivers[0]
+    moved_grid = make_receiver_grid(origin=(g.origin + torch.tensor(shift)).tolist(), x_axis=g.x_axis.tolist(),
+                                    y_axis=g.y_axis.tolist(), shape=g.shape, spacing=g.spacing)
+    # the moved sinks are exactly the oracle's moved grid points
+    pts = moved_grid.points().float()
+    moved_sinks = _batch(pts, g.polarization.detach().float().reshape(1, 3).expand(pts.shape[0], 3),
+                         [1000 + i for i in range(pts.shape[0])])
+    out = _replay(compiled, sources, moved_sinks, freq, prepared)
+    moved_scene = Scene(structures=scene.structures, endpoints=[scene.transmitters[0], moved_grid])
+    arr = osolve.scene_arrays(moved_scene, freq)
+    ref = osolve.solve(arr, frequency=freq, components={"los", "reflection"}, max_depth=2, coherent=True)["rows"]
+    face_group = compiled.native.groups()[0].cpu().numpy()
+    S = sources.count
+
+    def key(tx, rx, cid, depth, seq):
+        groups = tuple(int(face_group[f]) if f >= 0 else -1 for f in seq)
+        return (int(rx) * S + int(tx), int(cid), int(depth), groups)
+
+    W = int(prepared.topology.primitive_sequence.shape[1])
+    oracle_rows = {key(ref["tx_id"][i], ref["rx_id"][i], ref["component_id"][i], ref["depth"][i],
+                       [int(x) for x in ref["primitive_sequence"][i][:W]]): complex(ref["path_field"][i])
+                   for i in range(len(ref["tx_id"]))}
+    t = out.paths.topology
+    valid = out.row_valid.cpu().numpy()
+    coef = out.paths.transport.coefficient.cpu().numpy().astype(np.complex128)
+    strongest = max(abs(v) for v in oracle_rows.values())
+    keys = [key(*row) for row in zip(t.source_index.tolist(), t.sink_index.tolist(), t.component_id.tolist(),
+                                     t.depth.tolist(), t.primitive_sequence.tolist())]
+    frozen = {k: i for i, k in enumerate(keys)}
+    checked = 0
+    for i, k in enumerate(keys):
+        if not valid[i]:
+            assert k not in oracle_rows, k
+            continue
+        assert k in oracle_rows, k
+        want = oracle_rows[k]
+        if abs(want) > 1e-3 * strongest:
+            assert abs(20.0 * np.log10(abs(coef[i]) / abs(want))) <= 0.01, k
+            assert abs(np.angle(coef[i] / want)) <= 1e-3, k
+            checked += 1
+    assert checked > 20
+    for k in oracle_rows:
+        if k in frozen:
+            assert valid[frozen[k]], k
