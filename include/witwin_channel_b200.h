@@ -84,7 +84,7 @@ int wcb_scene_refit(wcb_scene* scene, const float* vertices, int64_t num_vertice
                     void* stream);
 /* counts[0..5] = faces, groups, selected edges, bvh depth, bvh nodes, representative faces */
 /* Rebuilds the compiled scene's BVH on the device from its current vertices
- * (north_star (a): a linear BVH from 30-bit Morton codes of the face
+ * (a linear BVH from 30-bit Morton codes of the face
  * centroids, radix-sorted, the radix tree of Karras (HPG 2012), boxes
  * bottom-up); no reference counterpart (the reference builds its BVH inside
  * RayD on the host at compile, scene/compiler.py:1306-1450).  Same node
