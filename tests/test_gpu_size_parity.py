@@ -303,7 +303,7 @@ def test_gradient_run_sampled_cells_fd():
     pg_flat = _cell_index(res.path_gain.detach(), grid.shape)[0]
     tg_flat = _cell_index(target, grid.shape)[0]
     p0 = res.paths
-    fr = torch.complex(p0.field_real, p0.field_imag).cpu().numpy().astype(np.complex128)
+    fr = torch.complex(p0.field_real, p0.field_imag).detach().cpu().numpy().astype(np.complex128)
     rx0 = p0.rx_id.cpu().numpy()
     coh = np.zeros(n, dtype=np.complex128)
     mag = np.zeros(n)

@@ -29,7 +29,7 @@ tangents to the cells with the accumulation's pushforward.
 from __future__ import annotations
 
 import ctypes
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 from typing import Any
 
 import numpy as np
@@ -341,6 +341,118 @@ class _SolveFunction(torch.autograd.Function):
         return tuple(torch.stack([o[k] for o in per_freq]).to(torch.float32) for k in ACCUM_FIELDS)
 
 
+class RowFieldFunction(torch.autograd.Function):
+    """Per-row powered path fields (K,) complex as a function of the Tx and
+    point-Rx positions, the scene's vertices and material values and the
+    frequency, with the rows' records frozen (one frequency: ``state``'s
+    first).  ``live`` (int64) are the rows that carry derivatives, one for one
+    with ``state.selected``; the others are constants (replayed rows that
+    stopped existing).  Backward runs the native fixed-topology VJP
+    (``wcb_rows_vjp``: FP64 re-evaluation of every live row, reverse mode for
+    diffraction), forward mode the native JVP (``wcb_rows_jvp``).  Used by the
+    consumer's scalar coefficient, the deterministic path table and the path
+    solver's coefficients."""
+
+    @staticmethod
+    def forward(ctx, state, coefficient, live, src, snk, vertices, eps_r, sigma_e, layer_eps_r, layer_sigma_e,
+                frequency):
+        ctx.state = state
+        ctx.live = live
+        ctx.count = int(coefficient.shape[0])
+        ctx.shapes = [tuple(t.shape) for t in (vertices, eps_r, sigma_e, layer_eps_r, layer_sigma_e, frequency, src,
+                                               snk)]
+        ctx.dtypes = [t.dtype for t in (src, snk)]
+        return coefficient.clone()
+
+    @staticmethod
+    def backward(ctx, grad):
+        state = ctx.state
+        needs = ctx.needs_input_grad
+        want = 0
+        if needs[5]:
+            want |= WANT_VERTICES
+        if any(needs[6:10]):
+            want |= WANT_MATERIALS
+        if needs[10]:
+            want |= WANT_FREQ
+        if needs[3]:
+            want |= WANT_TX
+        if needs[4]:
+            want |= WANT_RX
+        none = (None,) * 11
+        if want == 0 or grad is None or int(state.selected.shape[0]) == 0:
+            return none
+        g = grad.index_select(0, ctx.live)
+        g_re = g.real.to(torch.float64).contiguous()
+        g_im = g.imag.to(torch.float64).contiguous()
+        dense, lay = rows_vjp(state, 0, None, g_re, g_im, want, vertex_mask=state.vertex_mask)
+        parts = [dense[lay[i]:lay[i + 1]] for i in range(8)]
+        s = ctx.shapes
+        vert = parts[0].reshape(s[0])
+        mats = [parts[i].reshape(s[i]) for i in (1, 2, 3, 4)]
+        freq = parts[5].reshape(s[5]) if parts[5].numel() else torch.zeros(s[5], dtype=torch.float64,
+                                                                            device=dense.device)
+        src = parts[6].reshape(s[6]).to(ctx.dtypes[0])
+        snk = parts[7].reshape(s[7]).to(ctx.dtypes[1])
+        grads = (src, snk, vert, *mats, freq)
+        return (None, None, None) + tuple(x if needs[i + 3] else None for i, x in enumerate(grads))
+
+    @staticmethod
+    def jvp(ctx, _t_state, _t_coefficient, _t_live, t_src, t_snk, t_vertices, t_eps, t_sig, t_leps, t_lsig, t_freq):
+        state = ctx.state
+        dev = state.rows.device
+        s = ctx.shapes
+
+        def flat(t, shape):
+            if t is None:
+                return torch.zeros(int(np.prod(shape)), dtype=torch.float64, device=dev)
+            return t.reshape(-1).to(device=dev, dtype=torch.float64)
+
+        out = torch.zeros(ctx.count, dtype=torch.complex64, device=dev)
+        if int(state.selected.shape[0]) == 0:
+            return out
+        tangent = torch.cat([flat(t_vertices, s[0]), flat(t_eps, s[1]), flat(t_sig, s[2]), flat(t_leps, s[3]),
+                             flat(t_lsig, s[4]), flat(t_freq, s[5]), flat(t_src, s[6]), flat(t_snk, s[7])])
+        _field, dfield = rows_jvp(state, 0, tangent)
+        out.index_copy_(0, ctx.live, torch.complex(dfield[:, 0], dfield[:, 1]).to(torch.complex64))
+        return out
+
+
+
+def differentiable_row_fields(scene: Any, compiled: Any, ep: engine.Endpoints, mats: Any, frequency: float,
+                              frequency_input: Any, components: int, max_depth: int, rows: torch.Tensor,
+                              selected: torch.Tensor, field: torch.Tensor, tx: torch.Tensor | None = None,
+                              rx: torch.Tensor | None = None) -> torch.Tensor:
+    """``field`` ((K,) complex64, the records ``selected`` of ``rows`` at
+    ``frequency``) made differentiable in the scene's vertices and material
+    values, the frequency (when ``frequency_input`` is a tensor) and the Tx /
+    point-Rx positions (the scene's endpoints, or ``tx`` / ``rx`` when given),
+    through :class:`RowFieldFunction`."""
+    device = field.device
+    if isinstance(frequency_input, torch.Tensor):
+        freqs_t = frequency_input.reshape(1).to(device=device, dtype=torch.float64)
+    else:
+        freqs_t = torch.tensor([float(frequency)], dtype=torch.float64, device=device)
+    inputs = _differentiable_inputs(scene, compiled, freqs_t, device)
+    state = _State(compiled=compiled, ep=ep, mats=mats, frequencies=[float(frequency)], components=components,
+                   max_depth=max_depth, coherent=True, rows=rows, selected=selected, flat={}, saved64=[None],
+                   outputs32=[], layer_counts=inputs["layer_counts"], vertex_mask=inputs["vertex_mask"])
+    live = torch.arange(int(selected.shape[0]), device=device, dtype=torch.int64)
+    return RowFieldFunction.apply(state, field, live, inputs["tx"] if tx is None else tx,
+                                  inputs["rx"] if rx is None else rx, inputs["vertices"], inputs["eps_r"],
+                                  inputs["sigma_e"], inputs["layer_eps_r"], inputs["layer_sigma_e"],
+                                  inputs["frequency"])
+
+
+def unit_coefficient(coefficient: torch.Tensor, path_field: torch.Tensor, tx_power: torch.Tensor) -> torch.Tensor:
+    """The unit-excitation coefficients with the derivatives of the powered
+    ``path_field`` divided by sqrt(power) (rows of a non-positive power carry
+    none); the values are ``coefficient``'s."""
+    amp = torch.sqrt(torch.clamp(tx_power.to(torch.float32), min=0.0))
+    inv = torch.where(amp > 0, 1.0 / torch.clamp(amp, min=1e-30), torch.zeros_like(amp))
+    return coefficient + (path_field - path_field.detach()) * inv
+
+
 def vjp_forward(scene: Any, config, frequencies_hz, evaluate_rows: bool | None = None,
                 precision: str = "mixed") -> dict:
     """Row-mode forward at every frequency (geometry and records frozen once)
@@ -394,7 +506,8 @@ def vjp_forward(scene: Any, config, frequencies_hz, evaluate_rows: bool | None =
     out = _SolveFunction.apply(state, inputs["vertices"], inputs["eps_r"], inputs["sigma_e"], inputs["layer_eps_r"],
                                inputs["layer_sigma_e"], inputs["frequency"], inputs["tx"], inputs["rx"])
     result = dict(zip(ACCUM_FIELDS, out))
-    result.update(compiled=compiled, ep=ep, dec=dec, evaluations=evs, count=K, width=width)
+    result.update(compiled=compiled, ep=ep, dec=dec, evaluations=evs, count=K, width=width, rows=rows,
+                  selected=selected, mats=mats, components=bits, ep_frequency=frequencies[0])
     return result
 
 
@@ -428,6 +541,17 @@ def solve_vjp(scene: Any, config, reference_frequency_hz, precision: str = "mixe
     counts = _component_counts(dec["component_id"])
     paths = _path_table(dec, v["evaluations"][0], v["width"], v["compiled"], config.return_field) \
         if config.export_paths else None
+    if paths is not None and v["count"] > 0:
+        # the table's per-path field, gain and coefficient carry the records'
+        # fixed-topology derivatives too
+        ev = v["evaluations"][0]
+        pf = differentiable_row_fields(scene, v["compiled"], v["ep"], v["mats"], float(v["ep_frequency"]),
+                                       reference_frequency_hz, v["components"], config.max_depth, v["rows"],
+                                       v["selected"], ev["path_field"])
+        gain = ev["path_gain"] + (pf.abs() ** 2 - (pf.abs() ** 2).detach())
+        coef = unit_coefficient(ev["coefficient"], pf, v["ep"].tx_power.index_select(0, dec["tx_id"].long()))
+        fields = dict(field_real=pf.real, field_imag=pf.imag) if config.return_field else {}
+        paths = replace(paths, path_gain=gain, coefficient=coef, **fields)
     meta = _metadata(config, counts, v["count"], _native.launch_count() - launches0,
                      {"ad": f"fixed-topology {config.ad_mode}"})
     return Result(

@@ -17,7 +17,9 @@ Antenna arrays (``path.py:1079-1486``): synthetic arrays expand the centre
 endpoints' paths by far-field steering and element patterns; explicit
 arrays trace every element as its own endpoint in the same native solve.
 Endpoint weights (precoding / combining) ride on the result for
-``beamform``.  Results have one time step.
+``beamform``.  With ``ad_mode`` "vjp" / "jvp" the coefficients ``a`` carry the
+records' fixed-topology derivatives (native VJP / JVP).  Results have one time
+step.
 """
 
 from __future__ import annotations
@@ -646,8 +648,6 @@ def _validate(scene: Any, config: Config) -> None:
         raise NotImplementedError("rough-surface scattering is outside this engine")
     if config.isb_boundary_taper:
         raise NotImplementedError("the ISB boundary taper is outside this engine")
-    if config.ad_mode != "none":
-        raise NotImplementedError("the path solver is forward only here; use the deterministic solve for gradients")
     if config.max_depth < 1 and ("reflection" in config.components or "diffraction" in config.components):
         raise RuntimeError("requested reflection/diffraction paths require max_depth >= 1")
     if not torch.cuda.is_available():
@@ -939,16 +939,19 @@ def solve(scene: Any, config: Config, *, reference_frequency_hz) -> PathResult:
     _validate(scene, config)
     if explicit:
         elements = _ElementEndpoints(transmitters, receivers)
-        base = _solve_base(scene, config, frequency, elements)
+        base = _solve_base(scene, config, frequency, elements, reference_frequency_hz)
         return pack_explicit_arrays(base, transmitters=transmitters, receivers=receivers, num_rx_ant=num_rx_ant,
                                     num_tx_ant=num_tx_ant)
-    base = _solve_base(scene, config, frequency, scene)
+    base = _solve_base(scene, config, frequency, scene, reference_frequency_hz)
     return pack_synthetic_arrays(base, frequency_hz=frequency, transmitters=transmitters, receivers=receivers)
 
 
-def _solve_base(scene: Any, config: Config, frequency: float, endpoints: Any) -> PathResult:
+def _solve_base(scene: Any, config: Config, frequency: float, endpoints: Any, frequency_input: Any = None) -> PathResult:
     """One centre-endpoint solve of ``scene``'s geometry between the
-    endpoints of ``endpoints`` (``.transmitters`` / ``.receivers``)."""
+    endpoints of ``endpoints`` (``.transmitters`` / ``.receivers``).  With
+    ``config.ad_mode`` "vjp" / "jvp" the coefficients carry the records'
+    fixed-topology derivatives (vertices, materials, a tensor frequency, the
+    endpoint positions)."""
     device = torch.device("cuda", torch.cuda.current_device())
     compiled = compile_scene(scene, device)
     ep = _endpoints(endpoints, device)
@@ -1008,9 +1011,22 @@ def _solve_base(scene: Any, config: Config, frequency: float, endpoints: Any) ->
     theta_t, phi_t = endpoint_angles(departure)
     theta_r, phi_r = endpoint_angles(-arrival)
     num_tx, num_rx = int(ep.num_tx), int(ep.num_rx)
+    coefficient = ev["coefficient"]
+    if config.ad_mode != "none" and K:
+        from .autograd import differentiable_row_fields, unit_coefficient
+
+        def stack(items: list) -> torch.Tensor:
+            return torch.stack([e.position.reshape(3).to(device=device, dtype=torch.float64) for e in items]) \
+                if items else torch.zeros((0, 3), dtype=torch.float64, device=device)
+
+        rx_input = stack(list(endpoints.receivers)) if ep.rx["kind"] != "grid" else None
+        pf = differentiable_row_fields(scene, compiled, ep, mats, frequency, frequency_input, bits,
+                                       config.max_depth, rows, selected, ev["path_field"],
+                                       tx=stack(list(endpoints.transmitters)), rx=rx_input)
+        coefficient = unit_coefficient(coefficient, pf, ep.tx_power.index_select(0, tx_id))
     ragged = RaggedPathSoA.from_flat(
         num_rx=num_rx, num_rx_ant=1, num_tx=num_tx, num_tx_ant=1, rx_id=rx_id, tx_id=tx_id,
-        field=ev["coefficient"].unsqueeze(-1), delay_s=ev["delay_s"], theta_t=theta_t, phi_t=phi_t,
+        field=coefficient.unsqueeze(-1), delay_s=ev["delay_s"], theta_t=theta_t, phi_t=phi_t,
         theta_r=theta_r, phi_r=phi_r, interaction_type=types, primitive_id=seq, material_id=mat_seq, position=pos,
         normal=nrm)
     counts = {name: int((cid == c).sum().item()) for name, c in

@@ -1048,80 +1048,6 @@ def _require_ad_request(compiled: CompiledScene, request: Any, response: str, ad
                                           "capabilities().supports_higher_order_ad is False")
 
 
-class _CoefficientFunction(torch.autograd.Function):
-    """The published scalar coefficients (K,) complex as a function of the
-    source and sink positions, the scene's vertices and material values and
-    the frequency, with the rows' topology frozen.  Backward runs the native
-    fixed-topology VJP (``wcb_rows_vjp``: FP64 re-evaluation of every live
-    row, reverse-mode for diffraction), forward mode the native JVP
-    (``wcb_rows_jvp``).  Rows outside ``live`` (replayed rows that stopped
-    existing) are constants."""
-
-    @staticmethod
-    def forward(ctx, state, coefficient, live, src, snk, vertices, eps_r, sigma_e, layer_eps_r, layer_sigma_e,
-                frequency):
-        ctx.state = state
-        ctx.live = live
-        ctx.count = int(coefficient.shape[0])
-        ctx.shapes = [tuple(t.shape) for t in (vertices, eps_r, sigma_e, layer_eps_r, layer_sigma_e, frequency, src,
-                                               snk)]
-        ctx.dtypes = [t.dtype for t in (src, snk)]
-        return coefficient.clone()
-
-    @staticmethod
-    def backward(ctx, grad):
-        state = ctx.state
-        needs = ctx.needs_input_grad
-        want = 0
-        if needs[5]:
-            want |= _ad.WANT_VERTICES
-        if any(needs[6:10]):
-            want |= _ad.WANT_MATERIALS
-        if needs[10]:
-            want |= _ad.WANT_FREQ
-        if needs[3]:
-            want |= _ad.WANT_TX
-        if needs[4]:
-            want |= _ad.WANT_RX
-        none = (None,) * 11
-        if want == 0 or grad is None or int(state.selected.shape[0]) == 0:
-            return none
-        g = grad.index_select(0, ctx.live)
-        g_re = g.real.to(torch.float64).contiguous()
-        g_im = g.imag.to(torch.float64).contiguous()
-        dense, lay = _ad.rows_vjp(state, 0, None, g_re, g_im, want, vertex_mask=state.vertex_mask)
-        parts = [dense[lay[i]:lay[i + 1]] for i in range(8)]
-        s = ctx.shapes
-        vert = parts[0].reshape(s[0])
-        mats = [parts[i].reshape(s[i]) for i in (1, 2, 3, 4)]
-        freq = parts[5].reshape(s[5]) if parts[5].numel() else torch.zeros(s[5], dtype=torch.float64,
-                                                                            device=dense.device)
-        src = parts[6].reshape(s[6]).to(ctx.dtypes[0])
-        snk = parts[7].reshape(s[7]).to(ctx.dtypes[1])
-        grads = (src, snk, vert, *mats, freq)
-        return (None, None, None) + tuple(x if needs[i + 3] else None for i, x in enumerate(grads))
-
-    @staticmethod
-    def jvp(ctx, _t_state, _t_coefficient, _t_live, t_src, t_snk, t_vertices, t_eps, t_sig, t_leps, t_lsig, t_freq):
-        state = ctx.state
-        dev = state.rows.device
-        s = ctx.shapes
-
-        def flat(t, shape):
-            if t is None:
-                return torch.zeros(int(np.prod(shape)), dtype=torch.float64, device=dev)
-            return t.reshape(-1).to(device=dev, dtype=torch.float64)
-
-        out = torch.zeros(ctx.count, dtype=torch.complex64, device=dev)
-        if int(state.selected.shape[0]) == 0:
-            return out
-        tangent = torch.cat([flat(t_vertices, s[0]), flat(t_eps, s[1]), flat(t_sig, s[2]), flat(t_leps, s[3]),
-                             flat(t_lsig, s[4]), flat(t_freq, s[5]), flat(t_src, s[6]), flat(t_snk, s[7])])
-        _field, dfield = _ad.rows_jvp(state, 0, tangent)
-        out.index_copy_(0, ctx.live, torch.complex(dfield[:, 0], dfield[:, 1]).to(torch.complex64))
-        return out
-
-
 def _differentiable_coefficient(compiled: CompiledScene, request: Any, coefficient: torch.Tensor,
                                 rows: torch.Tensor, selected: torch.Tensor, live: torch.Tensor,
                                 ep: engine.Endpoints, mats: Any, frequency: float, components: int,
@@ -1140,7 +1066,7 @@ def _differentiable_coefficient(compiled: CompiledScene, request: Any, coefficie
     state = _ad._State(compiled=compiled, ep=ep, mats=mats, frequencies=[frequency], components=components,
                        max_depth=max_depth, coherent=True, rows=rows, selected=selected, flat={}, saved64=[None],
                        outputs32=[], layer_counts=inputs["layer_counts"], vertex_mask=inputs["vertex_mask"])
-    out = _CoefficientFunction.apply(state, coefficient, live, request.sources.positions_m,
+    out = _ad.RowFieldFunction.apply(state, coefficient, live, request.sources.positions_m,
                                      request.sinks.positions_m, inputs["vertices"], inputs["eps_r"],
                                      inputs["sigma_e"], inputs["layer_eps_r"], inputs["layer_sigma_e"],
                                      inputs["frequency"])
