@@ -41,7 +41,7 @@ def test_capability_record_is_frozen_and_truthful():
     for response in caps.responses:
         want = frozenset({"los"}) if response == "polarimetric_transport" else c.COMPONENTS
         assert caps.components_for(response) == want
-        want_ad = c.AD_MODES if response == "scalar_transport" else frozenset({"none"})
+        want_ad = frozenset({"none"}) if response == "polarimetric_transport" else c.AD_MODES
         assert caps.ad_modes_for(response) == want_ad
     assert caps.supports_los_jones
     for component in c.COMPONENTS:

@@ -184,9 +184,9 @@ def test_empty_batches_and_refusals():
     assert tuple(out.paths.topology.primitive_sequence.shape) == (0, 1)
     with pytest.raises(ValueError):  # the polarimetric response needs both reference bases
         c.evaluate(compiled, _request(sources, sinks, freq, {"los"}, 0, response="polarimetric_transport"))
-    for ad_mode in ("vjp", "jvp"):  # AD is offered on the scalar coefficient only
+    for ad_mode in ("vjp", "jvp"):  # the Jones operator carries no derivative
         with pytest.raises(NotImplementedError):
-            c.evaluate(compiled, _request(sources, sinks, freq, {"los"}, 0, response="complex3_transport",
+            c.evaluate(compiled, _request(sources, sinks, freq, {"los"}, 0, response="polarimetric_transport",
                                           ad_mode=ad_mode))
     with pytest.raises(ValueError):
         c.evaluate(compiled, _request(sources, sinks, freq, {"reflection"}, 0))

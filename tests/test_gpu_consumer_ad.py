@@ -294,7 +294,7 @@ def test_ad_refusals_before_native_work():
     with pytest.raises(NotImplementedError):
         c.evaluate(plain, c.PropagationRequest(sources=sources, sinks=sinks, reference_frequency_hz=FREQ,
                                                components=frozenset({"los"}), max_depth=0,
-                                               response="complex3_transport", topology_mode="discover",
+                                               response="polarimetric_transport", topology_mode="discover",
                                                ad_mode="vjp"))
     import torch.autograd.forward_ad as fwAD
 
@@ -310,3 +310,54 @@ def test_ad_refusals_before_native_work():
             sources=sources, sinks=sinks, reference_frequency_hz=FREQ,
             topology=c.prepare_fixed_topology(found.paths.topology), response="scalar_transport", ad_mode="vjp",
             frequency_offsets_hz=(1.0e6,)))
+
+
+def test_complex3_field_vjp_matches_replay_finite_differences():
+    """The complex3 field (each world component through the native VJP with
+    that axis as the sink polarization) against central differences of the
+    replayed complex3 field, for the sink positions."""
+    scene = _walls()
+    compiled = compile_scene(scene, DEV)
+    sources, sinks = _batch(SRC, 0, powers=1.0), _batch(SNK, 10)
+
+    def request3(snk, ad):
+        return c.PropagationRequest(sources=sources, sinks=snk, reference_frequency_hz=FREQ,
+                                    components=frozenset({"los", "reflection"}), max_depth=2,
+                                    response="complex3_transport", topology_mode="discover", ad_mode=ad)
+
+    found = c.evaluate(compiled, request3(sinks, "none"))
+    prepared = c.prepare_fixed_topology(found.paths.topology)
+    K = found.paths.path_count
+    g = torch.Generator().manual_seed(17)
+    w = torch.complex(torch.randn((K, 3), generator=g), torch.randn((K, 3), generator=g)).to(DEV)
+    scale = float(found.paths.transport.field.abs().max())
+
+    def loss3(field, mask):
+        m = mask.to(device=field.device, dtype=field.real.dtype).view(-1, 1)
+        return (field * m * w.to(field.dtype)).real.sum() / scale
+
+    def replay(snk_pos):
+        with torch.no_grad():
+            out = c.reevaluate(compiled, c.FixedTopologyRequest(
+                sources=sources, sinks=_batch(snk_pos, 10), reference_frequency_hz=FREQ, topology=prepared,
+                response="complex3_transport", ad_mode="none"))
+            return out.paths.transport.field.to(torch.complex128), out.row_valid
+
+    h = 1e-3
+    base = torch.tensor(SNK)
+    points = []
+    for idx in range(base.numel()):
+        for sign in (1.0, -1.0):
+            p = base.clone().reshape(-1)
+            p[idx] += sign * h
+            points.append(p.reshape(base.shape))
+    stable = _stable_rows(replay, [(p,) for p in points])
+    snk_pos = torch.tensor(SNK, device=DEV, requires_grad=True)
+    sinks_ad = c.EndpointBatch(stable_ids=sinks.stable_ids, positions_m=snk_pos, polarizations=sinks.polarizations)
+    out = c.evaluate(compiled, request3(sinks_ad, "vjp"))
+    loss3(out.paths.transport.field, stable).backward()
+    fd = torch.zeros_like(base)
+    for idx in range(base.numel()):
+        fd.reshape(-1)[idx] = (float(loss3(replay(points[2 * idx])[0], stable))
+                               - float(loss3(replay(points[2 * idx + 1])[0], stable))) / (2 * h)
+    torch.testing.assert_close(snk_pos.grad.cpu(), fd.float(), rtol=0, atol=float(2e-3 * fd.abs().max()))

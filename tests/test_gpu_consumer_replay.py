@@ -329,7 +329,7 @@ def test_contract_bitmask_and_refusals():
     with pytest.raises(ValueError, match="bitmask 34"):
         _replay(compiled, _stack([sources, sources]), _stack([sinks, sinks]), freq, broken, slot_count=2)
     with pytest.raises(NotImplementedError):
-        _replay(compiled, sources, sinks, freq, prepared, response="complex3_transport", ad_mode="vjp")
+        _replay(compiled, sources, sinks, freq, prepared, response="polarimetric_transport", ad_mode="vjp")
     with pytest.raises(ValueError, match="polarization_basis"):
         _replay(compiled, sources, sinks, freq, prepared, response="polarimetric_transport")
     with pytest.raises(NotImplementedError):

@@ -30,12 +30,12 @@ launch: every row and every wideband frequency column in one pass, the
 contract validation folded into the same launch, one 8-byte status read per
 call.
 
-AD: ``ad_mode`` "vjp" and "jvp" differentiate the scalar coefficient on both
-routes (source and sink positions, vertices, eps_r / sigma_e and a tensor
-frequency) through the native fixed-topology VJP / JVP of the rows' records;
-the other responses, the wideband columns and the geometry outputs are
-primal-only, and requests that need them differentiated fail before any
-native work.
+AD: ``ad_mode`` "vjp" and "jvp" differentiate the scalar coefficient and the
+complex3 field on both routes (source and sink positions, vertices, eps_r /
+sigma_e and a tensor frequency) through the native fixed-topology VJP / JVP
+of the rows' records; the Jones operator, the wideband columns and the
+geometry outputs are primal-only, and requests that need them differentiated
+fail before any native work.
 """
 
 from __future__ import annotations
@@ -653,9 +653,9 @@ _CAPABILITIES = PropagationCapabilities(
     world_motions=WORLD_MOTIONS,
     world_version_domains=WORLD_VERSION_DOMAINS,
     response_components=_RESPONSE_COMPONENTS,
-    # the scalar coefficient is differentiated (native fixed-topology VJP / JVP
-    # of every component); the complex3 field and the Jones operator are not
-    response_ad_modes=tuple((response, AD_MODES if response == "scalar_transport" else _SUPPORTED_AD_MODES)
+    # the scalar coefficient and the complex3 field are differentiated (native
+    # fixed-topology VJP / JVP of every component); the Jones operator is not
+    response_ad_modes=tuple((response, _SUPPORTED_AD_MODES if response == "polarimetric_transport" else AD_MODES)
                             for response in sorted(_SUPPORTED_RESPONSES)),
     component_ad_modes=tuple((component, AD_MODES) for component in sorted(COMPONENTS)),
     fixed_topology_components=frozenset(name for name, _ in _FIXED_TOPOLOGY_COMPONENT_IDS),
@@ -960,8 +960,14 @@ def evaluate(compiled_scene: CompiledScene, request: PropagationRequest) -> Prop
             # published field carries the source amplitude sqrt(powers_w)
             # (a negative power counts as zero, as in the row kernel)
             amplitude = torch.sqrt(torch.clamp(sources.powers_w.index_select(0, tx.to(torch.int64)), min=0.0))
-            field = take(ev["field_xyz"], torch.complex64) * amplitude.view(-1, 1)
-            transport = Complex3Transport(field=field.contiguous(), direction=direction)
+            field = (take(ev["field_xyz"], torch.complex64) * amplitude.view(-1, 1)).contiguous()
+            if request.ad_mode != "none":
+                pub = selected if order is None else selected.index_select(0, order)
+                K = int(pub.shape[0])
+                field, ad_tape = _differentiable_field3(
+                    compiled, request, field, rows, pub.contiguous(),
+                    torch.arange(K, device=device, dtype=torch.int64), ep, mats, frequency, bits, width)
+            transport = Complex3Transport(field=field, direction=direction)
     paths = PropagationPathBatch(pair_count=S * R, path_count=int(pair_index.numel()), pair_index=pair_index,
                                  pair_offsets=pair_offsets, topology=topology, geometry=geometry, transport=transport)
     # host observations: the solve's record count (8 bytes) and status word
@@ -1023,8 +1029,8 @@ def _require_ad_request(compiled: CompiledScene, request: Any, response: str, ad
 
     if ad_mode == "none":
         return
-    if response != "scalar_transport":
-        raise NotImplementedError(f"ad_mode={ad_mode!r} is provided for scalar_transport only; "
+    if response == "polarimetric_transport":
+        raise NotImplementedError(f"ad_mode={ad_mode!r} is provided for scalar_transport and complex3_transport; "
                                   f"capabilities().ad_modes_for({response!r}) is {{'none'}}")
     values: list[tuple[str, object]] = [
         ("sources.powers_w", request.sources.powers_w), ("sources.polarizations", request.sources.polarizations),
@@ -1072,6 +1078,28 @@ def _differentiable_coefficient(compiled: CompiledScene, request: Any, coefficie
                                      inputs["frequency"])
     tape = rows.numel() * 4 + (selected.numel() + live.numel()) * 8
     return out, tape
+
+
+def _differentiable_field3(compiled: CompiledScene, request: Any, field: torch.Tensor, rows: torch.Tensor,
+                           selected: torch.Tensor, live: torch.Tensor, ep: engine.Endpoints, mats: Any,
+                           frequency: float, components: int, max_depth: int) -> tuple[torch.Tensor, int]:
+    """Attach the native fixed-topology derivatives to the complex3 field
+    ``field`` (K,3): component k is the row's field projected on the world
+    axis e_k, the scalar field with e_k as the sink polarization.  The field
+    is transverse to its arrival direction, so that projection is E_k and its
+    derivative is dE_k exactly (the direction's own derivative cancels)."""
+
+    columns, tape = [], 0
+    for k in range(3):
+        axis = torch.zeros((1, 3), dtype=torch.float32, device=field.device)
+        axis[0, k] = 1.0
+        ep_k = engine.Endpoints(tx_pos=ep.tx_pos, tx_power=ep.tx_power, tx_pol=ep.tx_pol,
+                                rx={**ep.rx, "pol": axis, "pol_stride": 0})
+        col, t = _differentiable_coefficient(compiled, request, field[:, k].contiguous(), rows, selected, live,
+                                             ep_k, mats, frequency, components, max_depth)
+        columns.append(col)
+        tape += t
+    return torch.stack(columns, dim=1), tape
 
 
 def _frozen_records(topology: PropagationTopology) -> torch.Tensor:
@@ -1587,9 +1615,15 @@ def reevaluate(compiled_scene: CompiledScene, request: FixedTopologyRequest) -> 
             rx={"kind": "point", "grid": None, "count": R, "shape": None, "pol": sinks.polarizations.detach(),
                 "pol_stride": 3 if R > 0 else 0, "positions": sinks.positions_m.detach()})
         mats1 = compiled.material_tables([frequency], device)
-        coefficient, ad_tape = _differentiable_coefficient(
-            compiled, request, coefficient, _frozen_records(topology), live, live, ep, mats1, frequency,
-            engine.component_bits(frozenset({"los", "reflection"})), max(width, 1))
+        bits = engine.component_bits(frozenset({"los", "reflection"}))
+        if response == "scalar_transport":
+            coefficient, ad_tape = _differentiable_coefficient(
+                compiled, request, coefficient, _frozen_records(topology), live, live, ep, mats1, frequency, bits,
+                max(width, 1))
+        else:
+            field, ad_tape = _differentiable_field3(
+                compiled, request, field, _frozen_records(topology), live, live, ep, mats1, frequency, bits,
+                max(width, 1))
     if polarimetric:
         transport: PropagationTransport = JonesTransport(matrix=jones, source_basis=source_basis,
                                                          sink_basis=sink_basis)
