@@ -357,8 +357,14 @@ __global__ void __launch_bounds__(kSplitBlock, sizeof(T) == 4 ? 3 : 2) k_reflect
             const double total = length(R - img);
             const V3<T> RT = cast3<T>(R);
             const V3<T> rx_pol = v3<T>(T(px), T(py), T(pz));
+            // a records-only solve (no cell output requested: the
+            // differentiable forward, which re-evaluates the records in FP64)
+            // keeps the path and skips its field
+            const int nf_fields = (p.out_comp_power || p.out_comp_field) ? NF : 0;
+            for (int f = nf_fields; f < NF; ++f)
+                for (int k = 0; k < 3; ++k) sh->contrib[(lane * NF + f) * 3 + k] = 0.f;
 #pragma unroll 1
-            for (int f = 0; f < NF; ++f) {
+            for (int f = 0; f < nf_fields; ++f) {
                 const double freq = p.freq[f];
                 const T wl = T(kC0 / freq);
                 V3<T> prev = ST;
