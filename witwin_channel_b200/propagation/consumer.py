@@ -46,8 +46,6 @@ from typing import Any, Literal, TypeAlias, get_args
 
 import torch
 
-import numpy as np
-
 from .. import _native, engine
 from .. import autograd as _ad
 from ..compiler import CompiledScene
