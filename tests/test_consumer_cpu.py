@@ -52,7 +52,7 @@ def test_capability_record_is_frozen_and_truthful():
     assert caps.material_leaves_for("los") == ()
     assert "layer_eps_r" in caps.material_leaves_for("transmission")
     assert caps.differentiable_geometry_for("discovery") == frozenset()
-    assert caps.differentiable_geometry_for("fixed_topology") == frozenset()
+    assert caps.differentiable_geometry_for("fixed_topology") == frozenset({"path_length_m", "delay_s"})
     assert caps.supports_fixed_topology and caps.supports_wideband_offsets and caps.supports_slot_batching
     assert caps.fixed_topology_components == frozenset({"los", "reflection"})
     assert caps.fixed_topology_row_validity_components == frozenset({"los", "reflection"})

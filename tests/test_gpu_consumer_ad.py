@@ -361,3 +361,58 @@ def test_complex3_field_vjp_matches_replay_finite_differences():
         fd.reshape(-1)[idx] = (float(loss3(replay(points[2 * idx])[0], stable))
                                - float(loss3(replay(points[2 * idx + 1])[0], stable))) / (2 * h)
     torch.testing.assert_close(snk_pos.grad.cpu(), fd.float(), rtol=0, atol=float(2e-3 * fd.abs().max()))
+
+
+def test_replayed_path_lengths_and_delays_carry_geometry_derivatives():
+    """Replay path lengths (and delays) differentiate in the sink positions and
+    a wall's vertices: against central differences of the replayed lengths."""
+    scene = _walls()
+    scene.structures[1].geometry.vertices = scene.structures[1].vertices.clone().requires_grad_(True)
+    compiled = compile_scene(scene, DEV)
+    sources, sinks = _batch(SRC, 0, powers=1.0), _batch(SNK, 10)
+    found = c.evaluate(compiled, _request(sources, sinks, ad="none"))
+    prepared = _unanchored(c.prepare_fixed_topology(found.paths.topology))
+    K = found.paths.path_count
+    w = torch.rand(K, generator=torch.Generator().manual_seed(23)).to(DEV)
+    v0 = scene.structures[1].vertices.detach().clone()
+
+    def replay(snk, verts=None):
+        sc = _walls()
+        if verts is not None:
+            sc.structures[1].geometry.vertices = verts
+        comp = compile_scene(sc, DEV)
+        with torch.no_grad():
+            out = _replay(comp, sources, _batch(snk, 10), prepared, ad="none")
+            return out.paths.geometry.path_length_m.double(), out.row_valid
+
+    h = 1e-3
+    base = torch.tensor(SNK)
+    snk_points, vert_points = [], []
+    for idx in range(base.numel()):
+        for sign in (1.0, -1.0):
+            p = base.clone().reshape(-1)
+            p[idx] += sign * h
+            snk_points.append(p.reshape(base.shape))
+    for idx in range(v0.numel()):
+        for sign in (1.0, -1.0):
+            p = v0.clone().reshape(-1)
+            p[idx] += sign * h
+            vert_points.append(p.reshape(v0.shape))
+    stable = _stable_rows(lambda s: replay(s), [(p,) for p in snk_points])
+    stable = stable & _stable_rows(lambda v: replay(base, v), [(v,) for v in vert_points])
+    m = stable.double()
+    snk_pos = torch.tensor(SNK, device=DEV, requires_grad=True)
+    sinks_ad = c.EndpointBatch(stable_ids=sinks.stable_ids, positions_m=snk_pos, polarizations=sinks.polarizations)
+    out = _replay(compiled, sources, sinks_ad, prepared)
+    L = out.paths.geometry.path_length_m
+    assert L.requires_grad and out.paths.geometry.delay_s.requires_grad
+    torch.testing.assert_close(out.paths.geometry.delay_s, L / 299_792_458.0, rtol=1e-6, atol=0.0)
+    (L.double() * w * m).sum().backward()
+    loss = lambda lengths: float((lengths * w * m).sum())
+    fd = torch.tensor([(loss(replay(snk_points[2 * i])[0]) - loss(replay(snk_points[2 * i + 1])[0])) / (2 * h)
+                       for i in range(base.numel())], dtype=torch.float64).reshape(base.shape)
+    torch.testing.assert_close(snk_pos.grad.cpu().double(), fd, rtol=0, atol=2e-3 * float(fd.abs().max()))
+    gv = scene.structures[1].vertices.grad.reshape(-1).double().cpu()
+    fdv = torch.tensor([(loss(replay(base, vert_points[2 * i])[0]) - loss(replay(base, vert_points[2 * i + 1])[0]))
+                        / (2 * h) for i in range(v0.numel())], dtype=torch.float64)
+    torch.testing.assert_close(gv, fdv, rtol=0, atol=3e-3 * float(fdv.abs().max()) + 1e-9)

@@ -675,7 +675,8 @@ _CAPABILITIES = PropagationCapabilities(
     max_frequency_offset_count=None,
     native_frequency_resolution_law=NATIVE_FREQUENCY_RESOLUTION_LAW,
     component_material_leaves=_COMPONENT_MATERIAL_LEAVES,
-    differentiable_geometry_outputs=(("discovery", frozenset()), ("fixed_topology", frozenset())),
+    differentiable_geometry_outputs=(("discovery", frozenset()),
+                                     ("fixed_topology", frozenset({"path_length_m", "delay_s"}))),
     direction_differentiable_components=frozenset(),
     primal_only_ad_inputs=_PRIMAL_ONLY_AD_INPUTS,
     supports_higher_order_ad=False,
@@ -838,6 +839,8 @@ def _preflight(compiled: object, request: object) -> float:
         raise ValueError("the compiled scene and the endpoint batches must share one CUDA device")
     return _frequency_value(frequency)
 
+
+_C0_M_PER_S = 299_792_458.0
 
 # Sources the canonical record key orders directly (its 11-bit source field).
 _CANONICAL_SOURCE_LIMIT = 2048
@@ -1098,6 +1101,44 @@ def _differentiable_field3(compiled: CompiledScene, request: Any, field: torch.T
         columns.append(col)
         tape += t
     return torch.stack(columns, dim=1), tape
+
+
+def _differentiable_lengths(compiled: CompiledScene, topology: PropagationTopology, sources: EndpointBatch,
+                            sinks: EndpointBatch, length: torch.Tensor, valid: torch.Tensor | None,
+                            frequency: float) -> torch.Tensor:
+    """The replayed path lengths with the derivatives of their FP64 unfolded
+    length: |sink - image| with the source mirrored across the planes of the
+    recorded faces (each from its own vertices, the plane its coplanar group
+    shares while the group holds), differentiable in the source and sink
+    positions and the vertices, as the native derivative kernels take the
+    winner faces' planes.  The values stay the kernel's; rows that stopped
+    existing stay constant zeros."""
+
+    device = length.device
+    cid = topology.component_id.to(torch.int64)
+    depth = topology.depth.to(torch.int64)
+    img = sources.positions_m.index_select(0, topology.source_index.to(torch.int64)).to(torch.float64)
+    snk = sinks.positions_m.index_select(0, topology.sink_index.to(torch.int64)).to(torch.float64)
+    width = int(topology.primitive_sequence.shape[1])
+    if width and bool((cid == 1).any()):
+        freqs_t = torch.tensor([float(frequency)], dtype=torch.float64, device=device)
+        V = _ad._differentiable_inputs(compiled.scene, compiled, freqs_t, device)["vertices"]
+        faces = compiled.native.faces.to(torch.int64)
+        seq = topology.primitive_sequence.to(torch.int64)
+        for k in range(width):
+            active = (cid == 1) & (depth > k)
+            f = torch.where(active, seq[:, k], torch.zeros_like(seq[:, k]))
+            a, b, c = (V.index_select(0, faces[f, j]) for j in range(3))
+            n = torch.linalg.cross(b - a, c - a)
+            n = n / torch.clamp(torch.linalg.vector_norm(n, dim=-1, keepdim=True), min=1e-6)
+            off = (n * a).sum(-1, keepdim=True)
+            mirrored = img - 2.0 * n * ((n * img).sum(-1, keepdim=True) - off)
+            img = torch.where(active.unsqueeze(-1), mirrored, img)
+    unfolded = torch.linalg.vector_norm(snk - img, dim=-1)
+    out = length + (unfolded - unfolded.detach()).to(length.dtype)
+    if valid is not None:
+        out = torch.where(valid, out, torch.zeros_like(out))
+    return out
 
 
 def _frozen_records(topology: PropagationTopology) -> torch.Tensor:
@@ -1622,6 +1663,8 @@ def reevaluate(compiled_scene: CompiledScene, request: FixedTopologyRequest) -> 
             field, ad_tape = _differentiable_field3(
                 compiled, request, field, _frozen_records(topology), live, live, ep, mats1, frequency, bits,
                 max(width, 1))
+        length = _differentiable_lengths(compiled, topology, sources, sinks, length, row_valid, frequency)
+        delay = delay + ((length - length.detach()) / _C0_M_PER_S).to(delay.dtype)
     if polarimetric:
         transport: PropagationTransport = JonesTransport(matrix=jones, source_basis=source_basis,
                                                          sink_basis=sink_basis)
