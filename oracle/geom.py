@@ -421,7 +421,8 @@ def trace_reflections(tris: Triangles, normals: np.ndarray, origin: np.ndarray, 
             hit = alive & np.isfinite(tmin)
             out[s:e, depth] = np.where(hit, f, -1)
             nn = normals[f]
-            o = np.where(hit[:, None], o + tmin[:, None] * d, o)
+            # misses step by 0 (not inf * 0): the origin is kept exactly
+            o = o + np.where(hit, tmin, 0.0)[:, None] * d
             d = np.where(hit[:, None], d - 2.0 * np.sum(d * nn, axis=1)[:, None] * nn, d)
             last = np.where(hit, f, -1)
             alive = hit
