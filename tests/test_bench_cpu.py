@@ -26,3 +26,41 @@ def test_batched_jobs_balance():
         biggest = max(cost((s, 0)) for s in range(8))
         # longest processing time first: no rank exceeds the mean by more than one job
         assert max(loads) <= sum(loads) / world + biggest
+
+
+def _reference_arm(env_extra):
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="", **env_extra)
+    return subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0"],
+                          cwd=root, env=env, capture_output=True, text=True, timeout=600)
+
+
+def test_reference_arm_non_zero_rank_exits_without_work():
+    """Under torchrun only rank 0 times the CPU reference; the others exit 0 silently."""
+    r = _reference_arm({"RANK": "1", "LOCAL_RANK": "1", "WORLD_SIZE": "2"})
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == ""
+
+
+def test_reference_arm_prints_one_line_on_the_native_metric():
+    """Rank 0 prints one JSON line on the native arm's metric, unit, direction
+    and workload, with its cpu_baseline and a zero-copy e2e block."""
+    import json
+
+    r = _reference_arm({"RANK": "0", "LOCAL_RANK": "0", "WORLD_SIZE": "1"})
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["metric"] == bench.METRIC and d["unit"] == "rays/s" and d["higher_is_better"] is True
+    assert d["config"]["workload"] == bench.BATCHED_WORKLOAD
+    assert d["value"] > 0 and d["steps"] == 1
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
