@@ -5,6 +5,9 @@ Restates the reference's complex mirrors ``tests/ad/_reference_fields.py:17-337`
 sequence) which in turn mirror ``native/channel/kernels/fields.cu:36-204`` and
 RayD's ``field_transport``.  All arrays are NumPy float64 / complex128 and
 vectorised over the leading row axis.
+
+Test infrastructure only: the tests, the smoke check and the benchmark's CPU
+baseline call it as the checker; the product path never does.
 """
 
 from __future__ import annotations

@@ -2,6 +2,9 @@
 ray queries, the image-method path solve and the discovery trace.
 
 Ray/segment queries test every triangle (no BVH) in float64.
+
+Test infrastructure only: the tests, the smoke check and the benchmark's CPU
+baseline call it as the checker; the product path never does.
 """
 
 from __future__ import annotations

@@ -6,6 +6,9 @@ transmission), ``propagation/topology.py:408-466`` plus
 ``native/channel/kernels/evaluated_paths.cu:560-760`` (canonical sort, dedup,
 max_paths), ``propagation/fields.py:949-1236`` (field evaluation) and
 ``native/channel/kernels/deterministic.cu:829-970`` (accumulation).
+
+Test infrastructure only: the tests, the smoke check and the benchmark's CPU
+baseline call it as the checker; the product path never does.
 """
 
 from __future__ import annotations

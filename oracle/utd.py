@@ -35,6 +35,9 @@ The Keller stationary point and the edge numbering reproduce the reference's
 single-wedge golden lengths exactly.  Its gains: edge 1 within 0.05 dB,
 edges 2 and 5 about 1.4-1.7 dB above the golden (the residue sits in the
 library's unshipped pair evaluation).
+
+Test infrastructure only: the tests, the smoke check and the benchmark's CPU
+baseline call it as the checker; the product path never does.
 """
 
 from __future__ import annotations
