@@ -202,3 +202,22 @@ def test_edge_policy_validation_matches_reference():
         EdgePolicy(edge_diffraction=False, boundary_edge_policy="half_plane")
     assert EdgePolicy(edge_diffraction=False).boundary_edge_policy == "exclude"
     assert EdgePolicy().boundary_edge_policy == "half_plane"
+
+
+def test_trace_reflections_between_parallel_mirrors():
+    """Known-answer bounce chains between the mirrors x = 0 and x = 4 (each
+    two triangles over y, z in [-100, 100]): a ray along +x alternates
+    between them, a ray along +z escapes at once, and a ray that leaves the
+    mirrors' extent after one bounce records one face then misses."""
+    from oracle import geom
+
+    sq = np.array([[-100, -100], [100, -100], [100, 100], [-100, 100]], dtype=np.float64)
+    verts = np.concatenate([np.c_[np.zeros(4), sq], np.c_[np.full(4, 4.0), sq]])
+    faces = np.array([[0, 1, 2], [0, 2, 3], [4, 5, 6], [4, 6, 7]])
+    normals = np.array([[1.0, 0, 0], [1.0, 0, 0], [-1.0, 0, 0], [-1.0, 0, 0]])
+    tris = geom.Triangles(verts, faces)
+    dirs = np.array([[1.0, 0, 0], [0, 0, 1.0], [1.0 / np.sqrt(2), 0, 1.0 / np.sqrt(2)]])
+    with np.errstate(invalid="raise"):
+        chains = [geom.trace_reflections(tris, normals, np.array(o), dirs[i:i + 1], max_depth=4)[0].tolist()
+                  for i, o in enumerate([(1.0, 0.3, 0.2), (1.0, 0.3, 0.2), (1.0, 0.3, 95.0)])]
+    assert chains == [[2, 0, 2, 0], [-1, -1, -1, -1], [3, -1, -1, -1]]
